@@ -1,0 +1,134 @@
+"""Host-side mirror of the reference's ExplicitConvection<Order, Flux, QuadC, QuadF>
+(include/DG/DG_Schemes/ExplicitConvection.h:9-45) over the B200 kernels.
+
+    conv = ExplicitConvection(mesh, order=3, flux="LF", quad_vol=-1, quad_face=-1, gamma=1.4)
+    R = conv.eval(U, t)          # ExplicitConvection::eval, ExplicitConvection.cpp:136-141
+    R = conv.eval_cells(U, t)    # :144-198
+    R = conv.eval_internals(U, t)# :201-272
+    R = conv.eval_boundarys(U, t)# :21-128
+
+U and R are float64 arrays of shape (ncell, 5*Nb) in the reference's coefficient layout
+coef[e][5*b + k]. Like the reference, eval is stateless with respect to U and returns a new array.
+Beyond the reference interface the object also owns a device-resident state for the SSP-RK3 loop
+(set_state / ssprk3 / get_state), the diagonal mass of the drivers, and conservation sums.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+FLUX = {"LF": 0, "Roe": 1}
+PRECISION = {"fp64": 0, "mixed": 1}
+
+
+class ExplicitConvection:
+    def __init__(self, mesh, order=3, flux="LF", quad_vol=-1, quad_face=-1, gamma=1.4,
+                 precision="fp64", device=0):
+        self.mesh = mesh
+        self.order = int(order)
+        self.flux = flux
+        self.gamma = float(gamma)
+        self.precision = precision
+        cfg = L.Config(order=self.order, flux=FLUX[flux] if isinstance(flux, str) else int(flux),
+                       quad_vol=int(quad_vol), quad_face=int(quad_face), gamma=self.gamma,
+                       precision=PRECISION[precision] if isinstance(precision, str) else int(precision),
+                       device=int(device))
+        self._desc = mesh.desc()
+        err = ctypes.c_int(0)
+        self._ctx = L.lib().dg_create(ctypes.byref(self._desc), ctypes.byref(cfg), ctypes.byref(err))
+        if not self._ctx:
+            raise L.DGError(err.value, "dg_create")
+        nb, nqv, nqf, qv, qf = (ctypes.c_int() for _ in range(5))
+        L.check(L.lib().dg_info(self._ctx, ctypes.byref(nb), ctypes.byref(nqv), ctypes.byref(nqf),
+                                ctypes.byref(qv), ctypes.byref(qf)), "dg_info")
+        self.num_basis, self.nq_vol, self.nq_face = nb.value, nqv.value, nqf.value
+        self.quad_vol, self.quad_face = qv.value, qf.value
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            L.lib().dg_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        return (self.mesh.ncell, 5 * self.num_basis)
+
+    def _state(self, U):
+        U = L.as_f64(U)
+        if U.shape != self.shape:
+            U = U.reshape(self.shape)
+        return U
+
+    def _eval(self, U, t, part):
+        U = self._state(U)
+        R = np.empty(self.shape)
+        L.check(L.lib().dg_residual(self._ctx, L.dptr(U), L.dptr(R), 0, float(t), part), "dg_residual")
+        return R
+
+    def eval(self, U, t=0.0):
+        return self._eval(U, t, 0)
+
+    def eval_cells(self, U, t=0.0):
+        return self._eval(U, t, 1)
+
+    def eval_internals(self, U, t=0.0):
+        return self._eval(U, t, 2)
+
+    def eval_boundarys(self, U, t=0.0):
+        return self._eval(U, t, 3)
+
+    def eval_device(self, U_ptr, R_ptr, t=0.0, part=0, stream=0):
+        """Residual on device buffers (raw pointers, packed layout) enqueued on a CUDA stream."""
+        L.check(L.lib().dg_residual_device(self._ctx, ctypes.c_void_p(U_ptr), ctypes.c_void_p(R_ptr),
+                                           float(t), part, ctypes.c_void_p(stream)), "dg_residual_device")
+
+    def mass(self):
+        b = np.empty(self.shape)
+        L.check(L.lib().dg_mass(self._ctx, L.dptr(b), 0), "dg_mass")
+        return b
+
+    def set_dirichlet(self, UD):
+        UD = L.as_f64(UD).reshape(self.mesh.nface, self.nq_face, 5)
+        L.check(L.lib().dg_set_dirichlet(self._ctx, L.dptr(UD)), "dg_set_dirichlet")
+
+    def set_state(self, U):
+        U = self._state(U)
+        L.check(L.lib().dg_set_state(self._ctx, L.dptr(U), 0), "dg_set_state")
+
+    def get_state(self):
+        U = np.empty(self.shape)
+        L.check(L.lib().dg_get_state(self._ctx, L.dptr(U), 0), "dg_get_state")
+        return U
+
+    def ssprk3(self, dt, nsteps=1, graph=False):
+        f = L.lib().dg_ssprk3_graph if graph else L.lib().dg_ssprk3
+        L.check(f(self._ctx, float(dt), int(nsteps)), "dg_ssprk3")
+
+    def conservation(self):
+        out = np.zeros(6)
+        L.check(L.lib().dg_conservation(self._ctx, L.dptr(out)), "dg_conservation")
+        return out
+
+    def max_wave_speed(self):
+        lam = ctypes.c_double(0.0)
+        L.check(L.lib().dg_max_wave_speed(self._ctx, ctypes.byref(lam)), "dg_max_wave_speed")
+        return lam.value
+
+    def check_state(self):
+        """Number of volume points with NaN/Inf, rho <= 0 or p <= 0 (0 when the state is physical)."""
+        bad = ctypes.c_int64(0)
+        rc = L.lib().dg_check_state(self._ctx, ctypes.byref(bad))
+        if rc not in (L.DG_OK, -5):
+            L.check(rc, "dg_check_state")
+        return bad.value
+
+
+def launch_count():
+    return int(L.lib().dg_launch_count())

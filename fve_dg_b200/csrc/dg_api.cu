@@ -1,0 +1,467 @@
+// C ABI of the B200 explicit DG operator: context management, uploads, launches, RK loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "dg_internal.h"
+#include "dg_kernels_fp64.cuh"
+#include "dg_kernels_mixed.cuh"
+#include "dg_reduce.cuh"
+
+using namespace fvedg;
+
+namespace {
+std::atomic<int64_t> g_launches{0};
+
+inline int cuda_ok(cudaError_t e) { return e == cudaSuccess ? DG_OK : DG_E_CUDA; }
+#define DG_CUDA(x)                                   \
+    do {                                             \
+        cudaError_t e_ = (x);                        \
+        if (e_ != cudaSuccess) return DG_E_CUDA;     \
+    } while (0)
+
+template <typename T>
+int dev_alloc(T** p, size_t n) {
+    *p = nullptr;
+    if (n == 0) return DG_OK;
+    return cudaMalloc((void**)p, n * sizeof(T)) == cudaSuccess ? DG_OK : DG_E_NOMEM;
+}
+template <typename T>
+int upload(T** p, const std::vector<T>& v) {
+    int rc = dev_alloc(p, v.size());
+    if (rc) return rc;
+    if (v.empty()) return DG_OK;
+    return cuda_ok(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+}
+}  // namespace
+
+struct dg_ctx {
+    dg_config cfg{};
+    int qv = 0, qf = 0;
+    int64_t ncell = 0, nface = 0;
+    Tables tab;
+    cudaStream_t stream = nullptr;
+    // device data
+    double* d_geo = nullptr;       // [ncell][10]
+    FaceInfo* d_fi = nullptr;      // [nface]
+    ElemFace* d_ef = nullptr;      // [ncell][4]
+    double* d_phi_v = nullptr;
+    double* d_dphi_vw = nullptr;
+    double* d_w_v = nullptr;
+    double* d_phi_f = nullptr;
+    double* d_w_f = nullptr;
+    double* d_mass_ref = nullptr;
+    double* d_UD = nullptr;        // Dirichlet data
+    double* d_Fh = nullptr;        // [nface][nqf][5] FP64 face fluxes
+    double* d_Un = nullptr;        // state U^n
+    double* d_Ua = nullptr;        // stage buffers
+    double* d_Ub = nullptr;
+    double* d_io = nullptr;        // residual input staging
+    double* d_R = nullptr;         // residual output staging
+    double* d_red = nullptr;       // reduction partials
+    double* d_red_out = nullptr;
+    MixedData mixed;               // mixed-precision form buffers
+    bool have_state = false;
+    bool has_dirichlet = false;    // some boundary face is Dirichlet: U_D must be set first
+    cudaGraphExec_t graph = nullptr;
+    double graph_dt = 0.0;
+};
+
+namespace {
+
+size_t elem_smem_bytes(int nb, int e, int nqv) { return sizeof(double) * (size_t)e * (5 * nb + 15 * nqv); }
+
+template <int NB, int E>
+int launch_element(const StageArgs& a, cudaStream_t s) {
+    const size_t smem = elem_smem_bytes(NB, E, a.nqv);
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(element_fp64<NB, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+            return DG_E_CUDA;
+        attr = true;
+    }
+    const int grid = (a.ncell + E - 1) / E;
+    element_fp64<NB, E><<<grid, 128, smem, s>>>(a);
+    ++g_launches;
+    return cuda_ok(cudaGetLastError());
+}
+
+template <int NB>
+int launch_face(const FaceArgs& a, cudaStream_t s) {
+    const int64_t total = (int64_t)a.nface * a.nqf;
+    const int grid = (int)((total + 255) / 256);
+    face_flux_fp64<NB><<<grid, 256, 0, s>>>(a);
+    ++g_launches;
+    return cuda_ok(cudaGetLastError());
+}
+
+int dispatch_face(int order, const FaceArgs& a, cudaStream_t s) {
+    switch (order) {
+        case 1: return launch_face<4>(a, s);
+        case 2: return launch_face<10>(a, s);
+        case 3: return launch_face<20>(a, s);
+        case 4: return launch_face<35>(a, s);
+    }
+    return DG_E_ARG;
+}
+int dispatch_element(int order, const StageArgs& a, cudaStream_t s) {
+    switch (order) {
+        case 1: return launch_element<4, 32>(a, s);
+        case 2: return launch_element<10, 16>(a, s);
+        case 3: return launch_element<20, 8>(a, s);
+        case 4: return launch_element<35, 4>(a, s);
+    }
+    return DG_E_ARG;
+}
+
+FaceArgs face_args(dg_ctx* c, const double* U, int mask) {
+    FaceArgs a;
+    a.U = U;
+    a.fi = c->d_fi;
+    a.phi_f = c->d_phi_f;
+    a.w_f = c->d_w_f;
+    a.UD = c->d_UD;
+    a.Fh = c->d_Fh;
+    a.nface = (int)c->nface;
+    a.nqf = c->tab.nqf;
+    a.gamma = c->cfg.gamma;
+    a.flux = c->cfg.flux;
+    a.faces_mask = mask;
+    return a;
+}
+
+StageArgs stage_args(dg_ctx* c, const double* U, const double* U0, double* out, int mode, double dt,
+                     double a0, double a1, int with_volume) {
+    StageArgs a;
+    a.U = U;
+    a.U0 = U0;
+    a.out = out;
+    a.Fh = c->d_Fh;
+    a.geo = c->d_geo;
+    a.ef = c->d_ef;
+    a.phi_v = c->d_phi_v;
+    a.dphi_vw = c->d_dphi_vw;
+    a.phi_f = c->d_phi_f;
+    a.mass_ref = c->d_mass_ref;
+    a.ncell = (int)c->ncell;
+    a.nqv = c->tab.nqv;
+    a.nqf = c->tab.nqf;
+    a.gamma = c->cfg.gamma;
+    a.dt = dt;
+    a.a0 = a0;
+    a.a1 = a1;
+    a.mode = mode;
+    a.with_volume = with_volume;
+    return a;
+}
+
+// One residual evaluation on device buffers (packed layout), FP64 form.
+int residual_fp64(dg_ctx* c, const double* U, double* R, int part, cudaStream_t s) {
+    if (c->cfg.flux != DG_FLUX_LF && c->cfg.flux != DG_FLUX_ROE) return DG_E_ARG;
+    if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
+    const int mask = part == 0 ? 3 : part == 1 ? 0 : part == 2 ? 1 : 2;
+    int rc = dispatch_face(c->cfg.order, face_args(c, U, mask), s);
+    if (rc) return rc;
+    return dispatch_element(c->cfg.order, stage_args(c, U, U, R, 0, 0.0, 0.0, 0.0, part == 0 || part == 1), s);
+}
+
+// One SSP-RK3 step (Shu-Osher) on the device state, FP64 form:
+//   U1 = U + dt L(U);  U2 = 3/4 U + 1/4 (U1 + dt L(U1));  U = 1/3 U + 2/3 (U2 + dt L(U2)).
+int step_fp64(dg_ctx* c, double dt, cudaStream_t s) {
+    const double A0[3] = {0.0, 0.75, 1.0 / 3.0};
+    const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
+    const double* in[3] = {c->d_Un, c->d_Ua, c->d_Ub};
+    double* out[3] = {c->d_Ua, c->d_Ub, c->d_Un};
+    for (int st = 0; st < 3; ++st) {
+        int rc = dispatch_face(c->cfg.order, face_args(c, in[st], 3), s);
+        if (rc) return rc;
+        rc = dispatch_element(c->cfg.order, stage_args(c, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 1), s);
+        if (rc) return rc;
+    }
+    return DG_OK;
+}
+
+int step(dg_ctx* c, double dt, cudaStream_t s) {
+    if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
+    if (c->cfg.precision == DG_PREC_MIXED) return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches);
+    return step_fp64(c, dt, s);
+}
+
+// copy between a host buffer with element stride `stride` and a packed device buffer
+int copy_in(dg_ctx* c, double* dev, const double* host, size_t stride, cudaStream_t s) {
+    const size_t blk = sizeof(double) * 5 * c->tab.nb;
+    if (stride == 0) stride = blk;
+    if (stride < blk) return DG_E_ARG;
+    if (stride == blk) return cuda_ok(cudaMemcpyAsync(dev, host, blk * c->ncell, cudaMemcpyHostToDevice, s));
+    return cuda_ok(cudaMemcpy2DAsync(dev, blk, host, stride, blk, c->ncell, cudaMemcpyHostToDevice, s));
+}
+int copy_out(dg_ctx* c, double* host, const double* dev, size_t stride, cudaStream_t s) {
+    const size_t blk = sizeof(double) * 5 * c->tab.nb;
+    if (stride == 0) stride = blk;
+    if (stride < blk) return DG_E_ARG;
+    if (stride == blk) return cuda_ok(cudaMemcpyAsync(host, dev, blk * c->ncell, cudaMemcpyDeviceToHost, s));
+    return cuda_ok(cudaMemcpy2DAsync(host, stride, dev, blk, blk, c->ncell, cudaMemcpyDeviceToHost, s));
+}
+
+void free_ctx(dg_ctx* c) {
+    if (!c) return;
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    void* ptrs[] = {c->d_geo, c->d_fi, c->d_ef, c->d_phi_v, c->d_dphi_vw, c->d_w_v, c->d_phi_f, c->d_w_f,
+                    c->d_mass_ref, c->d_UD, c->d_Fh, c->d_Un, c->d_Ua, c->d_Ub, c->d_io, c->d_R,
+                    c->d_red, c->d_red_out};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    free_mixed(c->mixed);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dg_status_string(int s) {
+    switch (s) {
+        case DG_OK: return "ok";
+        case DG_E_ARG: return "bad argument";
+        case DG_E_MESH: return "malformed mesh";
+        case DG_E_CUDA: return "CUDA runtime error";
+        case DG_E_NOMEM: return "out of memory";
+        case DG_E_NONPHYSICAL: return "non-physical state (NaN/Inf, rho <= 0 or p <= 0)";
+        case DG_E_WATCHDOG: return "bounded device wait expired";
+        case DG_E_STATE: return "call out of order";
+    }
+    return "unknown status";
+}
+
+int64_t dg_launch_count(void) { return g_launches.load(); }
+
+dg_ctx* dg_create(const dg_mesh_desc* mesh, const dg_config* cfg, int* err) {
+    auto fail = [&](dg_ctx* c, int e) -> dg_ctx* {
+        if (err) *err = e;
+        free_ctx(c);
+        return nullptr;
+    };
+    if (!mesh || !cfg) return fail(nullptr, DG_E_ARG);
+    if (cfg->order < 1 || cfg->order > kMaxOrder || !(cfg->gamma > 1.0)) return fail(nullptr, DG_E_ARG);
+    if (cfg->flux != DG_FLUX_LF && cfg->flux != DG_FLUX_ROE) return fail(nullptr, DG_E_ARG);
+    if (cfg->precision != DG_PREC_FP64 && cfg->precision != DG_PREC_MIXED) return fail(nullptr, DG_E_ARG);
+    const int qv = cfg->quad_vol < 0 ? auto_tet_rule(cfg->order) : cfg->quad_vol;
+    const int qf = cfg->quad_face < 0 ? auto_tri_rule(cfg->order) : cfg->quad_face;
+    if (tet_rule_npts(qv) <= 0 || tri_rule_npts(qf) <= 0) return fail(nullptr, DG_E_ARG);
+    if (mesh->ncell <= 0 || mesh->ncell > (int64_t)1 << 30 || mesh->nface <= 0 || mesh->nface > (int64_t)1 << 30)
+        return fail(nullptr, DG_E_ARG);
+    Geometry geo;
+    int rc = build_geometry(mesh, &geo);
+    if (rc) return fail(nullptr, rc);
+    dg_ctx* c = new (std::nothrow) dg_ctx;
+    if (!c) return fail(nullptr, DG_E_NOMEM);
+    c->cfg = *cfg;
+    c->qv = qv;
+    c->qf = qf;
+    c->cfg.quad_vol = qv;
+    c->cfg.quad_face = qf;
+    c->ncell = mesh->ncell;
+    c->nface = mesh->nface;
+    if (cudaSetDevice(cfg->device) != cudaSuccess) return fail(c, DG_E_CUDA);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(c, DG_E_CUDA);
+    build_tables(cfg->order, qv, qf, &c->tab);
+    const int nb = c->tab.nb, nqf = c->tab.nqf;
+    // element geometry and element -> face lists
+    std::vector<double> hgeo(10 * c->ncell);
+    for (int64_t e = 0; e < c->ncell; ++e) {
+        for (int i = 0; i < 9; ++i) hgeo[10 * e + i] = geo.invjac[9 * e + i];
+        hgeo[10 * e + 9] = geo.detj[e];
+    }
+    std::vector<FaceInfo> hfi(c->nface);
+    std::vector<ElemFace> hef(4 * c->ncell);
+    std::vector<int> fill(c->ncell, 0);
+    for (int64_t f = 0; f < c->nface; ++f) {
+        FaceInfo& fi = hfi[f];
+        for (int i = 0; i < 3; ++i) fi.n[i] = geo.normal[3 * f + i];
+        fi.jw = geo.area[f] * 2.0;
+        fi.c0 = (int)mesh->face_cells[2 * f];
+        fi.c1 = mesh->face_cells[2 * f + 1] == DG_NO_CELL ? -1 : (int)mesh->face_cells[2 * f + 1];
+        const int bc = mesh->face_bc ? mesh->face_bc[f] : DG_BC_PSEUDO3DZ;
+        const int per = mesh->face_periodic ? (mesh->face_periodic[f] ? 1 : 0) : 0;
+        const int p0 = geo.perm[2 * f], p1 = fi.c1 >= 0 ? geo.perm[2 * f + 1] : 0;
+        fi.meta = p0 | (p1 << 8) | (bc << 16) | (per << 24);
+        if (fi.c1 < 0 && bc == DG_BC_DIRICHLET) c->has_dirichlet = true;
+        fi.pad = 0;
+        hef[4 * fi.c0 + fill[fi.c0]++] = ElemFace{(int)f, p0};
+        if (fi.c1 >= 0) hef[4 * fi.c1 + fill[fi.c1]++] = ElemFace{(int)f, p1 | (1 << 8)};
+    }
+    const size_t nstate = (size_t)c->ncell * 5 * nb;
+    if ((rc = upload(&c->d_geo, hgeo)) || (rc = upload(&c->d_fi, hfi)) || (rc = upload(&c->d_ef, hef)) ||
+        (rc = upload(&c->d_phi_v, c->tab.phi_v)) || (rc = upload(&c->d_dphi_vw, c->tab.dphi_vw)) ||
+        (rc = upload(&c->d_w_v, c->tab.w_v)) || (rc = upload(&c->d_phi_f, c->tab.phi_f)) ||
+        (rc = upload(&c->d_w_f, c->tab.w_f)) || (rc = upload(&c->d_mass_ref, c->tab.mass_ref)) ||
+        (rc = dev_alloc(&c->d_Fh, (size_t)c->nface * nqf * 5)) || (rc = dev_alloc(&c->d_Un, nstate)) ||
+        (rc = dev_alloc(&c->d_Ua, nstate)) || (rc = dev_alloc(&c->d_Ub, nstate)) ||
+        (rc = dev_alloc(&c->d_red, (size_t)kRedBlocks * 8)) || (rc = dev_alloc(&c->d_red_out, 8)))
+        return fail(c, rc);
+    if (cfg->precision == DG_PREC_MIXED) {
+        rc = init_mixed(c->mixed, c->tab, hgeo, hfi, hef, c->ncell, c->nface, cfg->gamma, cfg->flux);
+        if (rc) return fail(c, rc);
+    }
+    if (err) *err = DG_OK;
+    return c;
+}
+
+void dg_destroy(dg_ctx* c) {
+    if (c) cudaSetDevice(c->cfg.device);
+    free_ctx(c);
+}
+
+int dg_info(const dg_ctx* c, int* nb, int* nqv, int* nqf, int* qv, int* qf) {
+    if (!c) return DG_E_ARG;
+    if (nb) *nb = c->tab.nb;
+    if (nqv) *nqv = c->tab.nqv;
+    if (nqf) *nqf = c->tab.nqf;
+    if (qv) *qv = c->qv;
+    if (qf) *qf = c->qf;
+    return DG_OK;
+}
+
+int dg_residual_device(dg_ctx* c, const double* U, double* R, double t, int part, void* stream) {
+    (void)t;
+    if (!c || !U || !R || part < 0 || part > 3) return DG_E_ARG;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (c->cfg.precision == DG_PREC_MIXED) return residual_mixed(c->mixed, U, R, part, s, &g_launches);
+    return residual_fp64(c, U, R, part, s);
+}
+
+int dg_residual(dg_ctx* c, const double* U, double* R, size_t stride, double t, int part) {
+    if (!c || !U || !R || part < 0 || part > 3) return DG_E_ARG;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    const size_t nstate = (size_t)c->ncell * 5 * c->tab.nb;
+    int rc;
+    if (!c->d_io && (rc = dev_alloc(&c->d_io, nstate))) return rc;
+    if (!c->d_R && (rc = dev_alloc(&c->d_R, nstate))) return rc;
+    if ((rc = copy_in(c, c->d_io, U, stride, c->stream))) return rc;
+    if ((rc = dg_residual_device(c, c->d_io, c->d_R, t, part, c->stream))) return rc;
+    if ((rc = copy_out(c, R, c->d_R, stride, c->stream))) return rc;
+    return cuda_ok(cudaStreamSynchronize(c->stream));
+}
+
+int dg_set_state(dg_ctx* c, const double* U, size_t stride) {
+    if (!c || !U) return DG_E_ARG;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    int rc = copy_in(c, c->d_Un, U, stride, c->stream);
+    if (rc) return rc;
+    c->have_state = true;
+    return cuda_ok(cudaStreamSynchronize(c->stream));
+}
+
+int dg_get_state(dg_ctx* c, double* U, size_t stride) {
+    if (!c || !U) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    int rc = copy_out(c, U, c->d_Un, stride, c->stream);
+    if (rc) return rc;
+    return cuda_ok(cudaStreamSynchronize(c->stream));
+}
+
+int dg_ssprk3(dg_ctx* c, double dt, int nsteps) {
+    if (!c || nsteps < 0 || !(dt >= 0)) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    for (int i = 0; i < nsteps; ++i) {
+        int rc = step(c, dt, c->stream);
+        if (rc) return rc;
+    }
+    return cuda_ok(cudaStreamSynchronize(c->stream));
+}
+
+int dg_ssprk3_graph(dg_ctx* c, double dt, int nsteps) {
+    if (!c || nsteps < 0 || !(dt >= 0)) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    if (!c->graph || c->graph_dt != dt) {
+        if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+        cudaGraph_t g = nullptr;
+        DG_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const int64_t before = g_launches.load();
+        int rc = step(c, dt, c->stream);
+        cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+        if (rc || ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return rc ? rc : DG_E_CUDA; }
+        g_launches.store(before);  // captured launches are counted when the graph replays
+        ce = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) { c->graph = nullptr; return DG_E_CUDA; }
+        c->graph_dt = dt;
+    }
+    const int per_step = c->cfg.precision == DG_PREC_MIXED ? mixed_launches_per_step(c->mixed) : 6;
+    for (int i = 0; i < nsteps; ++i) {
+        DG_CUDA(cudaGraphLaunch(c->graph, c->stream));
+        g_launches += per_step;
+    }
+    return cuda_ok(cudaStreamSynchronize(c->stream));
+}
+
+int dg_mass(dg_ctx* c, double* mass, size_t stride) {
+    if (!c || !mass) return DG_E_ARG;
+    const int nb = c->tab.nb;
+    const size_t blk = sizeof(double) * 5 * nb;
+    if (stride == 0) stride = blk;
+    if (stride < blk) return DG_E_ARG;
+    // detJ * sum_g w_g phi_i^2, Riemann1D.cpp:108-121; host copy of the geometry is not kept, so
+    // read detJ back from the device table.
+    std::vector<double> geo(10 * c->ncell);
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    DG_CUDA(cudaMemcpy(geo.data(), c->d_geo, sizeof(double) * geo.size(), cudaMemcpyDeviceToHost));
+    for (int64_t e = 0; e < c->ncell; ++e) {
+        double* row = (double*)((char*)mass + stride * e);
+        for (int i = 0; i < nb; ++i)
+            for (int k = 0; k < 5; ++k) row[5 * i + k] = c->tab.mass_ref[i] * geo[10 * e + 9];
+    }
+    return DG_OK;
+}
+
+int dg_set_dirichlet(dg_ctx* c, const double* UD) {
+    if (!c || !UD) return DG_E_ARG;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    const size_t n = (size_t)c->nface * c->tab.nqf * 5;
+    int rc;
+    if (!c->d_UD && (rc = dev_alloc(&c->d_UD, n))) return rc;
+    DG_CUDA(cudaMemcpy(c->d_UD, UD, n * sizeof(double), cudaMemcpyHostToDevice));
+    if (c->cfg.precision == DG_PREC_MIXED) set_mixed_dirichlet(c->mixed, c->d_UD);
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    return DG_OK;
+}
+
+int dg_conservation(dg_ctx* c, double out[6]) {
+    if (!c || !out) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    return reduce_conservation(c->d_Un, c->d_geo, c->d_phi_v, c->d_w_v, (int)c->ncell, c->tab.nb, c->tab.nqv,
+                               c->d_red, out, c->stream, &g_launches);
+}
+
+int dg_max_wave_speed(dg_ctx* c, double* lam) {
+    if (!c || !lam) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    return reduce_wave_speed(c->d_Un, c->d_phi_v, (int)c->ncell, c->tab.nb, c->tab.nqv, c->cfg.gamma, c->d_red,
+                             lam, c->stream, &g_launches);
+}
+
+int dg_check_state(dg_ctx* c, int64_t* bad) {
+    if (!c) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    double nbad = 0;
+    int rc = reduce_bad_points(c->d_Un, c->d_phi_v, (int)c->ncell, c->tab.nb, c->tab.nqv, c->cfg.gamma, c->d_red,
+                               &nbad, c->stream, &g_launches);
+    if (rc) return rc;
+    if (bad) *bad = (int64_t)nbad;
+    return nbad > 0 ? DG_E_NONPHYSICAL : DG_OK;
+}
+
+}  // extern "C"

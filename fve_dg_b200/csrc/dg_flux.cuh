@@ -1,0 +1,111 @@
+// Pointwise Euler physics shared by the kernels, templated on the arithmetic type so the FP64 form
+// and the mixed form (FP32 flux) use one definition.
+//
+// Physical flux, pressure and wave speed follow src/DG/DG_Flux/EulerPhysicalFlux.cpp:7-89,
+// including the positivity clamp max(rho, 1e-16) (:59-61) and c = sqrt(gamma max(p/rho, 1e-16))
+// (:70-73). Local Lax-Friedrichs follows ExplicitConvection.cpp:232-240. The Roe flux is new (the
+// reference declares one in tests/test_flux/RiemannSolvers.h:21-27 but never defines it): Roe
+// averages, the five characteristic waves of 3D Euler, Harten's entropy fix on the acoustic waves
+// with delta = 0.1 c_roe.
+#pragma once
+
+namespace fvedg {
+
+template <typename T>
+struct Phys {
+    static __device__ __forceinline__ T positive(T v) { return v > T(1e-16) ? v : T(1e-16); }
+
+    // F . n for the state U (the 5x3 physical flux contracted with the unit normal), plus the
+    // primitive quantities the Riemann solvers reuse.
+    static __device__ __forceinline__ void flux_n(const T U[5], const T n[3], T gm1, T Fn[5], T& rho,
+                                                  T vel[3], T& p) {
+        rho = positive(U[0]);
+        const T ir = T(1) / rho;
+        vel[0] = U[1] * ir;
+        vel[1] = U[2] * ir;
+        vel[2] = U[3] * ir;
+        const T e = U[4] * ir;
+        p = gm1 * (rho * e - T(0.5) * rho * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]));
+        const T un = vel[0] * n[0] + vel[1] * n[1] + vel[2] * n[2];
+        Fn[0] = rho * un;
+        Fn[1] = rho * vel[0] * un + p * n[0];
+        Fn[2] = rho * vel[1] * un + p * n[1];
+        Fn[3] = rho * vel[2] * un + p * n[2];
+        Fn[4] = un * (rho * e + p);
+    }
+
+    // Full 5x3 flux, row = variable, column = direction (EulerPhysicalFlux.cpp:8-18).
+    static __device__ __forceinline__ void flux(const T U[5], T gm1, T F[5][3]) {
+        const T rho = positive(U[0]);
+        const T ir = T(1) / rho;
+        const T u = U[1] * ir, v = U[2] * ir, w = U[3] * ir, e = U[4] * ir;
+        const T p = gm1 * (rho * e - T(0.5) * rho * (u * u + v * v + w * w));
+        F[0][0] = rho * u;         F[0][1] = rho * v;         F[0][2] = rho * w;
+        F[1][0] = rho * u * u + p; F[1][1] = rho * v * u;     F[1][2] = rho * w * u;
+        F[2][0] = rho * u * v;     F[2][1] = rho * v * v + p; F[2][2] = rho * w * v;
+        F[3][0] = rho * u * w;     F[3][1] = rho * v * w;     F[3][2] = rho * w * w + p;
+        const T h = rho * e + p;
+        F[4][0] = u * h;           F[4][1] = v * h;           F[4][2] = w * h;
+    }
+
+    static __device__ __forceinline__ T wave_speed(T rho, const T vel[3], T p, T gam) {
+        const T c = sqrt(gam * positive(p / rho));
+        return sqrt(vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]) + c;
+    }
+
+    static __device__ __forceinline__ void lax_friedrichs(const T UL[5], const T UR[5], const T n[3],
+                                                          T gam, T Fh[5]) {
+        T FL[5], FR[5], vL[3], vR[3], rL, rR, pL, pR;
+        flux_n(UL, n, gam - T(1), FL, rL, vL, pL);
+        flux_n(UR, n, gam - T(1), FR, rR, vR, pR);
+        const T a = wave_speed(rL, vL, pL, gam), b = wave_speed(rR, vR, pR, gam);
+        const T lam = a > b ? a : b;
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) Fh[k] = T(0.5) * (FL[k] + FR[k] + lam * (UL[k] - UR[k]));
+    }
+
+    static __device__ __forceinline__ void roe(const T UL[5], const T UR[5], const T n[3], T gam, T Fh[5]) {
+        T FL[5], FR[5], uL[3], uR[3], rL, rR, pL, pR;
+        const T gm1 = gam - T(1);
+        flux_n(UL, n, gm1, FL, rL, uL, pL);
+        flux_n(UR, n, gm1, FR, rR, uR, pR);
+        const T HL = (UL[4] + pL) / rL, HR = (UR[4] + pR) / rR;
+        const T sL = sqrt(rL), sR = sqrt(rR), iden = T(1) / (sL + sR);
+        T ut[3];
+        #pragma unroll
+        for (int i = 0; i < 3; ++i) ut[i] = (sL * uL[i] + sR * uR[i]) * iden;
+        const T Ht = (sL * HL + sR * HR) * iden;
+        const T q2 = ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2];
+        const T c2 = positive(gm1 * (Ht - T(0.5) * q2));
+        const T ct = sqrt(c2);
+        const T rt = sL * sR;
+        const T unt = ut[0] * n[0] + ut[1] * n[1] + ut[2] * n[2];
+        const T dr = rR - rL, dp = pR - pL;
+        T du[3];
+        #pragma unroll
+        for (int i = 0; i < 3; ++i) du[i] = uR[i] - uL[i];
+        const T dun = du[0] * n[0] + du[1] * n[1] + du[2] * n[2];
+        T l1 = fabs(unt - ct), l2 = fabs(unt), l5 = fabs(unt + ct);
+        const T delta = T(0.1) * ct;
+        if (l1 < delta) l1 = (l1 * l1 + delta * delta) / (T(2) * delta);
+        if (l5 < delta) l5 = (l5 * l5 + delta * delta) / (T(2) * delta);
+        const T a1 = (dp - rt * ct * dun) / (T(2) * c2);
+        const T a5 = (dp + rt * ct * dun) / (T(2) * c2);
+        const T a2 = dr - dp / c2;
+        const T w1 = l1 * a1, w5 = l5 * a5, w2 = l2 * a2;
+        T D[5];
+        D[0] = w1 + w5 + w2;
+        T uds = T(0);
+        #pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const T sh = du[i] - dun * n[i];
+            D[1 + i] = w1 * (ut[i] - ct * n[i]) + w5 * (ut[i] + ct * n[i]) + w2 * ut[i] + l2 * rt * sh;
+            uds += ut[i] * sh;
+        }
+        D[4] = w1 * (Ht - ct * unt) + w5 * (Ht + ct * unt) + w2 * T(0.5) * q2 + l2 * rt * uds;
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) Fh[k] = T(0.5) * (FL[k] + FR[k]) - T(0.5) * D[k];
+    }
+};
+
+}  // namespace fvedg

@@ -1,0 +1,210 @@
+// FP64 kernels of the explicit DG operator (the plain form).
+//
+// One RK stage is two launches:
+//   face_flux_fp64   one thread per (face, face point): two-sided trace through the face-map
+//                    tables, numerical flux, times w_g * 2A; writes Fh[face][g][5].
+//                    Replaces eval_internals + eval_boundarys' point loop
+//                    (ExplicitConvection.cpp:21-128, 201-272) minus the scatter.
+//   element_fp64     a CTA owns E elements: volume integral (eval_cells, :144-198) plus an
+//                    element-owned gather of its four faces' Fh (the atomic-free replacement of
+//                    the reference's omp atomic scatter), then either stores R or applies the
+//                    inverse diagonal mass and the SSP-RK3 stage combination in place.
+#pragma once
+#include <cstdint>
+
+#include "dg_flux.cuh"
+
+namespace fvedg {
+
+struct FaceInfo {     // 48 bytes
+    double n[3];      // unit normal out of cells[0]
+    double jw;        // 2A (the face Jacobian of CompTriangleFace::compute_jacobian_det)
+    int c0, c1;       // c1 < 0: boundary face
+    int meta;         // perm0 | perm1 << 8 | bc << 16 | flags << 24 (bit 0: periodic)
+    int pad;
+};
+
+struct ElemFace {     // one of the four faces of an element
+    int face;         // face id
+    int meta;         // perm | side << 8
+};
+
+struct StageArgs {
+    const double* U;      // stage input state [ncell][5*NB]
+    const double* U0;     // U^n (RK base), may alias U
+    double* out;          // R (residual mode) or the new stage state
+    const double* Fh;     // [nface][nqf][5]
+    const double* geo;    // [ncell][10]: invJ (9, row-major) then detJ
+    const ElemFace* ef;   // [ncell][4]
+    const double* phi_v;  // [nqv][NB]
+    const double* dphi_vw;// [nqv][NB][3]
+    const double* phi_f;  // [24][nqf][NB]
+    const double* mass_ref; // [NB]
+    int ncell, nqv, nqf;
+    double gamma;
+    double dt, a0, a1;    // out = a0 * U0 + a1 * (U + dt * (-R / b))
+    int mode;             // 0 = store R, 1 = RK stage
+    int with_volume;      // 0 skips the volume term (eval_internals / eval_boundarys only)
+};
+
+struct FaceArgs {
+    const double* U;
+    const FaceInfo* fi;
+    const double* phi_f;  // [24][nqf][NB]
+    const double* w_f;    // [nqf]
+    const double* UD;     // Dirichlet data [nface][nqf][5] or nullptr
+    double* Fh;
+    int nface, nqf;
+    double gamma;
+    int flux;             // 0 = LF, 1 = Roe
+    int faces_mask;       // bit 0: interior faces, bit 1: boundary faces
+};
+
+template <int NB>
+__global__ void __launch_bounds__(256) face_flux_fp64(FaceArgs a) {
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t total = (int64_t)a.nface * a.nqf;
+    if (tid >= total) return;
+    const int f = (int)(tid / a.nqf);
+    const int g = (int)(tid - (int64_t)f * a.nqf);
+    const FaceInfo fi = a.fi[f];
+    const int p0 = fi.meta & 0xff, p1 = (fi.meta >> 8) & 0xff, bc = (fi.meta >> 16) & 0xff;
+    const bool interior = fi.c1 >= 0;
+    double* out = a.Fh + ((int64_t)f * a.nqf + g) * 5;
+    const bool active = interior ? (a.faces_mask & 1)
+                                 : ((a.faces_mask & 2) && ((bc == 0 && a.UD != nullptr) || bc == 5));
+    if (!active) {
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) out[k] = 0.0;
+        return;
+    }
+    const double* phL = a.phi_f + ((int64_t)p0 * a.nqf + g) * NB;
+    const double* cL = a.U + (int64_t)fi.c0 * (5 * NB);
+    double UL[5] = {0, 0, 0, 0, 0}, UR[5] = {0, 0, 0, 0, 0};
+    #pragma unroll 5
+    for (int b = 0; b < NB; ++b) {
+        const double ph = __ldg(phL + b);
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) UL[k] = fma(ph, __ldg(cL + 5 * b + k), UL[k]);
+    }
+    if (interior) {
+        const double* phR = a.phi_f + ((int64_t)p1 * a.nqf + g) * NB;
+        const double* cR = a.U + (int64_t)fi.c1 * (5 * NB);
+        #pragma unroll 5
+        for (int b = 0; b < NB; ++b) {
+            const double ph = __ldg(phR + b);
+            #pragma unroll
+            for (int k = 0; k < 5; ++k) UR[k] = fma(ph, __ldg(cR + 5 * b + k), UR[k]);
+        }
+    } else if (bc == 0) {  // Dirichlet ghost 2 U_D - U_in (ExplicitConvection.cpp:53)
+        const double* ud = a.UD + ((int64_t)f * a.nqf + g) * 5;
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) UR[k] = ud[k] + (ud[k] - UL[k]);
+    } else {               // Pseudo3DZ mirror (:92)
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) UR[k] = UL[k];
+        UR[3] = -UL[3];
+    }
+    double Fh[5];
+    if (a.flux == 1) Phys<double>::roe(UL, UR, fi.n, a.gamma, Fh);
+    else Phys<double>::lax_friedrichs(UL, UR, fi.n, a.gamma, Fh);
+    const double jw = __ldg(a.w_f + g) * fi.jw;
+    #pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = Fh[k] * jw;
+}
+
+// E elements per CTA; dynamic shared memory holds the stage state of the tile and the
+// flux-times-inverse-Jacobian values G at every volume point.
+template <int NB, int E>
+__global__ void __launch_bounds__(256) element_fp64(StageArgs a) {
+    extern __shared__ double smem[];
+    double* sC = smem;                      // [E][5*NB]
+    double* sG = smem + E * 5 * NB;         // [E][nqv][15]
+    const int e0 = blockIdx.x * E;
+    const int ne = min(E, a.ncell - e0);
+    const int nqv = a.nqv;
+    // stage the tile's coefficients (contiguous, coalesced)
+    {
+        const double* src = a.U + (int64_t)e0 * (5 * NB);
+        const int n = ne * 5 * NB;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) sC[i] = src[i];
+    }
+    __syncthreads();
+    if (a.with_volume) {
+        // phase 1: (element, volume point) -> G = detJ * F(U(x_g)) . J^{-T}
+        for (int it = threadIdx.x; it < ne * nqv; it += blockDim.x) {
+            const int e = it / nqv, g = it - e * nqv;
+            const double* c = sC + e * 5 * NB;
+            const double* ph = a.phi_v + g * NB;
+            double U[5] = {0, 0, 0, 0, 0};
+            #pragma unroll 5
+            for (int b = 0; b < NB; ++b) {
+                const double p = __ldg(ph + b);
+                #pragma unroll
+                for (int k = 0; k < 5; ++k) U[k] = fma(p, c[5 * b + k], U[k]);
+            }
+            double F[5][3];
+            Phys<double>::flux(U, a.gamma - 1.0, F);
+            const double* geo = a.geo + (int64_t)(e0 + e) * 10;
+            double J[9];
+            #pragma unroll
+            for (int i = 0; i < 9; ++i) J[i] = __ldg(geo + i);
+            const double dj = __ldg(geo + 9);
+            double* G = sG + (e * nqv + g) * 15;
+            #pragma unroll
+            for (int k = 0; k < 5; ++k)
+                #pragma unroll
+                for (int cdir = 0; cdir < 3; ++cdir)
+                    G[3 * k + cdir] = dj * (F[k][0] * J[0 * 3 + cdir] + F[k][1] * J[1 * 3 + cdir] + F[k][2] * J[2 * 3 + cdir]);
+        }
+        __syncthreads();
+    }
+    // phase 2: (element, basis function j)
+    for (int it = threadIdx.x; it < ne * NB; it += blockDim.x) {
+        const int e = it / NB, j = it - e * NB;
+        const int ge = e0 + e;
+        double acc[5] = {0, 0, 0, 0, 0};
+        if (a.with_volume) {
+            const double* G = sG + e * nqv * 15;
+            for (int g = 0; g < nqv; ++g) {
+                const double* d = a.dphi_vw + (g * NB + j) * 3;
+                const double d0 = __ldg(d), d1 = __ldg(d + 1), d2 = __ldg(d + 2);
+                const double* Gg = G + g * 15;
+                #pragma unroll
+                for (int k = 0; k < 5; ++k) acc[k] -= Gg[3 * k] * d0 + Gg[3 * k + 1] * d1 + Gg[3 * k + 2] * d2;
+            }
+        }
+        #pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const ElemFace ef = a.ef[(int64_t)ge * 4 + q];
+            const int perm = ef.meta & 0xff;
+            const double sgn = (ef.meta >> 8) ? -1.0 : 1.0;
+            const double* F = a.Fh + (int64_t)ef.face * a.nqf * 5;
+            const double* ph = a.phi_f + (int64_t)perm * a.nqf * NB + j;
+            double s[5] = {0, 0, 0, 0, 0};
+            for (int g = 0; g < a.nqf; ++g) {
+                const double p = __ldg(ph + g * NB);
+                #pragma unroll
+                for (int k = 0; k < 5; ++k) s[k] = fma(p, __ldg(F + 5 * g + k), s[k]);
+            }
+            #pragma unroll
+            for (int k = 0; k < 5; ++k) acc[k] = fma(sgn, s[k], acc[k]);
+        }
+        double* o = a.out + (int64_t)ge * 5 * NB + 5 * j;
+        if (a.mode == 0) {
+            #pragma unroll
+            for (int k = 0; k < 5; ++k) o[k] = acc[k];
+        } else {
+            const double ib = 1.0 / (__ldg(a.geo + (int64_t)ge * 10 + 9) * __ldg(a.mass_ref + j));
+            const double* u0 = a.U0 + (int64_t)ge * 5 * NB + 5 * j;
+            const double* us = sC + e * 5 * NB + 5 * j;
+            #pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                const double L = -acc[k] * ib;
+                o[k] = a.a0 * u0[k] + a.a1 * (us[k] + a.dt * L);
+            }
+        }
+    }
+}
+
+}  // namespace fvedg

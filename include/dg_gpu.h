@@ -1,0 +1,193 @@
+/* dg_gpu.h — C ABI of the B200 explicit DG operator for the 3D compressible Euler equations on
+ * affine tetrahedra (modal basis P1..P4, Lax-Friedrichs or Roe flux, SSP-RK3).
+ *
+ * It replaces the reference's explicit convection path:
+ *   ExplicitConvection<Order, Flux, QuadC, QuadF>::eval(mesh, U, t)
+ *       include/DG/DG_Schemes/ExplicitConvection.h:31-33, src/DG/DG_Schemes/ExplicitConvection.cpp:136-141
+ *   its parts eval_cells / eval_internals / eval_boundarys   ExplicitConvection.h:34-44
+ *   the drivers' explicit time loop  U += dt * (-(1/b) * eval(U))   examples/Vortex/123/VortexRK.cpp:264-271
+ *   the drivers' diagonal mass b     examples/Eular1D/Sod1D/Riemann1D.cpp:108-121
+ *
+ * Conventions shared with the reference:
+ *   - state and residual: element-major, basis-major, variable-minor, coef[e][5*b + k] with
+ *     k in {rho, rho u, rho v, rho w, rho E} (include/Matrix/LongVector.h:10). Host buffers may
+ *     have a padded element stride (LongVector pads each block to 32 bytes, DenseMatrix.h:15):
+ *     pass it as elem_stride_bytes, or 0 for the packed 5*Nb*8 bytes.
+ *   - residual sign and scaling are those of ExplicitConvection::eval: no mass inverse, no dt.
+ *   - face_cells[f][1] == DG_NO_CELL marks a boundary face (uInt(-1) in ComputingMesh.h:21).
+ *
+ * All entry points return DG_OK (0) or a negative DG_E* code; nothing throws across the ABI.
+ * A dg_ctx owns its device buffers; host pointers are borrowed for the duration of a call.
+ * A dg_ctx is not safe for concurrent use from several host threads.
+ */
+#ifndef FVEDG_DG_GPU_H
+#define FVEDG_DG_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DG_NO_CELL (-1)
+
+enum dg_status {
+    DG_OK = 0,
+    DG_E_ARG = -1,        /* bad argument (null pointer, unsupported order or rule, ...) */
+    DG_E_MESH = -2,       /* malformed mesh: bad index, face/cell mismatch, bad face map */
+    DG_E_CUDA = -3,       /* a CUDA runtime call failed */
+    DG_E_NOMEM = -4,      /* device or host allocation failed */
+    DG_E_NONPHYSICAL = -5,/* the state has NaN/Inf or non-positive density or pressure */
+    DG_E_WATCHDOG = -6,   /* a bounded device wait ran out (batched persistent form) */
+    DG_E_STATE = -7       /* call out of order (e.g. stepping before a state was set) */
+};
+
+enum dg_flux_kind { DG_FLUX_LF = 0, DG_FLUX_ROE = 1 };
+enum dg_precision { DG_PREC_FP64 = 0, DG_PREC_MIXED = 1 };
+
+/* BoundaryType of include/Mesh/ComputingMesh.h:71-86. eval_boundarys acts on Dirichlet and
+ * Pseudo3DZ only; every other type contributes nothing (ExplicitConvection.cpp:47-125). */
+enum dg_boundary {
+    DG_BC_DIRICHLET = 0, DG_BC_NEUMANN = 1, DG_BC_ROBIN = 2, DG_BC_PSEUDO3DX = 3,
+    DG_BC_PSEUDO3DY = 4, DG_BC_PSEUDO3DZ = 5, DG_BC_INFLOW = 6, DG_BC_OUTFLOW = 7,
+    DG_BC_WALL = 8, DG_BC_WALLTD = 9, DG_BC_WALLTN = 10, DG_BC_WALLTR = 11
+};
+
+/* Quadrature rule ids. -1 selects the reference's AutoQuadSelector choice for the order
+ * (include/GaussQuadrature/AutoQuadSelectorTet.h:2-50, AutoQuadSelectorTri.h:1-45). */
+enum dg_tet_rule {
+    DG_TET_D2P4 = 0, DG_TET_D4P11 = 1, DG_TET_D5P15 = 2, DG_TET_D6P23 = 3,
+    DG_TET_D7P31 = 4, DG_TET_D8P44 = 5, DG_TET_D9P57 = 6
+};
+enum dg_tri_rule { DG_TRI_D3P4 = 0, DG_TRI_D3P6 = 1, DG_TRI_D4P7 = 2, DG_TRI_D10P24 = 3 };
+
+/* Flattened mesh. Topology follows DGMesh (include/Mesh/MeshGenerator.h:46-57) and
+ * ComputingMesh(const DGMesh&) (src/Mesh/ComputingMesh.cpp:268-298); geometry follows
+ * CompTetrahedron / CompTriangleFace (ComputingMesh.cpp:27-171).
+ *
+ * Two ways to describe it:
+ *  (a) from a reference ComputingMesh: give face_cells, face_natural, face_normal, face_area,
+ *      cell_invjac and cell_detj exactly as the reference holds them (m_neighbor_cells,
+ *      m_natural_coords, m_normal, m_area, m_invJac, compute_jacobian_det());
+ *  (b) from raw topology: leave the geometry pointers NULL and give points, cell_nodes,
+ *      face_nodes (and, for periodic faces, face_nodes1 + face_periodic). The library then
+ *      computes the geometry with the reference's formulas, bit for bit. */
+typedef struct dg_mesh_desc {
+    int64_t ncell;
+    int64_t nface;
+    const int64_t* face_cells;   /* [nface][2]; [f][1] = DG_NO_CELL on a boundary face        */
+    const uint8_t* face_bc;      /* [nface] dg_boundary for boundary faces; NULL = Pseudo3DZ   */
+    /* (a) geometry as held by a reference ComputingMesh (all or none) */
+    const double* face_natural;  /* [nface][2][3][3] m_natural_coords                          */
+    const double* face_normal;   /* [nface][3] unit normal out of cells[0]                     */
+    const double* face_area;     /* [nface]                                                    */
+    const double* cell_invjac;   /* [ncell][9] row-major inverse of rows {p1-p0,p2-p0,p3-p0}   */
+    const double* cell_detj;     /* [ncell] 6 |V|                                              */
+    /* (b) raw topology */
+    int64_t npts;
+    const double* points;        /* [npts][3]                                                  */
+    const int64_t* cell_nodes;   /* [ncell][4]                                                 */
+    const int64_t* face_nodes;   /* [nface][3] (face node order defines the face parameters)   */
+    const int64_t* face_nodes1;  /* [nface][3] the face's nodes as numbered in cells[1]; NULL = face_nodes */
+    const uint8_t* face_periodic;/* [nface] 1 = periodic pair (normal by the boundary rule); NULL = none */
+} dg_mesh_desc;
+
+typedef struct dg_config {
+    int order;       /* 1..4 */
+    int flux;        /* dg_flux_kind */
+    int quad_vol;    /* dg_tet_rule or -1 */
+    int quad_face;   /* dg_tri_rule or -1 */
+    double gamma;    /* 1.4 (AirFluxC) or 5/3 (MonatomicFluxC), any value > 1 accepted */
+    int precision;   /* dg_precision */
+    int device;      /* CUDA device ordinal */
+} dg_config;
+
+typedef struct dg_ctx dg_ctx;
+
+/* Create a context: validates and uploads the mesh, builds basis/face tables and the diagonal
+ * mass. Replaces constructing ExplicitConvection<...> plus the driver's mass loop. */
+dg_ctx* dg_create(const dg_mesh_desc* mesh, const dg_config* cfg, int* err);
+void dg_destroy(dg_ctx* ctx);
+
+/* Residual R(U) with the sign and scaling of ExplicitConvection::eval (ExplicitConvection.cpp:136-141),
+ * host buffers in, host buffer out. part: 0 = eval, 1 = eval_cells, 2 = eval_internals,
+ * 3 = eval_boundarys. */
+int dg_residual(dg_ctx* ctx, const double* U, double* R, size_t elem_stride_bytes, double t, int part);
+
+/* Same on device buffers (packed layout), enqueued on `stream` (a cudaStream_t, NULL = default). */
+int dg_residual_device(dg_ctx* ctx, const double* U_dev, double* R_dev, double t, int part, void* stream);
+
+/* Device-resident time stepping (the driver loop of VortexRK.cpp:264-271 with SSP-RK3). */
+int dg_set_state(dg_ctx* ctx, const double* U, size_t elem_stride_bytes);
+int dg_get_state(dg_ctx* ctx, double* U, size_t elem_stride_bytes);
+int dg_ssprk3(dg_ctx* ctx, double dt, int nsteps);
+/* Capture one SSP-RK3 step in a CUDA graph and replay it nsteps times. */
+int dg_ssprk3_graph(dg_ctx* ctx, double dt, int nsteps);
+
+/* Diagonal mass b[e][5i+k] = detJ * sum_g w_g phi_i(x_g)^2 (Riemann1D.cpp:108-121). */
+int dg_mass(dg_ctx* ctx, double* mass, size_t elem_stride_bytes);
+
+/* Boundary data: U_D at every face point of every Dirichlet face, [nface][nqf][5] indexed by face
+ * id (entries of other faces are ignored). Stands in for the rho_Xi .. rhoe_Xi hooks of
+ * include/base/exact.h:32-52 evaluated at the face points (ExplicitConvection.cpp:47-53). */
+int dg_set_dirichlet(dg_ctx* ctx, const double* UD);
+
+/* Conservation sums of the device state (new; the reference drivers have none):
+ * out[0..4] = integrals of rho, rho u, rho v, rho w, rho E; out[5] = integral of rho|u|^2/2. */
+int dg_conservation(dg_ctx* ctx, double out[6]);
+
+/* Largest LF wave speed |u| + c over the volume points of the device state (for a CFL dt). */
+int dg_max_wave_speed(dg_ctx* ctx, double* lam);
+
+/* Non-physical-state check of the device state: returns DG_OK or DG_E_NONPHYSICAL and writes the
+ * number of offending volume points. */
+int dg_check_state(dg_ctx* ctx, int64_t* bad_points);
+
+/* Sizes and the rules actually used. */
+int dg_info(const dg_ctx* ctx, int* num_basis, int* nq_vol, int* nq_face, int* quad_vol, int* quad_face);
+
+/* Geometry exactly as the reference's ComputingMesh computes it from raw topology (form (b) of
+ * dg_mesh_desc): unit normals, areas, natural coordinates [nface][2][3][3], J^{-T} [ncell][9],
+ * detJ, centroids. Host-only; no device needed. */
+int dg_mesh_geometry(const dg_mesh_desc* mesh, double* normal, double* area, double* natural,
+                     double* invjac, double* detj, double* centroid);
+
+/* Face maps: for every face and side the code 0..23 of the ordered vertex triple
+ * (slot of face node 0, 1, 2 in the cell), derived from the natural coordinates; -1 for the
+ * missing side of a boundary face. Host-only. */
+int dg_face_perms(const dg_mesh_desc* mesh, int8_t* perm);
+
+/* Basis values [npts][Nb] and reference gradients [npts][Nb][3] at reference-tet points
+ * (DGBasisEvaluator<P>::eval_all / grad_all, include/DG/DG_Basis/DG_Basis_Evaluator.h:14-31). */
+int dg_basis(int order, int npts, const double* xyz, double* phi, double* grad);
+/* Quadrature rule: kind 0 = tet (points [n][3]), 1 = triangle (points [n][2]); weights [n].
+ * Returns the number of points (either output may be NULL), or DG_E_ARG. */
+int dg_quad_rule(int kind, int id, double* pts, double* w);
+/* The reference's AutoQuadSelector choices for an order. */
+int dg_auto_rules(int order, int* quad_vol, int* quad_face);
+
+const char* dg_status_string(int status);
+
+/* Device name of the active context's GPU and the number of CUDA kernel launches issued by this
+ * library since load (for launch accounting in benchmarks). */
+int64_t dg_launch_count(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Periodic box mesh generator (new: the reference's split_hex6_scan is not periodic-conforming).
+ * n^3 cubes on [lo,hi]^3, each cut into 6 tetrahedra around the main diagonal (Kuhn split, which
+ * is translation invariant), vertices strictly inside the box jittered by a seeded uniform
+ * +-jitter*h. Axes flagged periodic pair their boundary faces (face_cells[1] = partner cell,
+ * face_nodes1 = translated nodes, face_periodic = 1); other boundary faces get boundary type bc.
+ * Output arrays follow dg_mesh_desc form (b). */
+typedef struct dg_box_mesh dg_box_mesh;
+dg_box_mesh* dg_box_mesh_create(int n, const double lo[3], const double hi[3], double jitter,
+                                uint64_t seed, const int periodic[3], int bc, int* err);
+void dg_box_mesh_destroy(dg_box_mesh* m);
+/* Borrowed views valid until dg_box_mesh_destroy. */
+int dg_box_mesh_view(const dg_box_mesh* m, dg_mesh_desc* desc, const int64_t** cell_faces,
+                     const int64_t** cell_cells);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

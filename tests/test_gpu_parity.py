@@ -1,0 +1,174 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle and the reference itself."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import CASES, rel_l2
+from fve_dg_b200 import ExplicitConvection, box_mesh, problems
+from fve_dg_b200 import _lib as L
+from oracle.pyoracle import Oracle, RefLib, RefMesh, ref_available
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12  # relative L2, the FP64 parity bar
+
+
+def noisy_state(m, P, seed, amp=1e-2):
+    U = problems.project(m, P, problems.density_wave())
+    return U + amp * np.random.default_rng(seed).standard_normal(U.shape) * np.abs(U).max()
+
+
+@pytest.fixture(scope="module")
+def mesh3():
+    return box_mesh(3, jitter=0.1, seed=5)
+
+
+@pytest.mark.parametrize("P,qv,qf", CASES)
+def test_residual_matches_oracle(mesh3, P, qv, qf):
+    U = noisy_state(mesh3, P, P)
+    conv = ExplicitConvection(mesh3, order=P, quad_vol=qv, quad_face=qf)
+    R = conv.eval(U)
+    Ro = Oracle.from_mesh(mesh3).residual(U, P, qv, qf)
+    assert rel_l2(R, Ro) < TOL
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("P,qv,qf", CASES)
+def test_residual_matches_reference(mesh3, P, qv, qf):
+    U = noisy_state(mesh3, P, 10 + P)
+    ref = RefLib()
+    rm = RefMesh.from_mesh(ref, mesh3)
+    Rr = rm.eval(U, P, qv, qf)
+    conv = ExplicitConvection(mesh3, order=P, quad_vol=qv, quad_face=qf)
+    assert rel_l2(conv.eval(U), Rr) < TOL
+    # the same operator fed the reference's own ComputingMesh geometry (dg_mesh_desc form (a))
+    g = rm.export()
+    from fve_dg_b200 import Mesh
+    ma = Mesh(mesh3.points, mesh3.cells, mesh3.faces, mesh3.face_cells, mesh3.face_nodes1, mesh3.periodic,
+              mesh3.bc, geometry=dict(natural=g["natural"], normal=g["normal"], area=g["area"],
+                                      invjac=g["invjac"], detj=g["detj"]))
+    conv_a = ExplicitConvection(ma, order=P, quad_vol=qv, quad_face=qf)
+    assert rel_l2(conv_a.eval(U), Rr) < TOL
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+def test_parts_and_roe(mesh3, P):
+    qv, qf = problems.auto_rules(P)
+    U = noisy_state(mesh3, P, 20 + P)
+    o = Oracle.from_mesh(mesh3)
+    conv = ExplicitConvection(mesh3, order=P, quad_vol=qv, quad_face=qf)
+    assert rel_l2(conv.eval_cells(U), o.residual(U, P, qv, qf, part=1)) < TOL
+    assert rel_l2(conv.eval_internals(U), o.residual(U, P, qv, qf, part=2)) < TOL
+    assert np.abs(conv.eval_boundarys(U)).max() == 0.0  # periodic box: no boundary faces
+    roe = ExplicitConvection(mesh3, order=P, flux="Roe", quad_vol=qv, quad_face=qf)
+    assert rel_l2(roe.eval(U), o.residual(U, P, qv, qf, flux="Roe")) < TOL
+
+
+def face_points_physical(m, qf):
+    pts, _ = problems.quad_rule(1, qf)
+    P = m.points[m.faces]  # (nf, 3, 3)
+    lam = np.stack([1 - pts[:, 0] - pts[:, 1], pts[:, 0], pts[:, 1]], axis=1)
+    return np.einsum("ga,fad->fgd", lam, P)
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+def test_boundary_faces(P):
+    """Non-periodic box: Dirichlet on all sides, then Pseudo3DZ, against oracle and reference."""
+    qv, qf = problems.auto_rules(P)
+    prm = np.array([1.0, 0.2, 1.0, 1.0, 1.0, 1.0, 0.5, 0.25, 1.0, 1.4])
+    for bc in ("Dirichlet", "Pseudo3DZ", "Wall"):
+        m = box_mesh(2, jitter=0.1, seed=3, periodic=(0, 0, 0), bc=bc)
+        U = noisy_state(m, P, 30 + P, amp=1e-3)
+        conv = ExplicitConvection(m, order=P, quad_vol=qv, quad_face=qf)
+        if bc == "Dirichlet":
+            X = face_points_physical(m, qf)
+            UD = problems.density_wave(A=prm[1], vel=tuple(prm[5:8]))(X)
+            conv.set_dirichlet(UD)
+        R = conv.eval(U)
+        Ro = Oracle.from_mesh(m).residual(U, P, qv, qf, dirichlet=prm)
+        assert rel_l2(R, Ro) < TOL, bc
+        if ref_available():
+            ref = RefLib()
+            ref.set_dirichlet(prm)
+            Rr = RefMesh.from_mesh(ref, m).eval(U, P, qv, qf)
+            assert rel_l2(R, Rr) < TOL, bc
+
+
+@pytest.mark.parametrize("P", [1, 3])
+def test_ssprk3_matches_oracle_and_graph(mesh3, P):
+    qv, qf = problems.auto_rules(P)
+    U0 = noisy_state(mesh3, P, 40 + P, amp=1e-3)
+    dt, n = 2e-3, 3
+    conv = ExplicitConvection(mesh3, order=P, quad_vol=qv, quad_face=qf)
+    conv.set_state(U0)
+    conv.ssprk3(dt, n)
+    Ug = conv.get_state()
+    Uo = Oracle.from_mesh(mesh3).ssprk3(U0, P, qv, qf, dt, n)
+    assert rel_l2(Ug, Uo) < TOL
+    conv.set_state(U0)
+    conv.ssprk3(dt, n, graph=True)
+    assert np.array_equal(conv.get_state(), Ug)  # the graph replays the same kernels
+    if ref_available():
+        ref = RefLib()
+        rm = RefMesh.from_mesh(ref, mesh3)
+        Ur = rm.ssprk3(U0, rm.mass(P, qv), P, qv, qf, dt, n)
+        assert rel_l2(Ug, Ur) < TOL
+
+
+def test_determinism_and_free_stream():
+    m = box_mesh(4, jitter=0.1, seed=9)
+    for P in (1, 2, 3, 4):
+        conv = ExplicitConvection(m, order=P)
+        U = noisy_state(m, P, 50 + P)
+        assert np.array_equal(conv.eval(U), conv.eval(U))  # no atomics: bitwise repeatable
+        Uc = problems.project(m, P, lambda X: problems.conserved(
+            np.ones(X.shape[:-1]), 0.3 + 0 * X[..., 0], -0.2 + 0 * X[..., 0], 0.1 + 0 * X[..., 0],
+            np.ones(X.shape[:-1]), 1.4))
+        R = conv.eval(Uc)
+        assert np.abs(R).max() < 1e-12 * 10  # free stream preserved on a periodic mesh
+
+
+def test_mass_conservation_and_sums(mesh3):
+    P = 2
+    qv, qf = problems.auto_rules(P)
+    U0 = noisy_state(mesh3, P, 60, amp=1e-3)
+    conv = ExplicitConvection(mesh3, order=P)
+    conv.set_state(U0)
+    c0 = conv.conservation()
+    co = Oracle.from_mesh(mesh3).conservation(U0, P, qv)
+    assert np.allclose(c0, co, rtol=1e-12, atol=1e-14)
+    conv.ssprk3(2e-3, 5)
+    c1 = conv.conservation()
+    assert np.all(np.abs(c1[:5] - c0[:5]) <= 1e-12 * np.maximum(1.0, np.abs(c0[:5])))
+    assert conv.check_state() == 0
+    assert conv.max_wave_speed() > 0
+
+
+def test_padded_stride_via_c_abi(mesh3):
+    """The reference pads each LongVector block to 32 bytes (P2: 400 -> 416 B)."""
+    P = 2
+    conv = ExplicitConvection(mesh3, order=P)
+    U = noisy_state(mesh3, P, 70)
+    nb5 = U.shape[1]
+    stride = 416
+    Up = np.zeros((mesh3.ncell, stride // 8))
+    Up[:, :nb5] = U
+    Rp = np.full_like(Up, 7.0)
+    L.check(L.lib().dg_residual(conv._ctx, L.dptr(Up), L.dptr(Rp), stride, 0.0, 0), "dg_residual")
+    assert np.array_equal(Rp[:, :nb5], conv.eval(U))
+    assert np.all(Rp[:, nb5:] == 7.0)  # padding untouched
+
+
+def test_errors_are_reported():
+    m = box_mesh(2)
+    with pytest.raises(L.DGError):
+        ExplicitConvection(m, order=7)
+    conv = ExplicitConvection(m, order=1)
+    with pytest.raises(L.DGError):
+        conv.get_state()  # no state set yet
+    bad = problems.project(m, 1, problems.density_wave())
+    bad[0, 0] = -1.0  # negative density mode
+    bad[1, :] = np.nan
+    conv.set_state(bad)
+    assert conv.check_state() > 0
