@@ -63,6 +63,8 @@ def lib():
         "dg_ssprk3": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
         "dg_ssprk3_graph": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
         "dg_mass": (ctypes.c_int, [vp, c_double_p, ctypes.c_size_t]),
+        "dg_ssprk3_timed": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int, c_double_p, ctypes.c_int]),
+        "dg_stream": (vp, [vp]),
         "dg_set_dirichlet": (ctypes.c_int, [vp, c_double_p]),
         "dg_conservation": (ctypes.c_int, [vp, c_double_p]),
         "dg_max_wave_speed": (ctypes.c_int, [vp, c_double_p]),
@@ -93,7 +95,7 @@ def lib():
 def exported_symbols():
     """Names this binding expects the library to export."""
     return ["dg_create", "dg_destroy", "dg_residual", "dg_residual_device", "dg_set_state", "dg_get_state",
-            "dg_ssprk3", "dg_ssprk3_graph", "dg_mass", "dg_set_dirichlet", "dg_conservation",
+            "dg_ssprk3", "dg_ssprk3_graph", "dg_ssprk3_timed", "dg_stream", "dg_mass", "dg_set_dirichlet", "dg_conservation",
             "dg_max_wave_speed", "dg_check_state", "dg_info", "dg_mesh_geometry", "dg_face_perms", "dg_basis",
             "dg_quad_rule", "dg_auto_rules", "dg_status_string", "dg_launch_count", "dg_box_mesh_create",
             "dg_box_mesh_destroy", "dg_box_mesh_view"]

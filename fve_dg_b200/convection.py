@@ -111,6 +111,17 @@ class ExplicitConvection:
         f = L.lib().dg_ssprk3_graph if graph else L.lib().dg_ssprk3
         L.check(f(self._ctx, float(dt), int(nsteps)), "dg_ssprk3")
 
+    def ssprk3_timed(self, dt, nsteps, nclass=4):
+        """Step with CUDA events around every launch; returns {class: (total_ms, launches)}."""
+        out = np.zeros(2 * nclass)
+        L.check(L.lib().dg_ssprk3_timed(self._ctx, float(dt), int(nsteps), L.dptr(out), nclass), "dg_ssprk3_timed")
+        return {k: (out[2 * k], int(out[2 * k + 1])) for k in range(nclass) if out[2 * k + 1] > 0}
+
+    @property
+    def stream(self):
+        """Raw cudaStream_t of the context (wrap with torch.cuda.ExternalStream to time on it)."""
+        return L.lib().dg_stream(self._ctx)
+
     def conservation(self):
         out = np.zeros(6)
         L.check(L.lib().dg_conservation(self._ctx, L.dptr(out)), "dg_conservation")

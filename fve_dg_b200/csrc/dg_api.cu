@@ -54,6 +54,8 @@ struct dg_ctx {
     double* d_dphi_vw = nullptr;
     double* d_w_v = nullptr;
     double* d_phi_f = nullptr;
+    double* d_phi_fT = nullptr;
+    double* d_phi_vT = nullptr;
     double* d_w_f = nullptr;
     double* d_mass_ref = nullptr;
     double* d_UD = nullptr;        // Dirichlet data
@@ -70,6 +72,11 @@ struct dg_ctx {
     bool has_dirichlet = false;    // some boundary face is Dirichlet: U_D must be set first
     cudaGraphExec_t graph = nullptr;
     double graph_dt = 0.0;
+    // optional per-launch event timing (dg_ssprk3_timed)
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> ev_cls;
+    size_t ev_used = 0;
 };
 
 namespace {
@@ -100,7 +107,51 @@ int launch_face(const FaceArgs& a, cudaStream_t s) {
     return cuda_ok(cudaGetLastError());
 }
 
-int dispatch_face(int order, const FaceArgs& a, cudaStream_t s) {
+// Fixed-size kernels for the (order, tet rule, tri rule) combinations in common use; any other
+// combination runs the runtime-size kernels above.
+template <int NB, int NQV, int NQF, int E, int NT>
+int launch_element_fixed(const StageArgs& a, cudaStream_t s) {
+    constexpr size_t smem = element_fixed_smem<NB, NQV, NQF, E>();
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(element_fp64_fixed<NB, NQV, NQF, E, NT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return DG_E_CUDA;
+        attr = true;
+    }
+    const int grid = (a.ncell + E - 1) / E;
+    element_fp64_fixed<NB, NQV, NQF, E, NT><<<grid, NT, smem, s>>>(a);
+    ++g_launches;
+    return cuda_ok(cudaGetLastError());
+}
+
+template <int NB, int NQF, int FT>
+int launch_face_fixed(const FaceArgs& a, cudaStream_t s) {
+    const int grid = (a.nface + FT - 1) / FT;
+    face_flux_fp64_fixed<NB, NQF, FT><<<grid, FT * NQF, 0, s>>>(a);
+    ++g_launches;
+    return cuda_ok(cudaGetLastError());
+}
+
+// X(order, qv, qf, NB, NQV, NQF, E, NT, FT)
+#define FVEDG_FIXED_COMBOS(X)                    \
+    X(1, 0, 1, 4, 4, 6, 16, 128, 32)             \
+    X(1, 0, 0, 4, 4, 4, 16, 128, 32)             \
+    X(1, 0, 2, 4, 4, 7, 16, 128, 32)             \
+    X(1, 2, 2, 4, 15, 7, 16, 128, 32)            \
+    X(2, 1, 2, 10, 11, 7, 16, 256, 32)           \
+    X(2, 1, 3, 10, 11, 24, 8, 128, 8)            \
+    X(2, 2, 3, 10, 15, 24, 8, 128, 8)            \
+    X(3, 3, 3, 20, 23, 24, 8, 192, 8)            \
+    X(3, 4, 3, 20, 31, 24, 8, 192, 8)            \
+    X(4, 5, 3, 35, 44, 24, 4, 192, 8)            \
+    X(4, 6, 3, 35, 57, 24, 4, 192, 8)
+
+int dispatch_face(int order, int qv, int qf, const FaceArgs& a, cudaStream_t s) {
+#define X(P, QV, QF, NB, NQV, NQF, E, NT, FT) \
+    if (order == P && qv == QV && qf == QF) return launch_face_fixed<NB, NQF, FT>(a, s);
+    FVEDG_FIXED_COMBOS(X)
+#undef X
     switch (order) {
         case 1: return launch_face<4>(a, s);
         case 2: return launch_face<10>(a, s);
@@ -109,7 +160,11 @@ int dispatch_face(int order, const FaceArgs& a, cudaStream_t s) {
     }
     return DG_E_ARG;
 }
-int dispatch_element(int order, const StageArgs& a, cudaStream_t s) {
+int dispatch_element(int order, int qv, int qf, const StageArgs& a, cudaStream_t s) {
+#define X(P, QV, QF, NB, NQV, NQF, E, NT, FT) \
+    if (order == P && qv == QV && qf == QF) return launch_element_fixed<NB, NQV, NQF, E, NT>(a, s);
+    FVEDG_FIXED_COMBOS(X)
+#undef X
     switch (order) {
         case 1: return launch_element<4, 32>(a, s);
         case 2: return launch_element<10, 16>(a, s);
@@ -123,7 +178,7 @@ FaceArgs face_args(dg_ctx* c, const double* U, int mask) {
     FaceArgs a;
     a.U = U;
     a.fi = c->d_fi;
-    a.phi_f = c->d_phi_f;
+    a.phi_fT = c->d_phi_fT;
     a.w_f = c->d_w_f;
     a.UD = c->d_UD;
     a.Fh = c->d_Fh;
@@ -144,7 +199,7 @@ StageArgs stage_args(dg_ctx* c, const double* U, const double* U0, double* out, 
     a.Fh = c->d_Fh;
     a.geo = c->d_geo;
     a.ef = c->d_ef;
-    a.phi_v = c->d_phi_v;
+    a.phi_vT = c->d_phi_vT;
     a.dphi_vw = c->d_dphi_vw;
     a.phi_f = c->d_phi_f;
     a.mass_ref = c->d_mass_ref;
@@ -165,9 +220,30 @@ int residual_fp64(dg_ctx* c, const double* U, double* R, int part, cudaStream_t 
     if (c->cfg.flux != DG_FLUX_LF && c->cfg.flux != DG_FLUX_ROE) return DG_E_ARG;
     if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
     const int mask = part == 0 ? 3 : part == 1 ? 0 : part == 2 ? 1 : 2;
-    int rc = dispatch_face(c->cfg.order, face_args(c, U, mask), s);
+    int rc = dispatch_face(c->cfg.order, c->qv, c->qf, face_args(c, U, mask), s);
     if (rc) return rc;
-    return dispatch_element(c->cfg.order, stage_args(c, U, U, R, 0, 0.0, 0.0, 0.0, part == 0 || part == 1), s);
+    return dispatch_element(c->cfg.order, c->qv, c->qf, stage_args(c, U, U, R, 0, 0.0, 0.0, 0.0, part == 0 || part == 1), s);
+}
+
+// Launch `fn` (which enqueues one kernel on stream s), bracketed by timing events when enabled.
+template <class F>
+int timed(dg_ctx* c, int cls, cudaStream_t s, F&& fn) {
+    if (!c->timing) return fn();
+    if (c->ev_used + 2 > c->ev.size()) {
+        for (int i = 0; i < 64; ++i) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return DG_E_CUDA;
+            c->ev.push_back(e);
+        }
+        c->ev_cls.resize(c->ev.size() / 2);
+    }
+    const size_t i = c->ev_used;
+    if (cudaEventRecord(c->ev[i], s) != cudaSuccess) return DG_E_CUDA;
+    const int rc = fn();
+    if (cudaEventRecord(c->ev[i + 1], s) != cudaSuccess) return DG_E_CUDA;
+    c->ev_cls[i / 2] = cls;
+    c->ev_used += 2;
+    return rc;
 }
 
 // One SSP-RK3 step (Shu-Osher) on the device state, FP64 form:
@@ -178,9 +254,11 @@ int step_fp64(dg_ctx* c, double dt, cudaStream_t s) {
     const double* in[3] = {c->d_Un, c->d_Ua, c->d_Ub};
     double* out[3] = {c->d_Ua, c->d_Ub, c->d_Un};
     for (int st = 0; st < 3; ++st) {
-        int rc = dispatch_face(c->cfg.order, face_args(c, in[st], 3), s);
+        int rc = timed(c, 0, s, [&] { return dispatch_face(c->cfg.order, c->qv, c->qf, face_args(c, in[st], 3), s); });
         if (rc) return rc;
-        rc = dispatch_element(c->cfg.order, stage_args(c, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 1), s);
+        rc = timed(c, 1, s, [&] {
+            return dispatch_element(c->cfg.order, c->qv, c->qf, stage_args(c, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 1), s);
+        });
         if (rc) return rc;
     }
     return DG_OK;
@@ -188,7 +266,9 @@ int step_fp64(dg_ctx* c, double dt, cudaStream_t s) {
 
 int step(dg_ctx* c, double dt, cudaStream_t s) {
     if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
-    if (c->cfg.precision == DG_PREC_MIXED) return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches);
+    if (c->cfg.precision == DG_PREC_MIXED)
+        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches,
+                          [&](int cls, auto&& fn) { return timed(c, cls, s, fn); });
     return step_fp64(c, dt, s);
 }
 
@@ -211,7 +291,9 @@ int copy_out(dg_ctx* c, double* host, const double* dev, size_t stride, cudaStre
 void free_ctx(dg_ctx* c) {
     if (!c) return;
     if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
     void* ptrs[] = {c->d_geo, c->d_fi, c->d_ef, c->d_phi_v, c->d_dphi_vw, c->d_w_v, c->d_phi_f, c->d_w_f,
+                    c->d_phi_fT, c->d_phi_vT,
                     c->d_mass_ref, c->d_UD, c->d_Fh, c->d_Un, c->d_Ua, c->d_Ub, c->d_io, c->d_R,
                     c->d_red, c->d_red_out};
     for (void* p : ptrs)
@@ -300,13 +382,15 @@ dg_ctx* dg_create(const dg_mesh_desc* mesh, const dg_config* cfg, int* err) {
     if ((rc = upload(&c->d_geo, hgeo)) || (rc = upload(&c->d_fi, hfi)) || (rc = upload(&c->d_ef, hef)) ||
         (rc = upload(&c->d_phi_v, c->tab.phi_v)) || (rc = upload(&c->d_dphi_vw, c->tab.dphi_vw)) ||
         (rc = upload(&c->d_w_v, c->tab.w_v)) || (rc = upload(&c->d_phi_f, c->tab.phi_f)) ||
+        (rc = upload(&c->d_phi_fT, c->tab.phi_fT)) || (rc = upload(&c->d_phi_vT, c->tab.phi_vT)) ||
         (rc = upload(&c->d_w_f, c->tab.w_f)) || (rc = upload(&c->d_mass_ref, c->tab.mass_ref)) ||
         (rc = dev_alloc(&c->d_Fh, (size_t)c->nface * nqf * 5)) || (rc = dev_alloc(&c->d_Un, nstate)) ||
         (rc = dev_alloc(&c->d_Ua, nstate)) || (rc = dev_alloc(&c->d_Ub, nstate)) ||
         (rc = dev_alloc(&c->d_red, (size_t)kRedBlocks * 8)) || (rc = dev_alloc(&c->d_red_out, 8)))
         return fail(c, rc);
     if (cfg->precision == DG_PREC_MIXED) {
-        rc = init_mixed(c->mixed, c->tab, hgeo, hfi, hef, c->ncell, c->nface, cfg->gamma, cfg->flux);
+        rc = init_mixed(c->mixed, c->tab, hgeo, hfi, hef, c->ncell, c->nface, cfg->gamma, cfg->flux, qv, qf,
+                        c->d_geo, c->d_fi, c->d_ef, c->d_mass_ref);
         if (rc) return fail(c, rc);
     }
     if (err) *err = DG_OK;
@@ -403,6 +487,29 @@ int dg_ssprk3_graph(dg_ctx* c, double dt, int nsteps) {
         g_launches += per_step;
     }
     return cuda_ok(cudaStreamSynchronize(c->stream));
+}
+
+void* dg_stream(dg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int dg_ssprk3_timed(dg_ctx* c, double dt, int nsteps, double* out, int nclass) {
+    if (!c || nsteps < 0 || !(dt >= 0) || !out || nclass <= 0) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    c->timing = true;
+    c->ev_used = 0;
+    int rc = DG_OK;
+    for (int i = 0; i < nsteps && rc == DG_OK; ++i) rc = step(c, dt, c->stream);
+    c->timing = false;
+    if (rc) return rc;
+    DG_CUDA(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 2 * nclass; ++k) out[k] = 0.0;
+    for (size_t i = 0; i + 1 < c->ev_used; i += 2) {
+        float ms = 0.f;
+        DG_CUDA(cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]));
+        const int k = c->ev_cls[i / 2];
+        if (k < nclass) { out[2 * k] += ms; out[2 * k + 1] += 1.0; }
+    }
+    return DG_OK;
 }
 
 int dg_mass(dg_ctx* c, double* mass, size_t stride) {

@@ -44,9 +44,11 @@ int build_geometry(const dg_mesh_desc* d, Geometry* g);
 struct Tables {
     int order = 0, nb = 0, nqv = 0, nqf = 0;
     std::vector<double> phi_v;      // [nqv][nb]
+    std::vector<double> phi_vT;     // [nb][nqv]
     std::vector<double> dphi_vw;    // [nqv][nb][3] reference gradients times w_g
     std::vector<double> w_v;        // [nqv]
     std::vector<double> phi_f;      // [24][nqf][nb] face point basis values per face map
+    std::vector<double> phi_fT;     // [24][nb][nqf]
     std::vector<double> w_f;        // [nqf]
     std::vector<double> mass_ref;   // [nb] sum_g w_g phi_i(x_g)^2 on the reference tet
 };

@@ -112,6 +112,14 @@ void build_tables(int order, int qv, int qf, Tables* t) {
             basis_eval(order, xi[0], xi[1], xi[2], phi, nullptr);
             for (int b = 0; b < nb; ++b) t->phi_f[((size_t)p * nqf + g) * nb + b] = phi[b];
         }
+    t->phi_vT.assign(nb * nqv, 0.0);
+    for (int g = 0; g < nqv; ++g)
+        for (int b = 0; b < nb; ++b) t->phi_vT[b * nqv + g] = t->phi_v[g * nb + b];
+    t->phi_fT.assign(t->phi_f.size(), 0.0);
+    for (int p = 0; p < kNumPerms; ++p)
+        for (int g = 0; g < nqf; ++g)
+            for (int b = 0; b < nb; ++b)
+                t->phi_fT[((size_t)p * nb + b) * nqf + g] = t->phi_f[((size_t)p * nqf + g) * nb + b];
 }
 
 }  // namespace fvedg

@@ -126,8 +126,11 @@ def taylor_green(mach=0.1, gamma=1.4):
     return f
 
 
-def cfl_dt(cfl, h, order, lam_max):
-    """dt = CFL h / ((2P + 1) lambda_max), h the cube edge (cf. TGBatch.cpp:358-383)."""
+def cfl_dt(cfl, edge, order, lam_max):
+    """dt = CFL h / ((2P + 1) lambda_max) with the reference drivers' length scale
+    h = edge / sqrt(3) / 3 for a box of cubes of side `edge` cut into tetrahedra
+    (examples/TaylerGreenVortex/TGBatch.cpp:358-383)."""
+    h = edge / np.sqrt(3.0) / 3.0
     return cfl * h / ((2 * order + 1) * lam_max)
 
 

@@ -124,6 +124,13 @@ int dg_ssprk3(dg_ctx* ctx, double dt, int nsteps);
 /* Capture one SSP-RK3 step in a CUDA graph and replay it nsteps times. */
 int dg_ssprk3_graph(dg_ctx* ctx, double dt, int nsteps);
 
+/* Same as dg_ssprk3, with CUDA events around every kernel launch on the context's stream.
+ * out[2k] = total milliseconds and out[2k+1] = launch count of kernel class k < nclass
+ * (FP64 form: 0 = face flux, 1 = element volume/lift/update; mixed form: see DESIGN). */
+int dg_ssprk3_timed(dg_ctx* ctx, double dt, int nsteps, double* out, int nclass);
+/* The context's CUDA stream (a cudaStream_t) on which every kernel of the context runs. */
+void* dg_stream(dg_ctx* ctx);
+
 /* Diagonal mass b[e][5i+k] = detJ * sum_g w_g phi_i(x_g)^2 (Riemann1D.cpp:108-121). */
 int dg_mass(dg_ctx* ctx, double* mass, size_t elem_stride_bytes);
 

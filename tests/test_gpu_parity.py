@@ -118,15 +118,19 @@ def test_ssprk3_matches_oracle_and_graph(mesh3, P):
 
 def test_determinism_and_free_stream():
     m = box_mesh(4, jitter=0.1, seed=9)
-    for P in (1, 2, 3, 4):
-        conv = ExplicitConvection(m, order=P)
+    # (order, tet rule, tri rule, tolerance): Degree10Points24 is itself exact only to ~1e-10
+    # (its source data, data/QuadData/rotationalsymmetry.txt, has that precision), which bounds
+    # how well the discrete divergence theorem, and so free-stream preservation, holds with it.
+    for P, qv, qf, tol in ((1, 0, 1, 1e-12), (2, 1, 2, 1e-12), (3, 3, 3, 1e-9), (4, 5, 3, 1e-9)):
+        conv = ExplicitConvection(m, order=P, quad_vol=qv, quad_face=qf)
         U = noisy_state(m, P, 50 + P)
         assert np.array_equal(conv.eval(U), conv.eval(U))  # no atomics: bitwise repeatable
         Uc = problems.project(m, P, lambda X: problems.conserved(
             np.ones(X.shape[:-1]), 0.3 + 0 * X[..., 0], -0.2 + 0 * X[..., 0], 0.1 + 0 * X[..., 0],
             np.ones(X.shape[:-1]), 1.4))
         R = conv.eval(Uc)
-        assert np.abs(R).max() < 1e-12 * 10  # free stream preserved on a periodic mesh
+        scale = np.abs(conv.eval_internals(Uc)).max()  # size of the individual face terms
+        assert np.abs(R).max() < tol * scale, P  # free stream preserved on a periodic mesh
 
 
 def test_mass_conservation_and_sums(mesh3):
