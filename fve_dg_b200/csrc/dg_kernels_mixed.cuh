@@ -1,23 +1,31 @@
 // Mixed-precision form of the explicit DG operator.
 //
 // The four dense contractions of a stage run on the tensor cores as BF16 MMAs with FP32
-// accumulation (mma.sync.m16n8k16), each operand split into hi + lo BF16 parts and the three
-// products hi*hi + hi*lo + lo*hi accumulated (about 16 significant bits per product):
-//   face traces      U'(x_g) = sum_{b>=1} phi_b(xi_g^perm) c_b          A = face-map table
-//   volume values    U'(x_g) = sum_{b>=1} phi_b(x_g) c_b                A = volume table
-//   volume integral  R_v[j]  = -sum_{g,d} w_g dphi_j,d(x_g) G'_d(x_g)   A = weighted gradients
-//   face integral    R_f[j]  = +-sum_g w_g phi_j(xi_g^perm) F'(x_g)     A = weighted face-map table
+// accumulation (mma.sync.m16n8k16). Both operands are split into hi + lo BF16 parts and the three
+// products hi*hi + hi*lo + lo*hi are accumulated (about 16 significant bits per product):
+//   face traces      U'(x_g) = sum_{b>=1} phi_b(xi_g^perm) c_b          B = face-map table
+//   volume values    U'(x_g) = sum_{b>=1} phi_b(x_g) c_b                B = volume table
+//   volume integral  R_v[j]  = -sum_{g,d} w_g dphi_j,d(x_g) G'_d(x_g)   B = weighted gradients
+//   face integral    R_f[j]  = +-sum_g w_g phi_j(xi_g^perm) F'(x_g)     B = weighted face-map table
+// The MMA's 16 rows hold (item, variable) pairs of three items (faces or elements) that share their
+// face maps, so one table fragment serves three items. Items are grouped that way on the host.
+//
 // Only deviations go through the tensor cores: the mode-0 coefficient c_0 (phi_0 = 1) is added to
-// the traces exactly, and the per-element/per-face means of G and F are integrated exactly in FP64
-// against precomputed moments (sum_g w_g dphi_j and sum_g w_g phi_j). Large constant backgrounds
-// (the p0 ~ 71 pressure of a Mach 0.1 flow) therefore never meet BF16 rounding. The pointwise flux
-// and the Riemann solvers run in FP32; the RK stage update, the inverse mass and the state stay in
-// FP64. Contractions follow ExplicitConvection.cpp:144-272 term by term.
+// the traces exactly; the volume flux is taken relative to the flux of the element mean state and
+// the face flux relative to its face mean, and those references are integrated exactly in FP64
+// against precomputed moments (sum_g w_g dphi_j and sum_g w_g phi_j). The mode-0 face integral
+// is summed in FP64 in one fixed order per face, so both sides receive exactly opposite amounts
+// and the element means (mass, momentum, energy) are conserved to round-off. Large constant
+// backgrounds (the p0 ~ 71 of a Mach 0.1 flow) never meet BF16 rounding. The pointwise flux and
+// the Riemann solvers run in FP32; the RK stage update, the inverse mass and the state are FP64.
+// The terms follow ExplicitConvection.cpp:144-272 one for one.
 #pragma once
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <map>
 #include <vector>
 
 #include "dg_flux.cuh"
@@ -27,24 +35,39 @@
 namespace fvedg {
 
 __host__ __device__ constexpr int pad16(int x) { return (x + 15) / 16 * 16; }
+__host__ __device__ constexpr int pad8(int x) { return (x + 7) / 8 * 8; }
 
-struct MixedTables {  // device pointers
-    const __nv_bfloat16 *tfa_hi, *tfa_lo;  // [24][MF][KB]   face traces
-    const __nv_bfloat16 *tva_hi, *tva_lo;  // [MV][KB]       volume values
-    const __nv_bfloat16 *tvp_hi, *tvp_lo;  // [MJ][KV]       volume integral
-    const __nv_bfloat16 *tfl_hi, *tfl_lo;  // [24][MJ][KF]   face integral
+struct MixedTables {  // device pointers; every table row-major [n][k] (the MMA's B operand)
+    const __nv_bfloat16 *tfa_hi, *tfa_lo;  // [24][MF][KB]   face traces:  n = face point, k = mode-1
+    const __nv_bfloat16 *tva_hi, *tva_lo;  // [MV][KB]       volume values: n = volume point
+    const __nv_bfloat16 *tvp_hi, *tvp_lo;  // [MJ][KV]       volume integral: n = mode, k = (point, dir)
+    const __nv_bfloat16 *tfl_hi, *tfl_lo;  // [24][MJ][KF]   face integral: n = mode, k = face point
     const double* mv;                      // [NB][3]  sum_g w_g dphi_j
     const double* mf;                      // [24][NB] sum_g w_g phi_j(xi_g^perm)
-    const double* wf;                      // [NQF] face weights
+    const double* wf;                      // [NQF]
+};
+
+struct FaceGroup {   // up to three faces with equal (perm0, perm1, kind)
+    int f[3];
+    int n;
+};
+struct ElemGroup {   // up to three elements with equal face maps in canonical face order
+    int e[3];
+    int n;
+    int face[3][4];  // face id of canonical local face q (the face opposite local vertex q)
+    int meta[4];     // perm | side << 8, shared by the group
 };
 
 struct MixedFaceArgs {
     const double* U;
     const FaceInfo* fi;
+    const FaceGroup* groups;
     const double* UD;
-    float* Fj;        // [nface][nqf][5]: 2A * numerical flux at the face points (no quadrature weight)
+    float* Fj;        // [nface][nqf][5] 2A * numerical flux at the face points
+    double* Fmean;    // [nface][5] mean over the face points of Fj
+    double* S0;       // [nface][5] sum_g w_g Fj
     MixedTables t;
-    int nface;
+    int ngroups;
     float gamma;
     int flux;
     int faces_mask;
@@ -55,11 +78,13 @@ struct MixedElemArgs {
     const double* U0;
     double* out;
     const float* Fj;
+    const double* Fmean;
+    const double* S0;
     const double* geo;
-    const ElemFace* ef;
+    const ElemGroup* groups;
     const double* mass_ref;
     MixedTables t;
-    int ncell;
+    int ngroups;
     float gamma;
     double dt, a0, a1;
     int mode;
@@ -84,95 +109,109 @@ __device__ __forceinline__ void mma16816(float d[4], const uint32_t a[4], const 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// A fragment of tile (mt, kt) of a row-major BF16 table with leading dimension ld.
-__device__ __forceinline__ void load_a(const __nv_bfloat16* T, int ld, int mt, int kt, int lane, uint32_t a[4]) {
-    const int gid = lane >> 2, tig = lane & 3;
-    const __nv_bfloat16* p = T + (mt * 16 + gid) * ld + kt * 16 + tig * 2;
-    a[0] = __ldg((const unsigned int*)p);
-    a[1] = __ldg((const unsigned int*)(p + 8 * ld));
-    a[2] = __ldg((const unsigned int*)(p + 8));
-    a[3] = __ldg((const unsigned int*)(p + 8 * ld + 8));
-}
-
-// B fragment (16 x 8, k-major) for k-tile kt from a value functor v(k, n) -> float, split hi/lo.
+// A fragment (16 x 16, row-major) of k-tile kt from a value functor v(row, col) -> float, split.
 template <class V>
-__device__ __forceinline__ void load_b(V v, int kt, int lane, uint32_t bh[2], uint32_t bl[2]) {
+__device__ __forceinline__ void build_a(V v, int kt, int lane, uint32_t ah[4], uint32_t al[4]) {
     const int gid = lane >> 2, tig = lane & 3;
-    __nv_bfloat16 h[4], l[4];
+    __nv_bfloat16 h[8], l[8];
     #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const int k = kt * 16 + tig * 2 + (r & 1) + (r >> 1) * 8;
-        split_bf16(v(k, gid), h[r], l[r]);
+    for (int r = 0; r < 8; ++r) {
+        const int row = gid + ((r >> 1) & 1) * 8;
+        const int col = kt * 16 + tig * 2 + (r & 1) + (r >> 2) * 8;
+        split_bf16(v(row, col), h[r], l[r]);
     }
-    bh[0] = pack_bf16(h[0], h[1]);
-    bh[1] = pack_bf16(h[2], h[3]);
-    bl[0] = pack_bf16(l[0], l[1]);
-    bl[1] = pack_bf16(l[2], l[3]);
+    #pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        ah[i] = pack_bf16(h[2 * i], h[2 * i + 1]);
+        al[i] = pack_bf16(l[2 * i], l[2 * i + 1]);
+    }
 }
 
-// acc += A * B with both operands split: hi*hi + hi*lo + lo*hi
-__device__ __forceinline__ void mma3(float acc[4], const __nv_bfloat16* Th, const __nv_bfloat16* Tl, int ld,
-                                     int mt, int kt, int lane, const uint32_t bh[2], const uint32_t bl[2]) {
-    uint32_t ah[4], al[4];
-    load_a(Th, ld, mt, kt, lane, ah);
-    load_a(Tl, ld, mt, kt, lane, al);
+// acc(16 x 8 tile nt) += A * B(nt, kt) with B read from a row-major [n][k] BF16 table of leading
+// dimension ld; three products hi*hi + hi*lo + lo*hi.
+__device__ __forceinline__ void mma3_b(float acc[4], const uint32_t ah[4], const uint32_t al[4],
+                                       const __nv_bfloat16* Th, const __nv_bfloat16* Tl, int ld, int nt, int kt,
+                                       int lane) {
+    const int gid = lane >> 2, tig = lane & 3;
+    const int off = (nt * 8 + gid) * ld + kt * 16 + tig * 2;
+    uint32_t bh[2], bl[2];
+    bh[0] = __ldg((const unsigned int*)(Th + off));
+    bh[1] = __ldg((const unsigned int*)(Th + off + 8));
+    bl[0] = __ldg((const unsigned int*)(Tl + off));
+    bl[1] = __ldg((const unsigned int*)(Tl + off + 8));
     mma16816(acc, ah, bh);
     mma16816(acc, ah, bl);
     mma16816(acc, al, bh);
 }
 
-// One warp per face: trace deviations of both sides on the tensor cores, then one lane per face
-// point adds the mode-0 coefficient and evaluates the numerical flux in FP32.
+// One warp per face group: trace deviations of each side for the three faces (rows (face, var))
+// on the tensor cores, then one lane per face point adds c_0 and evaluates the FP32 flux.
 template <int NB, int NQF, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
-    constexpr int KB = pad16(NB - 1), MF = pad16(NQF);
-    __shared__ float sU[WARPS][2][MF][8];
+    constexpr int KB = pad16(NB - 1), MF = pad8(NQF);
+    __shared__ float sU[WARPS][2][16][MF + 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gid = lane >> 2, tig = lane & 3;
-    for (int f = blockIdx.x * WARPS + warp; f < a.nface; f += gridDim.x * WARPS) {
-        const FaceInfo fi = a.fi[f];
-        const int p[2] = {fi.meta & 0xff, (fi.meta >> 8) & 0xff};
-        const int bc = (fi.meta >> 16) & 0xff;
-        const bool interior = fi.c1 >= 0;
+    for (int gi = blockIdx.x * WARPS + warp; gi < a.ngroups; gi += gridDim.x * WARPS) {
+        const FaceGroup grp = a.groups[gi];
+        const FaceInfo f0 = a.fi[grp.f[0]];  // shares perms and kind with the others
+        const int perm[2] = {f0.meta & 0xff, (f0.meta >> 8) & 0xff};
+        const int bc = (f0.meta >> 16) & 0xff;
+        const bool interior = f0.c1 >= 0;
         const bool active = interior ? (a.faces_mask & 1)
                                      : ((a.faces_mask & 2) && ((bc == 0 && a.UD != nullptr) || bc == 5));
         if (!active) {
-            for (int i = lane; i < NQF * 5; i += 32) a.Fj[(int64_t)f * NQF * 5 + i] = 0.f;
+            for (int i = lane; i < grp.n * NQF * 5; i += 32) {
+                const int fl = i / (NQF * 5);
+                a.Fj[(int64_t)grp.f[fl] * NQF * 5 + (i - fl * NQF * 5)] = 0.f;
+            }
+            for (int i = lane; i < grp.n * 5; i += 32) {
+                a.Fmean[(int64_t)grp.f[i / 5] * 5 + i % 5] = 0.0;
+                a.S0[(int64_t)grp.f[i / 5] * 5 + i % 5] = 0.0;
+            }
             continue;
         }
         const int nside = interior ? 2 : 1;
         for (int s = 0; s < nside; ++s) {
-            const double* coef = a.U + (int64_t)(s ? fi.c1 : fi.c0) * (5 * NB);
-            uint32_t bh[KB / 16][2], bl[KB / 16][2];
+            const double* cf[3];
+            #pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const FaceInfo& F = a.fi[grp.f[i]];
+                cf[i] = a.U + (int64_t)(s ? F.c1 : F.c0) * (5 * NB);
+            }
+            uint32_t ah[KB / 16][4], al[KB / 16][4];
             #pragma unroll
             for (int kt = 0; kt < KB / 16; ++kt)
-                load_b([&](int k, int n) {
-                    return (n < 5 && k + 1 < NB) ? (float)__ldg(coef + 5 * (k + 1) + n) : 0.f;
-                }, kt, lane, bh[kt], bl[kt]);
-            const __nv_bfloat16* th = a.t.tfa_hi + p[s] * MF * KB;
-            const __nv_bfloat16* tl = a.t.tfa_lo + p[s] * MF * KB;
+                build_a([&](int row, int col) {
+                    const int fl = row / 5, k = row - 5 * (row / 5), b = col + 1;
+                    return (row < 5 * grp.n && b < NB) ? (float)__ldg(cf[fl] + 5 * b + k) : 0.f;
+                }, kt, lane, ah[kt], al[kt]);
+            const __nv_bfloat16* th = a.t.tfa_hi + perm[s] * MF * KB;
+            const __nv_bfloat16* tl = a.t.tfa_lo + perm[s] * MF * KB;
             #pragma unroll
-            for (int mt = 0; mt < MF / 16; ++mt) {
+            for (int nt = 0; nt < MF / 8; ++nt) {
                 float acc[4] = {0.f, 0.f, 0.f, 0.f};
                 #pragma unroll
-                for (int kt = 0; kt < KB / 16; ++kt) mma3(acc, th, tl, KB, mt, kt, lane, bh[kt], bl[kt]);
-                sU[warp][s][mt * 16 + gid][tig * 2] = acc[0];
-                sU[warp][s][mt * 16 + gid][tig * 2 + 1] = acc[1];
-                sU[warp][s][mt * 16 + gid + 8][tig * 2] = acc[2];
-                sU[warp][s][mt * 16 + gid + 8][tig * 2 + 1] = acc[3];
+                for (int kt = 0; kt < KB / 16; ++kt) mma3_b(acc, ah[kt], al[kt], th, tl, KB, nt, kt, lane);
+                sU[warp][s][gid][nt * 8 + tig * 2] = acc[0];
+                sU[warp][s][gid][nt * 8 + tig * 2 + 1] = acc[1];
+                sU[warp][s][gid + 8][nt * 8 + tig * 2] = acc[2];
+                sU[warp][s][gid + 8][nt * 8 + tig * 2 + 1] = acc[3];
             }
         }
         __syncwarp();
-        if (lane < NQF) {
-            const int g = lane;
+        for (int p = lane; p < grp.n * NQF; p += 32) {
+            const int fl = p / NQF, g = p - fl * NQF;
+            const int f = grp.f[fl];
+            const FaceInfo fi = a.fi[f];
             const double* cL = a.U + (int64_t)fi.c0 * (5 * NB);
             float UL[5], UR[5];
             #pragma unroll
-            for (int k = 0; k < 5; ++k) UL[k] = (float)(__ldg(cL + k) + (double)sU[warp][0][g][k]);
+            for (int k = 0; k < 5; ++k) UL[k] = (float)(__ldg(cL + k) + (double)sU[warp][0][fl * 5 + k][g]);
             if (interior) {
                 const double* cR = a.U + (int64_t)fi.c1 * (5 * NB);
                 #pragma unroll
-                for (int k = 0; k < 5; ++k) UR[k] = (float)(__ldg(cR + k) + (double)sU[warp][1][g][k]);
+                for (int k = 0; k < 5; ++k) UR[k] = (float)(__ldg(cR + k) + (double)sU[warp][1][fl * 5 + k][g]);
             } else if (bc == 0) {
                 const double* ud = a.UD + ((int64_t)f * NQF + g) * 5;
                 #pragma unroll
@@ -190,164 +229,187 @@ __global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
             float* o = a.Fj + ((int64_t)f * NQF + g) * 5;
             #pragma unroll
             for (int k = 0; k < 5; ++k) o[k] = Fh[k] * jw;
+            // side-1 deviations are no longer needed: keep the face flux there for the sums below
+            #pragma unroll
+            for (int k = 0; k < 5; ++k) sU[warp][1][fl * 5 + k][g] = Fh[k] * jw;
+        }
+        __syncwarp();
+        if (lane < 5 * grp.n) {  // face mean and the exact mode-0 sum, FP64, fixed order
+            const int fl = lane / 5, k = lane - 5 * fl;
+            double s = 0.0, s0 = 0.0;
+            for (int g = 0; g < NQF; ++g) {
+                const double v = (double)sU[warp][1][fl * 5 + k][g];
+                s += v;
+                s0 += __ldg(a.t.wf + g) * v;
+            }
+            a.Fmean[(int64_t)grp.f[fl] * 5 + k] = s / NQF;
+            a.S0[(int64_t)grp.f[fl] * 5 + k] = s0;
         }
         __syncwarp();
     }
 }
 
-// One warp per element: volume values (MMA), FP32 flux, volume integral (MMA), the four face
-// integrals (MMA), exact FP64 mean-part integrals, then the FP64 RK stage update.
+template <int NB, int NQV, int NQF>
+struct ElemMixedSmem {
+    static constexpr int MV = pad8(NQV), KV = pad16(3 * NQV), KF = pad16(NQF);
+    double sGb[3][15];               // G(c_0) per element
+    double sFb[3][4][5];             // face means
+    double sS0[3][4][5];             // exact mode-0 face sums
+    float sU[16][MV + 1];            // volume deviations, rows (element, var), cols point
+    float sG[16][KV + 2];            // G - G(c_0), rows (element, var), cols (point, dir)
+    float sF[16][KF + 2];            // face flux deviations for one local face, rows (element, var)
+};
+
+// One warp per element group: volume values, FP32 flux, volume integral, the four face integrals,
+// the FP64 mean parts and the FP64 RK stage update.
 template <int NB, int NQV, int NQF, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) element_mixed(MixedElemArgs a) {
-    constexpr int KB = pad16(NB - 1), MV = pad16(NQV), MJ = pad16(NB), KV = pad16(3 * NQV), KF = pad16(NQF);
-    __shared__ float sU[WARPS][MV][8];
-    __shared__ float sG[WARPS][NQV * 15];
-    __shared__ float sF[WARPS][4][NQF * 5];
-    __shared__ double sGbar[WARPS][15];
-    __shared__ double sFbar[WARPS][4][5];
-    __shared__ double sS0[WARPS][4][5];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    using S = ElemMixedSmem<NB, NQV, NQF>;
+    constexpr int KB = pad16(NB - 1), MV = S::MV, MJ = pad8(NB), KV = S::KV, KF = S::KF;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    S& sm = reinterpret_cast<S*>(smem_raw)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
     const int gid = lane >> 2, tig = lane & 3;
-    for (int e = blockIdx.x * WARPS + warp; e < a.ncell; e += gridDim.x * WARPS) {
-        const double* coef = a.U + (int64_t)e * (5 * NB);
-        const double* geo = a.geo + (int64_t)e * 10;
-        float accv[MJ / 16][4], accf[MJ / 16][4];
+    for (int gi = blockIdx.x * WARPS + (threadIdx.x >> 5); gi < a.ngroups; gi += gridDim.x * WARPS) {
+        const ElemGroup grp = a.groups[gi];
+        const int ne = grp.n;
+        const double* coef[3];
         #pragma unroll
-        for (int mt = 0; mt < MJ / 16; ++mt)
+        for (int i = 0; i < 3; ++i) coef[i] = a.U + (int64_t)grp.e[i] * (5 * NB);
+        float accv[MJ / 8][4], accf[MJ / 8][4];
+        #pragma unroll
+        for (int nt = 0; nt < MJ / 8; ++nt)
             #pragma unroll
-            for (int r = 0; r < 4; ++r) accv[mt][r] = accf[mt][r] = 0.f;
+            for (int r = 0; r < 4; ++r) accv[nt][r] = accf[nt][r] = 0.f;
         if (a.with_volume) {
-            uint32_t bh[KB / 16][2], bl[KB / 16][2];
-            #pragma unroll
-            for (int kt = 0; kt < KB / 16; ++kt)
-                load_b([&](int k, int n) {
-                    return (n < 5 && k + 1 < NB) ? (float)__ldg(coef + 5 * (k + 1) + n) : 0.f;
-                }, kt, lane, bh[kt], bl[kt]);
-            #pragma unroll
-            for (int mt = 0; mt < MV / 16; ++mt) {
-                float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            // G(c_0): flux of the element mean state (FP64), the reference of the deviations
+            if (lane < ne) {
+                const double* geo = a.geo + (int64_t)grp.e[lane] * 10;
+                double c0[5], F[5][3];
                 #pragma unroll
-                for (int kt = 0; kt < KB / 16; ++kt) mma3(acc, a.t.tva_hi, a.t.tva_lo, KB, mt, kt, lane, bh[kt], bl[kt]);
-                sU[warp][mt * 16 + gid][tig * 2] = acc[0];
-                sU[warp][mt * 16 + gid][tig * 2 + 1] = acc[1];
-                sU[warp][mt * 16 + gid + 8][tig * 2] = acc[2];
-                sU[warp][mt * 16 + gid + 8][tig * 2 + 1] = acc[3];
+                for (int k = 0; k < 5; ++k) c0[k] = __ldg(coef[lane] + k);
+                Phys<double>::flux(c0, (double)a.gamma - 1.0, F);
+                const double dj = __ldg(geo + 9);
+                #pragma unroll
+                for (int k = 0; k < 5; ++k)
+                    #pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        sm.sGb[lane][3 * k + d] =
+                            dj * (F[k][0] * __ldg(geo + d) + F[k][1] * __ldg(geo + 3 + d) + F[k][2] * __ldg(geo + 6 + d));
+            }
+            {
+                uint32_t ah[KB / 16][4], al[KB / 16][4];
+                #pragma unroll
+                for (int kt = 0; kt < KB / 16; ++kt)
+                    build_a([&](int row, int col) {
+                        const int el = row / 5, k = row - 5 * (row / 5), b = col + 1;
+                        return (row < 5 * ne && b < NB) ? (float)__ldg(coef[el] + 5 * b + k) : 0.f;
+                    }, kt, lane, ah[kt], al[kt]);
+                #pragma unroll
+                for (int nt = 0; nt < MV / 8; ++nt) {
+                    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+                    #pragma unroll
+                    for (int kt = 0; kt < KB / 16; ++kt)
+                        mma3_b(acc, ah[kt], al[kt], a.t.tva_hi, a.t.tva_lo, KB, nt, kt, lane);
+                    sm.sU[gid][nt * 8 + tig * 2] = acc[0];
+                    sm.sU[gid][nt * 8 + tig * 2 + 1] = acc[1];
+                    sm.sU[gid + 8][nt * 8 + tig * 2] = acc[2];
+                    sm.sU[gid + 8][nt * 8 + tig * 2 + 1] = acc[3];
+                }
             }
             __syncwarp();
-            float J[9];
-            #pragma unroll
-            for (int i = 0; i < 9; ++i) J[i] = (float)__ldg(geo + i);
-            const float dj = (float)__ldg(geo + 9);
-            for (int g = lane; g < NQV; g += 32) {
-                float U[5], F[5][3];
+            for (int p = lane; p < ne * NQV; p += 32) {
+                const int el = p / NQV, g = p - el * NQV;
+                const double* geo = a.geo + (int64_t)grp.e[el] * 10;
+                float U[5], F[5][3], J[9];
                 #pragma unroll
-                for (int k = 0; k < 5; ++k) U[k] = (float)(__ldg(coef + k) + (double)sU[warp][g][k]);
+                for (int k = 0; k < 5; ++k) U[k] = (float)(__ldg(coef[el] + k) + (double)sm.sU[el * 5 + k][g]);
+                #pragma unroll
+                for (int i = 0; i < 9; ++i) J[i] = (float)__ldg(geo + i);
+                const float dj = (float)__ldg(geo + 9);
                 Phys<float>::flux(U, a.gamma - 1.f, F);
                 #pragma unroll
                 for (int k = 0; k < 5; ++k)
                     #pragma unroll
                     for (int d = 0; d < 3; ++d)
-                        sG[warp][g * 15 + 3 * k + d] = dj * (F[k][0] * J[d] + F[k][1] * J[3 + d] + F[k][2] * J[6 + d]);
+                        sm.sG[el * 5 + k][3 * g + d] =
+                            dj * (F[k][0] * J[d] + F[k][1] * J[3 + d] + F[k][2] * J[6 + d]) - (float)sm.sGb[el][3 * k + d];
             }
             __syncwarp();
-            if (lane < 15) {
-                double s = 0.0;
-                for (int g = 0; g < NQV; ++g) s += (double)sG[warp][g * 15 + lane];
-                sGbar[warp][lane] = s / NQV;
-            }
-            __syncwarp();
-            const float* G = sG[warp];
-            const double* Gb = sGbar[warp];
             #pragma unroll
             for (int kt = 0; kt < KV / 16; ++kt) {
-                uint32_t gh[2], gl[2];
-                load_b([&](int k, int n) {
-                    if (n >= 5 || k >= 3 * NQV) return 0.f;
-                    const int g = k / 3, d = k - 3 * g;
-                    return G[g * 15 + 3 * n + d] - (float)Gb[3 * n + d];
-                }, kt, lane, gh, gl);
+                uint32_t ah[4], al[4];
+                build_a([&](int row, int col) {
+                    return (row < 5 * ne && col < 3 * NQV) ? sm.sG[row][col] : 0.f;
+                }, kt, lane, ah, al);
                 #pragma unroll
-                for (int mt = 0; mt < MJ / 16; ++mt) mma3(accv[mt], a.t.tvp_hi, a.t.tvp_lo, KV, mt, kt, lane, gh, gl);
+                for (int nt = 0; nt < MJ / 8; ++nt) mma3_b(accv[nt], ah, al, a.t.tvp_hi, a.t.tvp_lo, KV, nt, kt, lane);
             }
         }
-        // face integrals
-        for (int i = lane; i < 4 * NQF * 5; i += 32) {
-            const int q = i / (NQF * 5), off = i - q * (NQF * 5);
-            const int face = a.ef[(int64_t)e * 4 + q].face;
-            sF[warp][q][off] = __ldcg(a.Fj + (int64_t)face * NQF * 5 + off);
-        }
-        __syncwarp();
-        if (lane < 20) {
-            // per face: the mean used for the deviations, and the exact mode-0 integral
-            // sum_g w_g F (phi_0 = 1), summed in one fixed order so that the two sides of a face
-            // receive exactly opposite contributions and the element means are conserved
-            const int q = lane / 5, k = lane - 5 * q;
-            double s = 0.0, s0 = 0.0;
-            for (int g = 0; g < NQF; ++g) {
-                const double v = (double)sF[warp][q][g * 5 + k];
-                s += v;
-                s0 += __ldg(a.t.wf + g) * v;
-            }
-            sFbar[warp][q][k] = s / NQF;
-            sS0[warp][q][k] = s0;
+        // face means and exact mode-0 sums of the four faces of each element
+        for (int i = lane; i < ne * 20; i += 32) {
+            const int el = i / 20, r = i - el * 20, q = r / 5, k = r - 5 * q;
+            const int f = grp.face[el][q];
+            sm.sFb[el][q][k] = __ldcg(a.Fmean + (int64_t)f * 5 + k);
+            sm.sS0[el][q][k] = __ldcg(a.S0 + (int64_t)f * 5 + k);
         }
         __syncwarp();
         #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int meta = a.ef[(int64_t)e * 4 + q].meta;
-            const int perm = meta & 0xff;
-            const float sgn = (meta >> 8) ? -1.f : 1.f;
-            const float* Fq = sF[warp][q];
-            const double* Fb = sFbar[warp][q];
+            const int perm = grp.meta[q] & 0xff;
+            const float sgn = (grp.meta[q] >> 8) ? -1.f : 1.f;
+            for (int i = lane; i < ne * NQF * 5; i += 32) {
+                const int el = i / (NQF * 5), r = i - el * NQF * 5, g = r / 5, k = r - 5 * g;
+                const float v = __ldcg(a.Fj + (int64_t)grp.face[el][q] * NQF * 5 + r);
+                sm.sF[el * 5 + k][g] = sgn * (v - (float)sm.sFb[el][q][k]);
+            }
+            __syncwarp();
             const __nv_bfloat16* th = a.t.tfl_hi + perm * MJ * KF;
             const __nv_bfloat16* tl = a.t.tfl_lo + perm * MJ * KF;
             #pragma unroll
             for (int kt = 0; kt < KF / 16; ++kt) {
-                uint32_t fh[2], fl[2];
-                load_b([&](int k, int n) {
-                    return (n < 5 && k < NQF) ? sgn * (Fq[k * 5 + n] - (float)Fb[n]) : 0.f;
-                }, kt, lane, fh, fl);
+                uint32_t ah[4], al[4];
+                build_a([&](int row, int col) {
+                    return (row < 5 * ne && col < NQF) ? sm.sF[row][col] : 0.f;
+                }, kt, lane, ah, al);
                 #pragma unroll
-                for (int mt = 0; mt < MJ / 16; ++mt) mma3(accf[mt], th, tl, KF, mt, kt, lane, fh, fl);
+                for (int nt = 0; nt < MJ / 8; ++nt) mma3_b(accf[nt], ah, al, th, tl, KF, nt, kt, lane);
             }
+            __syncwarp();
         }
-        // epilogue: this lane owns R[j][k] for j = mt*16 + gid (+8), k = 2 tig (+1)
-        const double detj = __ldg(geo + 9);
+        // epilogue: this lane owns rows (element, var) gid and gid + 8, modes nt*8 + 2 tig (+1)
         #pragma unroll
-        for (int mt = 0; mt < MJ / 16; ++mt) {
+        for (int nt = 0; nt < MJ / 8; ++nt) {
             #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                const int j = mt * 16 + gid + (r >> 1) * 8;
-                const int k = tig * 2 + (r & 1);
-                if (j >= NB || k >= 5) continue;
-                double R = (double)accf[mt][r] - (double)accv[mt][r];
+                const int row = gid + (r >> 1) * 8;
+                const int j = nt * 8 + tig * 2 + (r & 1);
+                if (row >= 5 * ne || j >= NB) continue;
+                const int el = row / 5, k = row - 5 * el;
+                double R;
                 if (j == 0) {  // grad phi_0 = 0: only the exact face sums
                     R = 0.0;
                     #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int meta = a.ef[(int64_t)e * 4 + q].meta;
-                        R += (meta >> 8) ? -sS0[warp][q][k] : sS0[warp][q][k];
+                    for (int q = 0; q < 4; ++q) R += (grp.meta[q] >> 8) ? -sm.sS0[el][q][k] : sm.sS0[el][q][k];
+                } else {
+                    R = (double)accf[nt][r] - (double)accv[nt][r];
+                    if (a.with_volume) {
+                        const double* gb = sm.sGb[el] + 3 * k;
+                        const double* mv = a.t.mv + 3 * j;
+                        R -= gb[0] * __ldg(mv) + gb[1] * __ldg(mv + 1) + gb[2] * __ldg(mv + 2);
                     }
-                } else {
-                if (a.with_volume) {
-                    const double* gb = sGbar[warp] + 3 * k;
-                    const double* mv = a.t.mv + 3 * j;
-                    R -= gb[0] * __ldg(mv) + gb[1] * __ldg(mv + 1) + gb[2] * __ldg(mv + 2);
+                    #pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const double m = __ldg(a.t.mf + (grp.meta[q] & 0xff) * NB + j) * sm.sFb[el][q][k];
+                        R += (grp.meta[q] >> 8) ? -m : m;
+                    }
                 }
-                #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int meta = a.ef[(int64_t)e * 4 + q].meta;
-                    const double m = __ldg(a.t.mf + (meta & 0xff) * NB + j) * sFbar[warp][q][k];
-                    R += (meta >> 8) ? -m : m;
-                }
-                }
-                double* o = a.out + (int64_t)e * (5 * NB) + 5 * j + k;
+                const int64_t idx = (int64_t)grp.e[el] * (5 * NB) + 5 * j + k;
                 if (a.mode == 0) {
-                    *o = R;
+                    a.out[idx] = R;
                 } else {
-                    const double ib = 1.0 / (detj * __ldg(a.mass_ref + j));
-                    const double u0 = a.U0[(int64_t)e * (5 * NB) + 5 * j + k];
-                    *o = a.a0 * u0 + a.a1 * (__ldg(coef + 5 * j + k) + a.dt * (-R * ib));
+                    const double ib = 1.0 / (__ldg(a.geo + (int64_t)grp.e[el] * 10 + 9) * __ldg(a.mass_ref + j));
+                    a.out[idx] = a.a0 * a.U0[idx] + a.a1 * (__ldg(a.U + idx) + a.dt * (-R * ib));
                 }
             }
         }
@@ -362,17 +424,21 @@ struct MixedData {
     bool ready = false;
     int order = 0, qv = 0, qf = 0, nb = 0, nqv = 0, nqf = 0;
     int64_t ncell = 0, nface = 0;
+    int nfgroups = 0, negroups = 0;
     float gamma = 1.4f;
     int flux = 0;
     int sms = 148;
     std::vector<void*> bufs;
     MixedTables t{};
     const FaceInfo* fi = nullptr;
-    const ElemFace* ef = nullptr;
+    const FaceGroup* fgroups = nullptr;
+    const ElemGroup* egroups = nullptr;
     const double* geo = nullptr;
     const double* mass_ref = nullptr;
     const double* UD = nullptr;
     float* Fj = nullptr;
+    double* Fmean = nullptr;
+    double* S0 = nullptr;
 };
 
 // X(order, qv, qf, NB, NQV, NQF)
@@ -400,10 +466,20 @@ inline bool mixed_supported(int order, int qv, int qf) {
 template <typename T>
 inline int mixed_upload(MixedData& m, const T** dst, const std::vector<T>& v) {
     void* p = nullptr;
-    if (cudaMalloc(&p, sizeof(T) * v.size()) != cudaSuccess) return DG_E_NOMEM;
+    if (cudaMalloc(&p, sizeof(T) * std::max<size_t>(v.size(), 1)) != cudaSuccess) return DG_E_NOMEM;
     m.bufs.push_back(p);
-    if (cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess) return DG_E_CUDA;
+    if (!v.empty() && cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return DG_E_CUDA;
     *dst = (const T*)p;
+    return DG_OK;
+}
+
+template <typename T>
+inline int mixed_alloc(MixedData& m, T** dst, size_t n) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, sizeof(T) * std::max<size_t>(n, 1)) != cudaSuccess) return DG_E_NOMEM;
+    m.bufs.push_back(p);
+    *dst = (T*)p;
     return DG_OK;
 }
 
@@ -417,13 +493,60 @@ inline void split_table(const std::vector<double>& x, std::vector<__nv_bfloat16>
     }
 }
 
-inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>&, const std::vector<FaceInfo>&,
-                      const std::vector<ElemFace>&, int64_t ncell, int64_t nface, double gamma, int flux,
-                      int qv, int qf, const double* d_geo, const FaceInfo* d_fi, const ElemFace* d_ef,
+// Faces with equal (perm0, perm1, kind) and elements with equal face maps (in canonical face
+// order: local face q is the one opposite local vertex q) are grouped in threes, in mesh order.
+// A partial group repeats its first member in the unused slots (never read as a row: rows of
+// unused slots are masked by the group size).
+inline void build_groups(const std::vector<FaceInfo>& hfi, const std::vector<ElemFace>& hef, int64_t ncell,
+                         std::vector<FaceGroup>& fg, std::vector<ElemGroup>& eg) {
+    std::map<int64_t, FaceGroup> open_f;
+    for (int64_t f = 0; f < (int64_t)hfi.size(); ++f) {
+        const FaceInfo& F = hfi[f];
+        const int64_t key = (int64_t)(F.meta & 0xffffff) * 2 + (F.c1 >= 0 ? 1 : 0);
+        FaceGroup& g = open_f[key];
+        g.f[g.n++] = (int)f;
+        if (g.n == 3) { fg.push_back(g); g = FaceGroup{}; }
+    }
+    for (auto& kv : open_f)
+        if (kv.second.n > 0) {
+            for (int i = kv.second.n; i < 3; ++i) kv.second.f[i] = kv.second.f[0];
+            fg.push_back(kv.second);
+        }
+    std::map<std::vector<int>, ElemGroup> open_e;
+    for (int64_t e = 0; e < ncell; ++e) {
+        int face[4] = {-1, -1, -1, -1}, meta[4] = {0, 0, 0, 0};
+        for (int i = 0; i < 4; ++i) {
+            const ElemFace& ef = hef[4 * e + i];
+            const int p = ef.meta & 0xff;
+            const int q = 6 - kPermSlots[p][0] - kPermSlots[p][1] - kPermSlots[p][2];  // missing vertex
+            face[q] = ef.face;
+            meta[q] = ef.meta;
+        }
+        std::vector<int> key(meta, meta + 4);
+        ElemGroup& g = open_e[key];
+        g.e[g.n] = (int)e;
+        for (int q = 0; q < 4; ++q) { g.face[g.n][q] = face[q]; g.meta[q] = meta[q]; }
+        ++g.n;
+        if (g.n == 3) { eg.push_back(g); g = ElemGroup{}; }
+    }
+    for (auto& kv : open_e)
+        if (kv.second.n > 0) {
+            ElemGroup g = kv.second;
+            for (int i = g.n; i < 3; ++i) {
+                g.e[i] = g.e[0];
+                for (int q = 0; q < 4; ++q) g.face[i][q] = g.face[0][q];
+            }
+            eg.push_back(g);
+        }
+}
+
+inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>&, const std::vector<FaceInfo>& hfi,
+                      const std::vector<ElemFace>& hef, int64_t ncell, int64_t nface, double gamma, int flux,
+                      int qv, int qf, const double* d_geo, const FaceInfo* d_fi, const ElemFace*,
                       const double* d_mass_ref) {
     if (!mixed_supported(tab.order, qv, qf)) return DG_E_ARG;
     const int NB = tab.nb, NQV = tab.nqv, NQF = tab.nqf;
-    const int KB = pad16(NB - 1), MF = pad16(NQF), MV = pad16(NQV), MJ = pad16(NB), KV = pad16(3 * NQV),
+    const int KB = pad16(NB - 1), MF = pad8(NQF), MV = pad8(NQV), MJ = pad8(NB), KV = pad16(3 * NQV),
               KF = pad16(NQF);
     m.order = tab.order; m.qv = qv; m.qf = qf; m.nb = NB; m.nqv = NQV; m.nqf = NQF;
     m.ncell = ncell; m.nface = nface; m.gamma = (float)gamma; m.flux = flux;
@@ -461,11 +584,16 @@ inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>
     if ((rc = mixed_upload(m, &m.t.mv, mv)) || (rc = mixed_upload(m, &m.t.mf, mf)) ||
         (rc = mixed_upload(m, &m.t.wf, tab.w_f)))
         return rc;
-    void* p = nullptr;
-    if (cudaMalloc(&p, sizeof(float) * (size_t)nface * NQF * 5) != cudaSuccess) return DG_E_NOMEM;
-    m.bufs.push_back(p);
-    m.Fj = (float*)p;
-    m.fi = d_fi; m.ef = d_ef; m.geo = d_geo; m.mass_ref = d_mass_ref;
+    std::vector<FaceGroup> fg;
+    std::vector<ElemGroup> eg;
+    build_groups(hfi, hef, ncell, fg, eg);
+    m.nfgroups = (int)fg.size();
+    m.negroups = (int)eg.size();
+    if ((rc = mixed_upload(m, &m.fgroups, fg)) || (rc = mixed_upload(m, &m.egroups, eg))) return rc;
+    if ((rc = mixed_alloc(m, &m.Fj, (size_t)nface * NQF * 5)) || (rc = mixed_alloc(m, &m.Fmean, (size_t)nface * 5)) ||
+        (rc = mixed_alloc(m, &m.S0, (size_t)nface * 5)))
+        return rc;
+    m.fi = d_fi; m.geo = d_geo; m.mass_ref = d_mass_ref;
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&m.sms, cudaDevAttrMultiProcessorCount, dev);
@@ -482,22 +610,30 @@ inline void free_mixed(MixedData& m) {
 inline void set_mixed_dirichlet(MixedData& m, const double* UD) { m.UD = UD; }
 inline int mixed_launches_per_step(const MixedData&) { return 6; }
 
-template <int NB, int NQV, int NQF, int kMixedWarps = (NB >= 35 ? 4 : 8)>
+template <int NB, int NQV, int NQF, int WF = 8, int WE = (NB >= 35 ? 4 : 8)>
 inline int mixed_launch(MixedData& m, int which, const double* U, const double* U0, double* out, int mode,
                         double dt, double a0, double a1, int face_mask, int with_volume, cudaStream_t s) {
     if (which == 0) {
         MixedFaceArgs fa;
-        fa.U = U; fa.fi = m.fi; fa.UD = m.UD; fa.Fj = m.Fj; fa.t = m.t; fa.nface = (int)m.nface;
-        fa.gamma = m.gamma; fa.flux = m.flux; fa.faces_mask = face_mask;
-        const int gf = (int)std::min<int64_t>((m.nface + kMixedWarps - 1) / kMixedWarps, (int64_t)m.sms * 16);
-        face_flux_mixed<NB, NQF, kMixedWarps><<<gf, kMixedWarps * 32, 0, s>>>(fa);
+        fa.U = U; fa.fi = m.fi; fa.groups = m.fgroups; fa.UD = m.UD; fa.Fj = m.Fj; fa.Fmean = m.Fmean; fa.S0 = m.S0;
+        fa.t = m.t; fa.ngroups = m.nfgroups; fa.gamma = m.gamma; fa.flux = m.flux; fa.faces_mask = face_mask;
+        const int gf = (int)std::min<int64_t>((m.nfgroups + WF - 1) / WF, (int64_t)m.sms * 16);
+        face_flux_mixed<NB, NQF, WF><<<gf, WF * 32, 0, s>>>(fa);
     } else {
+        constexpr size_t smem = sizeof(ElemMixedSmem<NB, NQV, NQF>) * WE;
+        static bool attr = false;
+        if (!attr) {
+            if (cudaFuncSetAttribute(element_mixed<NB, NQV, NQF, WE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem) != cudaSuccess)
+                return DG_E_CUDA;
+            attr = true;
+        }
         MixedElemArgs ea;
-        ea.U = U; ea.U0 = U0; ea.out = out; ea.Fj = m.Fj; ea.geo = m.geo; ea.ef = m.ef; ea.mass_ref = m.mass_ref;
-        ea.t = m.t; ea.ncell = (int)m.ncell; ea.gamma = m.gamma; ea.dt = dt; ea.a0 = a0; ea.a1 = a1;
-        ea.mode = mode; ea.with_volume = with_volume;
-        const int ge = (int)std::min<int64_t>((m.ncell + kMixedWarps - 1) / kMixedWarps, (int64_t)m.sms * 16);
-        element_mixed<NB, NQV, NQF, kMixedWarps><<<ge, kMixedWarps * 32, 0, s>>>(ea);
+        ea.U = U; ea.U0 = U0; ea.out = out; ea.Fj = m.Fj; ea.Fmean = m.Fmean; ea.S0 = m.S0; ea.geo = m.geo;
+        ea.groups = m.egroups; ea.mass_ref = m.mass_ref; ea.t = m.t; ea.ngroups = m.negroups; ea.gamma = m.gamma;
+        ea.dt = dt; ea.a0 = a0; ea.a1 = a1; ea.mode = mode; ea.with_volume = with_volume;
+        const int ge = (int)std::min<int64_t>((m.negroups + WE - 1) / WE, (int64_t)m.sms * 16);
+        element_mixed<NB, NQV, NQF, WE><<<ge, WE * 32, smem, s>>>(ea);
     }
     return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;
 }
