@@ -37,6 +37,9 @@ CONFIGS = {
     "vortex": dict(problem="vortex", n=8, L=10.0, jitter=0.0, P=1, qv=0, qf=1, flux="LF",
                    desc="isentropic vortex, [0,10]^3 periodic, 8^3x6=3,072 tets, P1, "
                         "Degree2Points4/Degree3Points6, LF, SSP-RK3 CFL 0.3"),
+    "ensemble": dict(problem="vortex", n=8, L=10.0, jitter=0.0, P=2, qv=1, qf=2, flux="LF",
+                     desc="64 isentropic-vortex instances on meshes n^3x6, n in U{8..32}, P2 (reference CPU "
+                          "sample: one 8^3x6 vortex)"),
     "dwave_p4": dict(problem="density_wave", n=64, L=1.0, jitter=0.1, P=4, qv=5, qf=3, flux="LF",
                      desc="density wave, [0,1]^3 periodic, 64^3x6=1,572,864 jittered tets, P4, "
                           "Degree8Points44/Degree10Points24, LF, SSP-RK3 CFL 0.3"),
@@ -121,16 +124,22 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def kernel_bytes(cls, P, ncell, nface, nqf, precision):
-    """Algorithmic bytes one launch must move (each input read once, each output written once)."""
+def kernel_bytes(name, P, ncell, nface, nqf):
+    """Algorithmic bytes one launch must move: each input read once, each output written once."""
     nb = nb_of(P)
     state = ncell * 5 * nb * 8
-    if precision == "fp64":
-        fh = nface * nqf * 5 * 8
-        if cls == 0:  # face_flux: state read, 48 B face record, Fh written
-            return state + nface * 48 + fh
-        # element: stage state + U^n read, new stage written, 80 B geometry + 32 B face list, Fh read
-        return 3 * state + ncell * (80 + 32) + fh
+    face_rec, elem_rec = 48, 80 + 32     # face record; element geometry + face list
+    if name == "face_flux_fp64":         # state read, face records, FP64 face fluxes written
+        return state + nface * face_rec + nface * nqf * 5 * 8
+    if name == "element_fp64":           # stage state + U^n read, new stage written, face fluxes read
+        return 3 * state + ncell * elem_rec + nface * nqf * 5 * 8
+    fj = nface * (nqf * 5 * 4 + 2 * 5 * 8)  # FP32 face fluxes + FP64 face means and mode-0 sums
+    if name == "face_flux_mixed":
+        return state + nface * face_rec + fj
+    if name == "element_mixed":
+        return 3 * state + ncell * elem_rec + fj
+    if name == "stage_persistent_mixed":  # both phases, the face data round trip included
+        return 3 * state + nface * face_rec + ncell * elem_rec + 2 * fj
     return None
 
 
@@ -213,7 +222,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="tgv", choices=sorted(CONFIGS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--schedule", default=None, choices=["two-launch", "persistent"])
+    ap.add_argument("--no-compare", action="store_true", help="skip timing the FP64 form beside the mixed one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n", type=int, default=0, help="override the mesh size (cubes per side), for profiling")
     args = ap.parse_args()
@@ -239,90 +250,59 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    if args.config == "ensemble":
+        run_ensemble(args, rank, world, local, dist)
+        if dist:
+            dist.destroy_process_group()
+        return
+
     P, qv, qf = cfg["P"], cfg["qv"], cfg["qf"]
     m = box_mesh(cfg["n"], hi=(cfg["L"],) * 3, jitter=cfg["jitter"])
     U0 = problems.project(m, P, problem_fn(cfg["problem"], problems))
+    schedule = args.schedule or ("persistent" if args.precision == "mixed" else "two-launch")
     conv = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf,
-                              precision=args.precision, device=local)
+                              precision=args.precision, device=local, schedule=schedule)
     conv.set_state(U0)
     dt = problems.cfl_dt(CFL, cfg["L"] / cfg["n"], P, conv.max_wave_speed())
     nb = conv.num_basis
     dof_stage_per_step = 5 * nb * m.ncell * 3
-    stream = torch.cuda.ExternalStream(conv.stream)
+    tune = conv.autotune(dt) if schedule == "persistent" else None
 
     sampler = ClockSampler(local)
     sampler.start()
-    conv.ssprk3(dt, args.warmup, graph=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    l0 = launch_count()
-    ev0.record(stream)
-    conv.ssprk3(dt, args.steps, graph=True)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    launches = launch_count() - l0
-    ms = ev0.elapsed_time(ev1)
-    if dist:
-        dist.barrier()
+    ms, launches = time_steps(conv, dt, args.warmup, args.steps, dist, torch, launch_count)
     clocks = sampler.stop()
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     value = dof_stage_per_step * args.steps * world / (ms / 1e3)
+    U_head = conv.get_state()
 
     # per-kernel durations with CUDA events on the context stream (same workload, separate pass)
     kt = conv.ssprk3_timed(dt, args.steps)
-    peak, peak_kind = read_peaks()
-    dom = max(kt, key=lambda k: kt[k][0])
-    dom_ms = kt[dom][0] / kt[dom][1]
-    names = {0: "face_flux_fp64", 1: "element_fp64"} if args.precision == "fp64" else {}
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            tj = json.load(f)
-        traffic = tj.get(f"{args.config}:{args.precision}", {}).get(names.get(dom, str(dom)))
-    except Exception:
-        pass
-    bytes_dom = kernel_bytes(dom, P, m.ncell, m.nface, conv.nq_face, args.precision)
-    stage_ms = sum(v[0] for v in kt.values()) / (3 * args.steps)
-    roofline = None
-    if bytes_dom:
-        ach = bytes_dom / (dom_ms / 1e3) / 1e9
-        roofline = {"bound": "hbm", "kernel": names.get(dom, str(dom)), "achieved": ach, "peak": peak,
-                    "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind, "traffic": traffic,
-                    "algorithmic_bytes_per_launch": bytes_dom, "avg_launch_ms": dom_ms,
-                    "stage": {"ms": stage_ms,
-                              "bytes_per_dof_stage_min": SURVEY_BYTES_PER_DOF_STAGE[P],
-                              "achieved_gbs_at_min_bytes": SURVEY_BYTES_PER_DOF_STAGE[P] * 5 * nb * m.ncell
-                              / (stage_ms / 1e3) / 1e9},
-                    "kernels_ms_per_launch": {names.get(k, str(k)): v[0] / v[1] for k, v in kt.items()}}
+    roofline = make_roofline(kt, args.precision, schedule, P, m.ncell, m.nface, conv.nq_face, nb, args.config)
+
+    # the other form on the same problem, same dt and steps from the same initial state
+    forms = {args.precision: {"value": value, "ms_per_step": ms / args.steps, "schedule": schedule}}
+    if args.precision == "mixed" and not args.no_compare:
+        f64 = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf, precision="fp64",
+                                 device=local)
+        f64.set_state(U0)
+        ms64, _ = time_steps(f64, dt, args.warmup, args.steps, dist, torch, launch_count)
+        kt64 = f64.ssprk3_timed(dt, 3)
+        forms["fp64"] = {"value": dof_stage_per_step * args.steps * world / (ms64 / 1e3),
+                         "ms_per_step": ms64 / args.steps, "schedule": "two-launch",
+                         "kernels_ms_per_launch": {KNAMES[("fp64", "two-launch")].get(k, str(k)): v[0] / v[1]
+                                                   for k, v in kt64.items()}}
+        # both forms stepped (warmup + steps) from U0 with the same dt: compare the states
+        err = problems.l2_errors(m, P, U_head, Uref=f64.get_state())
+        forms["mixed"]["l2_vs_fp64"] = {"rho": float(err[0]), "rhou": float(err[1]), "rhov": float(err[2]),
+                                        "rhow": float(err[3]), "E": float(err[4]),
+                                        "after_steps": args.warmup + args.steps}
+        forms["mixed_over_fp64"] = forms["mixed"]["value"] / forms["fp64"]["value"]
+        f64.close()
+    cons = conv.conservation()
 
     # end to end through the public API: H2D of the state from pinned memory, one SSP-RK3 step,
     # D2H of the result, every step
-    pinned = torch.empty(conv.shape, dtype=torch.float64, pin_memory=True)
-    pinned.numpy()[:] = conv.get_state()
-    host = pinned.numpy()
-    k_e2e = max(3, min(args.steps, 20))
-    from fve_dg_b200 import _lib as L
-    lib = L.lib()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(k_e2e):
-        L.check(lib.dg_set_state(conv._ctx, L.dptr(host), 0), "dg_set_state")
-        L.check(lib.dg_ssprk3_graph(conv._ctx, float(dt), 1), "dg_ssprk3_graph")
-        L.check(lib.dg_get_state(conv._ctx, L.dptr(host), 0), "dg_get_state")
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    state_bytes = int(np.prod(conv.shape)) * 8
-    e2e = {"value": dof_stage_per_step * k_e2e * world / e2e_s, "unit": "DOF-stage/s",
-           "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes, "steps": k_e2e}
+    e2e = time_e2e(conv, dt, args.steps, dof_stage_per_step, world, dist, torch)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -333,18 +313,194 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3/f32/f64",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "bf16x3 contractions, f32 flux, f64 state",
                 "data": "synthetic",
                 "config": {"workload": args.config, "desc": cfg["desc"], "precision": args.precision,
-                           "tets": m.ncell, "order": P, "dof_per_stage": 5 * nb * m.ncell,
-                           "l2": "state larger than L2 (no flush needed)",
+                           "schedule": schedule, "tets": m.ncell, "order": P, "dof_per_stage": 5 * nb * m.ncell,
+                           "dt": dt, "l2": "state larger than L2 (no flush needed)",
                            "parallelism": f"independent instance per GPU x{world}"},
-                "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "clocks": clocks}
+                "gpu_launches": launches, "roofline": roofline, "forms": forms, "autotune": tune,
+                "conservation": {"mass": cons[0], "energy": cons[4], "kinetic": cons[5]},
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks}
         print(json.dumps(line), flush=True)
     conv.close()
     if dist:
         dist.destroy_process_group()
+
+
+KNAMES = {("fp64", "two-launch"): {0: "face_flux_fp64", 1: "element_fp64"},
+          ("mixed", "two-launch"): {0: "face_flux_mixed", 1: "element_mixed"},
+          ("mixed", "persistent"): {2: "stage_persistent_mixed"}}
+
+
+def time_steps(conv, dt, warmup, steps, dist, torch, launch_count):
+    """Device time of `steps` SSP-RK3 steps (one CUDA graph per step) on the context's stream,
+    after `warmup` steps; barrier and synchronize on both sides, max over ranks."""
+    stream = torch.cuda.ExternalStream(conv.stream)
+    conv.ssprk3(dt, warmup, graph=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    l0 = launch_count()
+    ev0.record(stream)
+    conv.ssprk3(dt, steps, graph=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = launch_count() - l0
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, launches
+
+
+def time_e2e(conv, dt, steps, dof_stage_per_step, world, dist, torch):
+    from fve_dg_b200 import _lib as L
+    pinned = torch.empty(conv.shape, dtype=torch.float64, pin_memory=True)
+    host = pinned.numpy()
+    host[:] = conv.get_state()
+    k = max(3, min(steps, 20))
+    lib = L.lib()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(k):
+        L.check(lib.dg_set_state(conv._ctx, L.dptr(host), 0), "dg_set_state")
+        L.check(lib.dg_ssprk3_graph(conv._ctx, float(dt), 1), "dg_ssprk3_graph")
+        L.check(lib.dg_get_state(conv._ctx, L.dptr(host), 0), "dg_get_state")
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    state_bytes = int(np.prod(conv.shape)) * 8
+    return {"value": dof_stage_per_step * k * world / e2e_s, "unit": "DOF-stage/s",
+            "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes, "steps": k}
+
+
+def make_roofline(kt, precision, schedule, P, ncell, nface, nqf, nb, config):
+    names = KNAMES[(precision, schedule)]
+    peak, peak_kind = read_peaks()
+    dom = max(kt, key=lambda k: kt[k][0])
+    dom_ms = kt[dom][0] / kt[dom][1]
+    name = names.get(dom, str(dom))
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            traffic = json.load(f).get(config, {}).get(name)
+    except Exception:
+        pass
+    b = kernel_bytes(name, P, ncell, nface, nqf)
+    stage_ms = sum(v[0] for v in kt.values()) / kt[dom][1]  # every kernel class launches once per stage
+    ach = b / (dom_ms / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": b, "avg_launch_ms": dom_ms,
+            "stage": {"ms": stage_ms, "bytes_per_dof_stage_min": SURVEY_BYTES_PER_DOF_STAGE[P],
+                      "achieved_gbs_at_min_bytes": SURVEY_BYTES_PER_DOF_STAGE[P] * 5 * nb * ncell
+                      / (stage_ms / 1e3) / 1e9},
+            "kernels_ms_per_launch": {names.get(k, str(k)): v[0] / v[1] for k, v in kt.items()}}
+
+
+def run_ensemble(args, rank, world, local, dist):
+    """64 isentropic-vortex instances on meshes of 8^3..32^3 x 6 tets, P2: the batched mixed form
+    (one persistent launch per RK stage over all instances, a CUDA graph per step, autotuned tiles)
+    against 64 sequential plain FP64 solves. Instances are drawn from one seed per rank."""
+    import torch
+    from fve_dg_b200 import Ensemble, ExplicitConvection, box_mesh, launch_count, problems
+    rng = np.random.default_rng(20261203 + rank)
+    P, qv, qf, L = 2, 1, 2, 10.0
+    meshes, states, lam = [], [], []
+    for i in range(64):
+        n = int(rng.integers(8, 33))
+        beta = float(rng.uniform(1.0, 5.0))
+        center = rng.uniform(0.0, L, 3)
+        axis = rng.normal(size=3)
+        m = box_mesh(n, hi=(L, L, L))
+        U = problems.project(m, P, problems.isentropic_vortex(center=center, axis=axis, beta=beta, period=L))
+        meshes.append(m)
+        states.append(U)
+    singles = []
+    for m, U in zip(meshes, states):
+        c = ExplicitConvection(m, order=P, quad_vol=qv, quad_face=qf, precision="fp64", device=local)
+        c.set_state(U)
+        lam.append(c.max_wave_speed())
+        singles.append(c)
+    dts = np.array([problems.cfl_dt(CFL, L / m.n, P, l) for m, l in zip(meshes, lam)])
+    ens = Ensemble(meshes, order=P, quad_vol=qv, quad_face=qf, precision="mixed", schedule="persistent",
+                   device=local)
+    U0 = np.concatenate(states)
+    ens.set_state(U0)
+    tune = ens.autotune(float(dts.mean()))
+    dofs = 5 * ens.num_basis * ens.ncell * 3
+    stream = torch.cuda.ExternalStream(ens.stream)
+    sampler = ClockSampler(local)
+    sampler.start()
+    ens.ssprk3(dts, args.warmup, graph=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = launch_count()
+    e0.record(stream)
+    ens.ssprk3(dts, args.steps, graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = dofs * args.steps * world / (ms / 1e3)
+    U_batched = ens.get_state()  # after warmup + steps, before the timing pass below
+    kt = ens.ssprk3_timed(float(dts.mean()), 3)
+    # sequential plain FP64 solves of the same instances, same dt and steps
+    torch.cuda.synchronize()
+    ms_seq = 0.0
+    for c, dt in zip(singles, dts):
+        ms_c, _ = time_steps(c, float(dt), args.warmup, args.steps, None, torch, launch_count)
+        ms_seq += ms_c
+    seq_value = dofs * args.steps * world / (ms_seq / 1e3)
+    got = ens.split(U_batched)
+    errs = [problems.l2_errors(m, P, g, Uref=c.get_state()) for m, g, c in zip(meshes, got, singles)]
+    e2e = None
+    pinned = torch.empty(ens.shape, dtype=torch.float64, pin_memory=True)
+    host = pinned.numpy()
+    host[:] = ens.get_state()
+    k = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(k):
+        ens.set_state(host)
+        ens.ssprk3(dts, 1, graph=True)
+        host[:] = ens.get_state()
+    e2e_s = time.perf_counter() - t0
+    sb = int(np.prod(ens.shape)) * 8
+    e2e = {"value": dofs * k * world / e2e_s, "unit": "DOF-stage/s", "h2d_bytes_per_step": sb,
+           "d2h_bytes_per_step": sb, "steps": k,
+           "note": "includes the host-side copies into and out of the numpy state arrays"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16x3 contractions, f32 flux, f64 state", "data": "synthetic",
+                "config": {"workload": "ensemble", "desc": "64 isentropic vortices (strength U[1,5], centres and "
+                           "axes seeded), meshes n^3x6 with n in U{8..32}, P2, Degree4Points11/Degree4Points7, "
+                           "LF, SSP-RK3 CFL 0.3 per instance", "tets": int(ens.ncell), "instances": 64},
+                "gpu_launches": launches,
+                "forms": {"batched_mixed_persistent": {"value": value, "ms_per_step": ms / args.steps},
+                          "sequential_fp64": {"value": seq_value, "ms_per_step": ms_seq / args.steps},
+                          "batched_over_sequential": value / seq_value,
+                          "l2_vs_fp64_max_over_instances": {"rho": float(max(e[0] for e in errs)),
+                                                            "E": float(max(e[4] for e in errs))}},
+                "kernels_ms_per_launch": {KNAMES[("mixed", "persistent")].get(kk, str(kk)): v[0] / v[1]
+                                          for kk, v in kt.items()},
+                "autotune": tune, "e2e": e2e, "clocks": clocks}
+        print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

@@ -4,7 +4,7 @@ equations on affine tetrahedra: a drop-in for the explicit convection path of FV
 
 The compute path is libfvedg_b200.so (hand-written sm_100a CUDA kernels behind the C ABI of
 include/dg_gpu.h). This package is the host-side mirror of the reference interface."""
-from .convection import ExplicitConvection, launch_count  # noqa: F401
+from .convection import Ensemble, ExplicitConvection, launch_count  # noqa: F401
 from .mesh import Mesh, box_mesh  # noqa: F401
 from . import problems  # noqa: F401
 from ._lib import DGError, LIB_PATH  # noqa: F401

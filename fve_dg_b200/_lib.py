@@ -39,7 +39,7 @@ class MeshDesc(ctypes.Structure):
 class Config(ctypes.Structure):
     _fields_ = [("order", ctypes.c_int), ("flux", ctypes.c_int), ("quad_vol", ctypes.c_int),
                 ("quad_face", ctypes.c_int), ("gamma", ctypes.c_double), ("precision", ctypes.c_int),
-                ("device", ctypes.c_int)]
+                ("device", ctypes.c_int), ("schedule", ctypes.c_int)]
 
 
 _lib = None
@@ -65,6 +65,10 @@ def lib():
         "dg_mass": (ctypes.c_int, [vp, c_double_p, ctypes.c_size_t]),
         "dg_ssprk3_timed": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int, c_double_p, ctypes.c_int]),
         "dg_stream": (vp, [vp]),
+        "dg_create_ensemble": (vp, [ctypes.POINTER(MeshDesc), ctypes.c_int, ctypes.POINTER(Config), c_int_p]),
+        "dg_ensemble_offsets": (ctypes.c_int, [vp, c_int64_p]),
+        "dg_ssprk3_ensemble": (ctypes.c_int, [vp, c_double_p, ctypes.c_int, ctypes.c_int]),
+        "dg_autotune": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_char_p, ctypes.c_size_t]),
         "dg_set_dirichlet": (ctypes.c_int, [vp, c_double_p]),
         "dg_conservation": (ctypes.c_int, [vp, c_double_p]),
         "dg_max_wave_speed": (ctypes.c_int, [vp, c_double_p]),
@@ -95,7 +99,8 @@ def lib():
 def exported_symbols():
     """Names this binding expects the library to export."""
     return ["dg_create", "dg_destroy", "dg_residual", "dg_residual_device", "dg_set_state", "dg_get_state",
-            "dg_ssprk3", "dg_ssprk3_graph", "dg_ssprk3_timed", "dg_stream", "dg_mass", "dg_set_dirichlet", "dg_conservation",
+            "dg_ssprk3", "dg_ssprk3_graph", "dg_ssprk3_timed", "dg_stream", "dg_create_ensemble",
+            "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_mass", "dg_set_dirichlet", "dg_conservation",
             "dg_max_wave_speed", "dg_check_state", "dg_info", "dg_mesh_geometry", "dg_face_perms", "dg_basis",
             "dg_quad_rule", "dg_auto_rules", "dg_status_string", "dg_launch_count", "dg_box_mesh_create",
             "dg_box_mesh_destroy", "dg_box_mesh_view"]

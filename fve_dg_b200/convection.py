@@ -20,23 +20,29 @@ from . import _lib as L
 
 FLUX = {"LF": 0, "Roe": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
+SCHEDULE = {"two-launch": 0, "persistent": 1}
 
 
 class ExplicitConvection:
     def __init__(self, mesh, order=3, flux="LF", quad_vol=-1, quad_face=-1, gamma=1.4,
-                 precision="fp64", device=0):
+                 precision="fp64", device=0, schedule="two-launch", _ensemble=None):
         self.mesh = mesh
         self.order = int(order)
         self.flux = flux
         self.gamma = float(gamma)
         self.precision = precision
+        self.schedule = schedule
         cfg = L.Config(order=self.order, flux=FLUX[flux] if isinstance(flux, str) else int(flux),
                        quad_vol=int(quad_vol), quad_face=int(quad_face), gamma=self.gamma,
                        precision=PRECISION[precision] if isinstance(precision, str) else int(precision),
-                       device=int(device))
-        self._desc = mesh.desc()
+                       device=int(device), schedule=SCHEDULE[schedule] if isinstance(schedule, str) else int(schedule))
         err = ctypes.c_int(0)
-        self._ctx = L.lib().dg_create(ctypes.byref(self._desc), ctypes.byref(cfg), ctypes.byref(err))
+        if _ensemble is None:
+            self._desc = mesh.desc()
+            self._ctx = L.lib().dg_create(ctypes.byref(self._desc), ctypes.byref(cfg), ctypes.byref(err))
+        else:
+            self._descs = (L.MeshDesc * len(_ensemble))(*[m.desc() for m in _ensemble])
+            self._ctx = L.lib().dg_create_ensemble(self._descs, len(_ensemble), ctypes.byref(cfg), ctypes.byref(err))
         if not self._ctx:
             raise L.DGError(err.value, "dg_create")
         nb, nqv, nqf, qv, qf = (ctypes.c_int() for _ in range(5))
@@ -57,8 +63,20 @@ class ExplicitConvection:
             pass
 
     @property
+    def ncell(self):
+        return self.mesh.ncell
+
+    @property
     def shape(self):
-        return (self.mesh.ncell, 5 * self.num_basis)
+        return (self.ncell, 5 * self.num_basis)
+
+    def autotune(self, dt):
+        """Time the persistent schedule's tile candidates on the current state (which is restored)
+        and keep the fastest; returns the JSON record of all candidates and the choice."""
+        buf = ctypes.create_string_buffer(1 << 14)
+        L.check(L.lib().dg_autotune(self._ctx, float(dt), buf, len(buf)), "dg_autotune")
+        import json
+        return json.loads(buf.value.decode())
 
     def _state(self, U):
         U = L.as_f64(U)
@@ -139,6 +157,37 @@ class ExplicitConvection:
         if rc not in (L.DG_OK, -5):
             L.check(rc, "dg_check_state")
         return bad.value
+
+
+class Ensemble(ExplicitConvection):
+    """Independent solves on several meshes (of different sizes) in one context: the instances are
+    laid end to end as one disconnected mesh, so each RK stage of all instances is one set of
+    launches. State arrays are the instances' states concatenated in order."""
+
+    def __init__(self, meshes, **kw):
+        self.meshes = list(meshes)
+        offs = np.cumsum([0] + [m.ncell for m in self.meshes])
+        self._offsets = offs
+        super().__init__(_Union(int(offs[-1])), _ensemble=self.meshes, **kw)
+        got = np.zeros(len(self.meshes) + 1, dtype=np.int64)
+        n = L.lib().dg_ensemble_offsets(self._ctx, L.iptr(got))
+        assert n == len(self.meshes) and np.array_equal(got, offs)
+
+    @property
+    def offsets(self):
+        return self._offsets
+
+    def split(self, U):
+        return [U[self._offsets[i]:self._offsets[i + 1]] for i in range(len(self.meshes))]
+
+    def ssprk3(self, dt, nsteps=1, graph=False):
+        dt = L.as_f64(np.broadcast_to(np.asarray(dt, dtype=np.float64), (len(self.meshes),)))
+        L.check(L.lib().dg_ssprk3_ensemble(self._ctx, L.dptr(dt), int(nsteps), int(bool(graph))), "dg_ssprk3_ensemble")
+
+
+class _Union:
+    def __init__(self, ncell):
+        self.ncell = ncell
 
 
 def launch_count():

@@ -6,11 +6,13 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "dg_internal.h"
 #include "dg_kernels_fp64.cuh"
 #include "dg_kernels_mixed.cuh"
+#include "dg_persistent.cuh"
 #include "dg_reduce.cuh"
 
 using namespace fvedg;
@@ -77,6 +79,14 @@ struct dg_ctx {
     std::vector<cudaEvent_t> ev;
     std::vector<int> ev_cls;
     size_t ev_used = 0;
+    // persistent schedule (mixed form): queue state and tile parameters (chosen by dg_autotune)
+    QueueState* d_queue = nullptr;
+    PersistentParams pp;
+    // ensembles: instance element offsets, per-instance dt on the device, instance of each element
+    int ninst = 1;
+    std::vector<int64_t> inst_off;
+    double* d_dt_inst = nullptr;
+    int* d_elem_inst = nullptr;
 };
 
 namespace {
@@ -212,6 +222,8 @@ StageArgs stage_args(dg_ctx* c, const double* U, const double* U0, double* out, 
     a.a1 = a1;
     a.mode = mode;
     a.with_volume = with_volume;
+    a.dt_inst = mode == 1 ? c->d_dt_inst : nullptr;
+    a.elem_inst = c->d_elem_inst;
     return a;
 }
 
@@ -266,10 +278,28 @@ int step_fp64(dg_ctx* c, double dt, cudaStream_t s) {
 
 int step(dg_ctx* c, double dt, cudaStream_t s) {
     if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
-    if (c->cfg.precision == DG_PREC_MIXED)
-        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches,
-                          [&](int cls, auto&& fn) { return timed(c, cls, s, fn); });
+    auto tm = [&](int cls, auto&& fn) { return timed(c, cls, s, fn); };
+    if (c->cfg.precision == DG_PREC_MIXED) {
+        if (c->cfg.schedule == 1)
+            return step_persistent(c->mixed, c->d_queue, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm);
+        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm);
+    }
     return step_fp64(c, dt, s);
+}
+
+int launches_per_step(const dg_ctx* c) {
+    if (c->cfg.precision == DG_PREC_MIXED && c->cfg.schedule == 1) return 3;
+    return 6;
+}
+
+// After a synchronize: the watchdog word of the persistent queue (DG_OK or DG_E_WATCHDOG).
+int check_queue(dg_ctx* c) {
+    if (!c->d_queue) return DG_OK;
+    int err = 0;
+    if (cudaMemcpy(&err, &c->d_queue->error, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return DG_E_CUDA;
+    if (err == DG_OK) return DG_OK;
+    cudaMemset(c->d_queue, 0, sizeof(QueueState));
+    return DG_E_WATCHDOG;
 }
 
 // copy between a host buffer with element stride `stride` and a packed device buffer
@@ -299,6 +329,9 @@ void free_ctx(dg_ctx* c) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     free_mixed(c->mixed);
+    if (c->d_queue) cudaFree(c->d_queue);
+    if (c->d_dt_inst) cudaFree(c->d_dt_inst);
+    if (c->d_elem_inst) cudaFree(c->d_elem_inst);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -323,7 +356,10 @@ const char* dg_status_string(int s) {
 
 int64_t dg_launch_count(void) { return g_launches.load(); }
 
-dg_ctx* dg_create(const dg_mesh_desc* mesh, const dg_config* cfg, int* err) {
+}  // extern "C"
+
+namespace {
+dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, const std::vector<int64_t>* inst_off) {
     auto fail = [&](dg_ctx* c, int e) -> dg_ctx* {
         if (err) *err = e;
         free_ctx(c);
@@ -333,6 +369,7 @@ dg_ctx* dg_create(const dg_mesh_desc* mesh, const dg_config* cfg, int* err) {
     if (cfg->order < 1 || cfg->order > kMaxOrder || !(cfg->gamma > 1.0)) return fail(nullptr, DG_E_ARG);
     if (cfg->flux != DG_FLUX_LF && cfg->flux != DG_FLUX_ROE) return fail(nullptr, DG_E_ARG);
     if (cfg->precision != DG_PREC_FP64 && cfg->precision != DG_PREC_MIXED) return fail(nullptr, DG_E_ARG);
+    if (cfg->schedule != 0 && !(cfg->schedule == 1 && cfg->precision == DG_PREC_MIXED)) return fail(nullptr, DG_E_ARG);
     const int qv = cfg->quad_vol < 0 ? auto_tet_rule(cfg->order) : cfg->quad_vol;
     const int qf = cfg->quad_face < 0 ? auto_tri_rule(cfg->order) : cfg->quad_face;
     if (tet_rule_npts(qv) <= 0 || tri_rule_npts(qf) <= 0) return fail(nullptr, DG_E_ARG);
@@ -388,13 +425,108 @@ dg_ctx* dg_create(const dg_mesh_desc* mesh, const dg_config* cfg, int* err) {
         (rc = dev_alloc(&c->d_Ua, nstate)) || (rc = dev_alloc(&c->d_Ub, nstate)) ||
         (rc = dev_alloc(&c->d_red, (size_t)kRedBlocks * 8)) || (rc = dev_alloc(&c->d_red_out, 8)))
         return fail(c, rc);
+    if (inst_off && inst_off->size() >= 2) {
+        c->ninst = (int)inst_off->size() - 1;
+        c->inst_off = *inst_off;
+        std::vector<int> inst(c->ncell);
+        for (int i = 0; i < c->ninst; ++i)
+            for (int64_t e = (*inst_off)[i]; e < (*inst_off)[i + 1]; ++e) inst[e] = i;
+        std::vector<double> dts(c->ninst, 0.0);
+        if ((rc = upload(&c->d_elem_inst, inst)) || (rc = upload(&c->d_dt_inst, dts))) return fail(c, rc);
+    }
     if (cfg->precision == DG_PREC_MIXED) {
         rc = init_mixed(c->mixed, c->tab, hgeo, hfi, hef, c->ncell, c->nface, cfg->gamma, cfg->flux, qv, qf,
                         c->d_geo, c->d_fi, c->d_ef, c->d_mass_ref);
         if (rc) return fail(c, rc);
+        c->mixed.dt_inst = c->d_dt_inst;
+        c->mixed.elem_inst = c->d_elem_inst;
+        if (cudaMalloc((void**)&c->d_queue, sizeof(QueueState)) != cudaSuccess) return fail(c, DG_E_NOMEM);
+        if (cudaMemset(c->d_queue, 0, sizeof(QueueState)) != cudaSuccess) return fail(c, DG_E_CUDA);
     }
     if (err) *err = DG_OK;
     return c;
+}
+}  // namespace
+
+extern "C" {
+
+dg_ctx* dg_create(const dg_mesh_desc* mesh, const dg_config* cfg, int* err) {
+    return create_impl(mesh, cfg, err, nullptr);
+}
+
+dg_ctx* dg_create_ensemble(const dg_mesh_desc* meshes, int ninst, const dg_config* cfg, int* err) {
+    if (!meshes || ninst < 1 || !cfg) {
+        if (err) *err = DG_E_ARG;
+        return nullptr;
+    }
+    // lay the instances end to end as one disconnected mesh
+    const bool given = meshes[0].face_natural != nullptr;
+    int64_t nc = 0, nf = 0, np = 0;
+    for (int i = 0; i < ninst; ++i) {
+        const dg_mesh_desc& d = meshes[i];
+        const bool gi = d.face_natural != nullptr;
+        if (gi != given || !d.face_cells || (!gi && (!d.points || !d.cell_nodes || !d.face_nodes))) {
+            if (err) *err = DG_E_ARG;
+            return nullptr;
+        }
+        nc += d.ncell;
+        nf += d.nface;
+        np += d.npts;
+    }
+    std::vector<int64_t> fc(2 * nf), cn, fn, fn1;
+    std::vector<uint8_t> bc(nf, DG_BC_PSEUDO3DZ), per(nf, 0);
+    std::vector<double> pts, nat, nrm, area, invj, detj;
+    if (given) { nat.reserve(18 * nf); nrm.reserve(3 * nf); area.reserve(nf); invj.reserve(9 * nc); detj.reserve(nc); }
+    else { pts.reserve(3 * np); cn.reserve(4 * nc); fn.reserve(3 * nf); fn1.reserve(3 * nf); }
+    std::vector<int64_t> off(1, 0);
+    int64_t co = 0, fo = 0, po = 0;
+    for (int i = 0; i < ninst; ++i) {
+        const dg_mesh_desc& d = meshes[i];
+        for (int64_t f = 0; f < d.nface; ++f) {
+            fc[2 * (fo + f)] = d.face_cells[2 * f] + co;
+            fc[2 * (fo + f) + 1] = d.face_cells[2 * f + 1] == DG_NO_CELL ? DG_NO_CELL : d.face_cells[2 * f + 1] + co;
+            if (d.face_bc) bc[fo + f] = d.face_bc[f];
+            if (d.face_periodic) per[fo + f] = d.face_periodic[f];
+        }
+        if (given) {
+            nat.insert(nat.end(), d.face_natural, d.face_natural + 18 * d.nface);
+            nrm.insert(nrm.end(), d.face_normal, d.face_normal + 3 * d.nface);
+            area.insert(area.end(), d.face_area, d.face_area + d.nface);
+            invj.insert(invj.end(), d.cell_invjac, d.cell_invjac + 9 * d.ncell);
+            detj.insert(detj.end(), d.cell_detj, d.cell_detj + d.ncell);
+        } else {
+            pts.insert(pts.end(), d.points, d.points + 3 * d.npts);
+            for (int64_t k = 0; k < 4 * d.ncell; ++k) cn.push_back(d.cell_nodes[k] + po);
+            for (int64_t k = 0; k < 3 * d.nface; ++k) {
+                fn.push_back(d.face_nodes[k] + po);
+                fn1.push_back((d.face_nodes1 ? d.face_nodes1[k] : d.face_nodes[k]) + po);
+            }
+        }
+        co += d.ncell;
+        fo += d.nface;
+        po += d.npts;
+        off.push_back(co);
+    }
+    dg_mesh_desc u{};
+    u.ncell = nc;
+    u.nface = nf;
+    u.face_cells = fc.data();
+    u.face_bc = bc.data();
+    if (given) {
+        u.face_natural = nat.data(); u.face_normal = nrm.data(); u.face_area = area.data();
+        u.cell_invjac = invj.data(); u.cell_detj = detj.data();
+    } else {
+        u.npts = np; u.points = pts.data(); u.cell_nodes = cn.data(); u.face_nodes = fn.data();
+        u.face_nodes1 = fn1.data(); u.face_periodic = per.data();
+    }
+    return create_impl(&u, cfg, err, &off);
+}
+
+int dg_ensemble_offsets(const dg_ctx* c, int64_t* elem_offsets) {
+    if (!c || !elem_offsets) return DG_E_ARG;
+    if (c->inst_off.empty()) { elem_offsets[0] = 0; elem_offsets[1] = c->ncell; return 1; }
+    for (size_t i = 0; i < c->inst_off.size(); ++i) elem_offsets[i] = c->inst_off[i];
+    return c->ninst;
 }
 
 void dg_destroy(dg_ctx* c) {
@@ -460,7 +592,8 @@ int dg_ssprk3(dg_ctx* c, double dt, int nsteps) {
         int rc = step(c, dt, c->stream);
         if (rc) return rc;
     }
-    return cuda_ok(cudaStreamSynchronize(c->stream));
+    DG_CUDA(cudaStreamSynchronize(c->stream));
+    return check_queue(c);
 }
 
 int dg_ssprk3_graph(dg_ctx* c, double dt, int nsteps) {
@@ -481,12 +614,24 @@ int dg_ssprk3_graph(dg_ctx* c, double dt, int nsteps) {
         if (ce != cudaSuccess) { c->graph = nullptr; return DG_E_CUDA; }
         c->graph_dt = dt;
     }
-    const int per_step = c->cfg.precision == DG_PREC_MIXED ? mixed_launches_per_step(c->mixed) : 6;
+    const int per_step = launches_per_step(c);
     for (int i = 0; i < nsteps; ++i) {
         DG_CUDA(cudaGraphLaunch(c->graph, c->stream));
         g_launches += per_step;
     }
-    return cuda_ok(cudaStreamSynchronize(c->stream));
+    DG_CUDA(cudaStreamSynchronize(c->stream));
+    return check_queue(c);
+}
+
+int dg_ssprk3_ensemble(dg_ctx* c, const double* dt, int nsteps, int use_graph) {
+    if (!c || !dt || nsteps < 0) return DG_E_ARG;
+    if (!c->d_dt_inst) return DG_E_STATE;
+    for (int i = 0; i < c->ninst; ++i)
+        if (!(dt[i] >= 0)) return DG_E_ARG;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    DG_CUDA(cudaMemcpyAsync(c->d_dt_inst, dt, sizeof(double) * c->ninst, cudaMemcpyHostToDevice, c->stream));
+    // the kernels read the per-instance dt from device memory; the uniform dt argument is unused
+    return use_graph ? dg_ssprk3_graph(c, 0.0, nsteps) : dg_ssprk3(c, 0.0, nsteps);
 }
 
 void* dg_stream(dg_ctx* c) { return c ? (void*)c->stream : nullptr; }
@@ -502,6 +647,7 @@ int dg_ssprk3_timed(dg_ctx* c, double dt, int nsteps, double* out, int nclass) {
     c->timing = false;
     if (rc) return rc;
     DG_CUDA(cudaStreamSynchronize(c->stream));
+    if ((rc = check_queue(c))) return rc;
     for (int k = 0; k < 2 * nclass; ++k) out[k] = 0.0;
     for (size_t i = 0; i + 1 < c->ev_used; i += 2) {
         float ms = 0.f;
@@ -510,6 +656,64 @@ int dg_ssprk3_timed(dg_ctx* c, double dt, int nsteps, double* out, int nclass) {
         if (k < nclass) { out[2 * k] += ms; out[2 * k + 1] += 1.0; }
     }
     return DG_OK;
+}
+
+int dg_autotune(dg_ctx* c, double dt, char* report, size_t len) {
+    if (!c || !(dt >= 0)) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    if (c->cfg.precision != DG_PREC_MIXED || c->cfg.schedule != 1) return DG_E_ARG;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    const size_t nstate = (size_t)c->ncell * 5 * c->tab.nb;
+    double* save = nullptr;
+    if (dev_alloc(&save, nstate)) return DG_E_NOMEM;
+    DG_CUDA(cudaMemcpyAsync(save, c->d_Un, nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    static const int cand[][3] = {{4, 2, 0},  {8, 4, 0},  {16, 8, 0},  {32, 16, 0}, {64, 32, 0},
+                                  {16, 4, 0}, {32, 8, 0}, {8, 4, 1},   {16, 8, 1},  {32, 16, 1}};
+    const int ncand = (int)(sizeof(cand) / sizeof(cand[0]));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::string js = "{\"order\": " + std::to_string(c->cfg.order) + ", \"quad_vol\": " + std::to_string(c->qv) +
+                     ", \"quad_face\": " + std::to_string(c->qf) + ", \"ncell\": " + std::to_string(c->ncell) +
+                     ", \"face_groups\": " + std::to_string(c->mixed.nfgroups) +
+                     ", \"element_groups\": " + std::to_string(c->mixed.negroups) + ", \"candidates\": [";
+    float best = 1e30f;
+    PersistentParams bestp = c->pp;
+    int rc = DG_OK;
+    for (int i = 0; i < ncand && rc == DG_OK; ++i) {
+        c->pp.tile_f = cand[i][0];
+        c->pp.tile_e = cand[i][1];
+        c->pp.max_blocks = cand[i][2];
+        rc = step(c, dt, c->stream);  // warm-up
+        cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < 2 && rc == DG_OK; ++r) rc = step(c, dt, c->stream);
+        cudaEventRecord(e1, c->stream);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = DG_E_CUDA;
+        if (rc == DG_OK) rc = check_queue(c);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms *= 0.5f;
+        js += std::string(i ? ", " : "") + "{\"tile_f\": " + std::to_string(cand[i][0]) + ", \"tile_e\": " +
+              std::to_string(cand[i][1]) + ", \"max_blocks_per_sm\": " + std::to_string(cand[i][2]) +
+              ", \"ms_per_step\": " + std::to_string(ms) + "}";
+        if (rc == DG_OK && ms < best) { best = ms; bestp = c->pp; }
+    }
+    c->pp = bestp;
+    js += "], \"chosen\": {\"tile_f\": " + std::to_string(bestp.tile_f) + ", \"tile_e\": " +
+          std::to_string(bestp.tile_e) + ", \"max_blocks_per_sm\": " + std::to_string(bestp.max_blocks) +
+          ", \"ms_per_step\": " + std::to_string(best) + "}}";
+    cudaMemcpyAsync(c->d_Un, save, nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(save);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    if (report && len > 0) {
+        const size_t n = std::min(len - 1, js.size());
+        std::memcpy(report, js.data(), n);
+        report[n] = 0;
+    }
+    return rc;
 }
 
 int dg_mass(dg_ctx* c, double* mass, size_t stride) {

@@ -45,6 +45,8 @@ struct StageArgs {
     double dt, a0, a1;    // out = a0 * U0 + a1 * (U + dt * (-R / b))
     int mode;             // 0 = store R, 1 = RK stage
     int with_volume;      // 0 skips the volume term (eval_internals / eval_boundarys only)
+    const double* dt_inst;  // optional per-instance time step (ensembles), indexed by elem_inst
+    const int* elem_inst;   // [ncell] instance of each element
 };
 
 struct FaceArgs {
@@ -198,10 +200,11 @@ __global__ void __launch_bounds__(256) element_fp64(StageArgs a) {
             const double ib = 1.0 / (__ldg(a.geo + (int64_t)ge * 10 + 9) * __ldg(a.mass_ref + j));
             const double* u0 = a.U0 + (int64_t)ge * 5 * NB + 5 * j;
             const double* us = sC + e * 5 * NB + 5 * j;
+            const double dt = a.dt_inst ? __ldg(a.dt_inst + __ldg(a.elem_inst + ge)) : a.dt;
             #pragma unroll
             for (int k = 0; k < 5; ++k) {
                 const double L = -acc[k] * ib;
-                o[k] = a.a0 * u0[k] + a.a1 * (us[k] + a.dt * L);
+                o[k] = a.a0 * u0[k] + a.a1 * (us[k] + dt * L);
             }
         }
     }
@@ -383,8 +386,9 @@ __global__ void __launch_bounds__(NT) element_fp64_fixed(StageArgs a) {
             const double ib = 1.0 / (__ldg(a.geo + (int64_t)ge * 10 + 9) * __ldg(a.mass_ref + j));
             const double* u0 = a.U0 + (int64_t)ge * B5 + 5 * j;
             const double* us = sC + e * B5 + 5 * j;
+            const double dt = a.dt_inst ? __ldg(a.dt_inst + __ldg(a.elem_inst + ge)) : a.dt;
             #pragma unroll
-            for (int k = 0; k < 5; ++k) o[k] = a.a0 * u0[k] + a.a1 * (us[k] + a.dt * (-acc[k] * ib));
+            for (int k = 0; k < 5; ++k) o[k] = a.a0 * u0[k] + a.a1 * (us[k] + dt * (-acc[k] * ib));
         }
     }
 }

@@ -89,6 +89,8 @@ struct MixedElemArgs {
     double dt, a0, a1;
     int mode;
     int with_volume;
+    const double* dt_inst;  // optional per-instance time step (ensembles), indexed by elem_inst
+    const int* elem_inst;   // [ncell] instance of each element
 };
 
 __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo_k, __nv_bfloat16 hi_k) {
@@ -146,13 +148,17 @@ __device__ __forceinline__ void mma3_b(float acc[4], const uint32_t ah[4], const
 
 // One warp per face group: trace deviations of each side for the three faces (rows (face, var))
 // on the tensor cores, then one lane per face point adds c_0 and evaluates the FP32 flux.
-template <int NB, int NQF, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
+template <int NQF>
+struct FaceMixedSmem {
+    float sU[2][16][pad8(NQF) + 1];
+};
+
+template <int NB, int NQF>
+__device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi, FaceMixedSmem<NQF>& sm, int lane) {
     constexpr int KB = pad16(NB - 1), MF = pad8(NQF);
-    __shared__ float sU[WARPS][2][16][MF + 1];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto& sU = sm.sU;
     const int gid = lane >> 2, tig = lane & 3;
-    for (int gi = blockIdx.x * WARPS + warp; gi < a.ngroups; gi += gridDim.x * WARPS) {
+    {
         const FaceGroup grp = a.groups[gi];
         const FaceInfo f0 = a.fi[grp.f[0]];  // shares perms and kind with the others
         const int perm[2] = {f0.meta & 0xff, (f0.meta >> 8) & 0xff};
@@ -169,7 +175,7 @@ __global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
                 a.Fmean[(int64_t)grp.f[i / 5] * 5 + i % 5] = 0.0;
                 a.S0[(int64_t)grp.f[i / 5] * 5 + i % 5] = 0.0;
             }
-            continue;
+            return;
         }
         const int nside = interior ? 2 : 1;
         for (int s = 0; s < nside; ++s) {
@@ -193,10 +199,10 @@ __global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
                 float acc[4] = {0.f, 0.f, 0.f, 0.f};
                 #pragma unroll
                 for (int kt = 0; kt < KB / 16; ++kt) mma3_b(acc, ah[kt], al[kt], th, tl, KB, nt, kt, lane);
-                sU[warp][s][gid][nt * 8 + tig * 2] = acc[0];
-                sU[warp][s][gid][nt * 8 + tig * 2 + 1] = acc[1];
-                sU[warp][s][gid + 8][nt * 8 + tig * 2] = acc[2];
-                sU[warp][s][gid + 8][nt * 8 + tig * 2 + 1] = acc[3];
+                sU[s][gid][nt * 8 + tig * 2] = acc[0];
+                sU[s][gid][nt * 8 + tig * 2 + 1] = acc[1];
+                sU[s][gid + 8][nt * 8 + tig * 2] = acc[2];
+                sU[s][gid + 8][nt * 8 + tig * 2 + 1] = acc[3];
             }
         }
         __syncwarp();
@@ -207,11 +213,11 @@ __global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
             const double* cL = a.U + (int64_t)fi.c0 * (5 * NB);
             float UL[5], UR[5];
             #pragma unroll
-            for (int k = 0; k < 5; ++k) UL[k] = (float)(__ldg(cL + k) + (double)sU[warp][0][fl * 5 + k][g]);
+            for (int k = 0; k < 5; ++k) UL[k] = (float)(__ldg(cL + k) + (double)sU[0][fl * 5 + k][g]);
             if (interior) {
                 const double* cR = a.U + (int64_t)fi.c1 * (5 * NB);
                 #pragma unroll
-                for (int k = 0; k < 5; ++k) UR[k] = (float)(__ldg(cR + k) + (double)sU[warp][1][fl * 5 + k][g]);
+                for (int k = 0; k < 5; ++k) UR[k] = (float)(__ldg(cR + k) + (double)sU[1][fl * 5 + k][g]);
             } else if (bc == 0) {
                 const double* ud = a.UD + ((int64_t)f * NQF + g) * 5;
                 #pragma unroll
@@ -231,14 +237,14 @@ __global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
             for (int k = 0; k < 5; ++k) o[k] = Fh[k] * jw;
             // side-1 deviations are no longer needed: keep the face flux there for the sums below
             #pragma unroll
-            for (int k = 0; k < 5; ++k) sU[warp][1][fl * 5 + k][g] = Fh[k] * jw;
+            for (int k = 0; k < 5; ++k) sU[1][fl * 5 + k][g] = Fh[k] * jw;
         }
         __syncwarp();
         if (lane < 5 * grp.n) {  // face mean and the exact mode-0 sum, FP64, fixed order
             const int fl = lane / 5, k = lane - 5 * fl;
             double s = 0.0, s0 = 0.0;
             for (int g = 0; g < NQF; ++g) {
-                const double v = (double)sU[warp][1][fl * 5 + k][g];
+                const double v = (double)sU[1][fl * 5 + k][g];
                 s += v;
                 s0 += __ldg(a.t.wf + g) * v;
             }
@@ -247,6 +253,14 @@ __global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
         }
         __syncwarp();
     }
+}
+
+template <int NB, int NQF, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
+    __shared__ FaceMixedSmem<NQF> sm[WARPS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int gi = blockIdx.x * WARPS + warp; gi < a.ngroups; gi += gridDim.x * WARPS)
+        face_group_mixed<NB, NQF>(a, gi, sm[warp], lane);
 }
 
 template <int NB, int NQV, int NQF>
@@ -262,15 +276,13 @@ struct ElemMixedSmem {
 
 // One warp per element group: volume values, FP32 flux, volume integral, the four face integrals,
 // the FP64 mean parts and the FP64 RK stage update.
-template <int NB, int NQV, int NQF, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) element_mixed(MixedElemArgs a) {
+template <int NB, int NQV, int NQF>
+__device__ __forceinline__ void elem_group_mixed(const MixedElemArgs& a, int gi, ElemMixedSmem<NB, NQV, NQF>& sm,
+                                                 int lane) {
     using S = ElemMixedSmem<NB, NQV, NQF>;
     constexpr int KB = pad16(NB - 1), MV = S::MV, MJ = pad8(NB), KV = S::KV, KF = S::KF;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    S& sm = reinterpret_cast<S*>(smem_raw)[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
     const int gid = lane >> 2, tig = lane & 3;
-    for (int gi = blockIdx.x * WARPS + (threadIdx.x >> 5); gi < a.ngroups; gi += gridDim.x * WARPS) {
+    {
         const ElemGroup grp = a.groups[gi];
         const int ne = grp.n;
         const double* coef[3];
@@ -409,12 +421,23 @@ __global__ void __launch_bounds__(WARPS * 32) element_mixed(MixedElemArgs a) {
                     a.out[idx] = R;
                 } else {
                     const double ib = 1.0 / (__ldg(a.geo + (int64_t)grp.e[el] * 10 + 9) * __ldg(a.mass_ref + j));
-                    a.out[idx] = a.a0 * a.U0[idx] + a.a1 * (__ldg(a.U + idx) + a.dt * (-R * ib));
+                    const double dt = a.dt_inst ? __ldg(a.dt_inst + __ldg(a.elem_inst + grp.e[el])) : a.dt;
+                    a.out[idx] = a.a0 * a.U0[idx] + a.a1 * (__ldg(a.U + idx) + dt * (-R * ib));
                 }
             }
         }
         __syncwarp();
     }
+}
+
+template <int NB, int NQV, int NQF, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) element_mixed(MixedElemArgs a) {
+    using S = ElemMixedSmem<NB, NQV, NQF>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    S& sm = reinterpret_cast<S*>(smem_raw)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    for (int gi = blockIdx.x * WARPS + (threadIdx.x >> 5); gi < a.ngroups; gi += gridDim.x * WARPS)
+        elem_group_mixed<NB, NQV, NQF>(a, gi, sm, lane);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -439,6 +462,8 @@ struct MixedData {
     float* Fj = nullptr;
     double* Fmean = nullptr;
     double* S0 = nullptr;
+    const double* dt_inst = nullptr;  // ensembles: per-instance dt (device), else null
+    const int* elem_inst = nullptr;
 };
 
 // X(order, qv, qf, NB, NQV, NQF)
@@ -632,6 +657,7 @@ inline int mixed_launch(MixedData& m, int which, const double* U, const double* 
         ea.U = U; ea.U0 = U0; ea.out = out; ea.Fj = m.Fj; ea.Fmean = m.Fmean; ea.S0 = m.S0; ea.geo = m.geo;
         ea.groups = m.egroups; ea.mass_ref = m.mass_ref; ea.t = m.t; ea.ngroups = m.negroups; ea.gamma = m.gamma;
         ea.dt = dt; ea.a0 = a0; ea.a1 = a1; ea.mode = mode; ea.with_volume = with_volume;
+        ea.dt_inst = m.dt_inst; ea.elem_inst = m.elem_inst;
         const int ge = (int)std::min<int64_t>((m.negroups + WE - 1) / WE, (int64_t)m.sms * 16);
         element_mixed<NB, NQV, NQF, WE><<<ge, WE * 32, smem, s>>>(ea);
     }

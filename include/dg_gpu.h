@@ -100,6 +100,9 @@ typedef struct dg_config {
     double gamma;    /* 1.4 (AirFluxC) or 5/3 (MonatomicFluxC), any value > 1 accepted */
     int precision;   /* dg_precision */
     int device;      /* CUDA device ordinal */
+    int schedule;    /* 0: two launches per RK stage (face fluxes, then elements);
+                        1: one persistent cooperative launch per stage pulling face and element
+                           tiles from work queues (mixed precision only; see dg_autotune) */
 } dg_config;
 
 typedef struct dg_ctx dg_ctx;
@@ -123,6 +126,23 @@ int dg_get_state(dg_ctx* ctx, double* U, size_t elem_stride_bytes);
 int dg_ssprk3(dg_ctx* ctx, double dt, int nsteps);
 /* Capture one SSP-RK3 step in a CUDA graph and replay it nsteps times. */
 int dg_ssprk3_graph(dg_ctx* ctx, double dt, int nsteps);
+
+/* Ensembles of independent solves on meshes of different sizes (new; the reference runs one mesh
+ * per process). The meshes are laid end to end as one disconnected mesh in one context, all with
+ * the same configuration; every stage of every instance then runs in the same launches.
+ * dg_set_state / dg_get_state / dg_conservation act on the concatenated state, instance i owning
+ * elements [offsets[i], offsets[i+1]). */
+dg_ctx* dg_create_ensemble(const dg_mesh_desc* meshes, int ninstances, const dg_config* cfg, int* err);
+/* Writes ninstances + 1 element offsets; returns ninstances (1 for an ordinary context). */
+int dg_ensemble_offsets(const dg_ctx* ctx, int64_t* elem_offsets);
+/* nsteps SSP-RK3 steps with a per-instance time step dt[ninstances]; use_graph replays one CUDA
+ * graph per step (the dt values are read from device memory, so one graph serves any dt). */
+int dg_ssprk3_ensemble(dg_ctx* ctx, const double* dt, int nsteps, int use_graph);
+
+/* Autotuner of the persistent schedule: times each candidate tile shape (face and element groups
+ * per queue ticket, CTAs per SM) on the current state (restored afterwards), keeps the fastest and
+ * writes a JSON record of every candidate and the choice into report[len]. */
+int dg_autotune(dg_ctx* ctx, double dt, char* report, size_t len);
 
 /* Same as dg_ssprk3, with CUDA events around every kernel launch on the context's stream.
  * out[2k] = total milliseconds and out[2k+1] = launch count of kernel class k < nclass
