@@ -58,6 +58,8 @@ def lib():
         "dg_destroy": (None, [vp]),
         "dg_residual": (ctypes.c_int, [vp, c_double_p, c_double_p, ctypes.c_size_t, ctypes.c_double, ctypes.c_int]),
         "dg_residual_device": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, ctypes.c_int, vp]),
+        "dg_residual_device_static": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp]),
+        "dg_static_scratch_capacity": (ctypes.c_int64, []),
         "dg_set_state": (ctypes.c_int, [vp, c_double_p, ctypes.c_size_t]),
         "dg_get_state": (ctypes.c_int, [vp, c_double_p, ctypes.c_size_t]),
         "dg_ssprk3": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
@@ -98,7 +100,8 @@ def lib():
 
 def exported_symbols():
     """Names this binding expects the library to export."""
-    return ["dg_create", "dg_destroy", "dg_residual", "dg_residual_device", "dg_set_state", "dg_get_state",
+    return ["dg_create", "dg_destroy", "dg_residual", "dg_residual_device", "dg_residual_device_static",
+            "dg_static_scratch_capacity", "dg_set_state", "dg_get_state",
             "dg_ssprk3", "dg_ssprk3_graph", "dg_ssprk3_timed", "dg_stream", "dg_create_ensemble",
             "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_mass", "dg_set_dirichlet", "dg_conservation",
             "dg_max_wave_speed", "dg_check_state", "dg_info", "dg_mesh_geometry", "dg_face_perms", "dg_basis",

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -551,6 +552,57 @@ int dg_residual_device(dg_ctx* c, const double* U, double* R, double t, int part
     cudaStream_t s = (cudaStream_t)stream;
     if (c->cfg.precision == DG_PREC_MIXED) return residual_mixed(c->mixed, U, R, part, s, &g_launches);
     return residual_fp64(c, U, R, part, s);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Residual without any allocation: the face-flux scratch lives in a fixed device array of this
+// library instead of the context's buffer. For callers that must not allocate device memory at the
+// point of the call (see dg_residual_device_static in dg_gpu.h).
+// ------------------------------------------------------------------------------------------------
+constexpr size_t kStaticScratchDoubles = (size_t)4 << 20;  // 32 MiB of FP64 face fluxes
+static __device__ __align__(256) double g_static_face_scratch[kStaticScratchDoubles];
+
+namespace {
+std::mutex g_static_mu;
+double* g_static_ptr[64] = {};
+
+// Device address of this device's copy of the array, looked up once per device with that device
+// current (the name is only a host-side stand-in for it).
+int static_scratch(int dev, double** out) {
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (dev < 0 || dev >= 64) return DG_E_ARG;
+    if (!g_static_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_static_face_scratch) != cudaSuccess || !p) return DG_E_CUDA;
+        g_static_ptr[dev] = (double*)p;
+    }
+    *out = g_static_ptr[dev];
+    return DG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int64_t dg_static_scratch_capacity(void) { return (int64_t)kStaticScratchDoubles; }
+
+int dg_residual_device_static(dg_ctx* c, const double* U, double* R, int part, void* stream) {
+    if (!c || !U || !R || part < 0 || part > 3) return DG_E_ARG;
+    if ((size_t)c->nface * c->tab.nqf * 5 > kStaticScratchDoubles) return DG_E_ARG;  // mesh too large
+    if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    double* scratch = nullptr;
+    int rc = static_scratch(c->cfg.device, &scratch);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int mask = part == 0 ? 3 : part == 1 ? 0 : part == 2 ? 1 : 2;
+    FaceArgs fa = face_args(c, U, mask);
+    fa.Fh = scratch;  // every face's entries are written (zeros for faces that contribute nothing)
+    StageArgs sa = stage_args(c, U, U, R, 0, 0.0, 0.0, 0.0, part == 0 || part == 1);
+    sa.Fh = scratch;
+    if ((rc = dispatch_face(c->cfg.order, c->qv, c->qf, fa, s))) return rc;
+    return dispatch_element(c->cfg.order, c->qv, c->qf, sa, s);
 }
 
 int dg_residual(dg_ctx* c, const double* U, double* R, size_t stride, double t, int part) {

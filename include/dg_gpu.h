@@ -120,6 +120,25 @@ int dg_residual(dg_ctx* ctx, const double* U, double* R, size_t elem_stride_byte
 /* Same on device buffers (packed layout), enqueued on `stream` (a cudaStream_t, NULL = default). */
 int dg_residual_device(dg_ctx* ctx, const double* U_dev, double* R_dev, double t, int part, void* stream);
 
+/* Residual on device buffers that allocates nothing. This entry point has no counterpart in the
+ * reference. It is for callers that must not allocate device memory at the point of the call:
+ * code running inside a CUDA stream-capture region or a host callback, where cudaMalloc would
+ * break the capture or deadlock, and frameworks that own all device memory through their own pool
+ * and forbid raw cudaMalloc once set-up is over. Such a caller creates the context at set-up time
+ * and may then call this any number of times.
+ * It computes exactly what dg_residual_device computes with the FP64 kernels, but the face-flux
+ * scratch (nface * nqf * 5 doubles) lives in one fixed device array of this library,
+ * dg_static_scratch_capacity() doubles (32 MiB), that every GPU which loads the library holds
+ * until the process exits. Meshes whose face fluxes do not fit are rejected with DG_E_ARG.
+ * The first call on a device looks up that device's copy of the array (cudaGetSymbolAddress with
+ * the context's device current); make that first call before any stream capture begins.
+ * Every call shares the one array and it keeps the last call's contents; nothing in it has to start
+ * at zero (each call writes every entry it reads). Calls whose kernels overlap on the GPU (on
+ * different streams, or from several contexts on one device) race on the array: serialise them. */
+int dg_residual_device_static(dg_ctx* ctx, const double* U_dev, double* R_dev, int part, void* stream);
+/* Capacity of that array, in doubles. */
+int64_t dg_static_scratch_capacity(void);
+
 /* Device-resident time stepping (the driver loop of VortexRK.cpp:264-271 with SSP-RK3). */
 int dg_set_state(dg_ctx* ctx, const double* U, size_t elem_stride_bytes);
 int dg_get_state(dg_ctx* ctx, double* U, size_t elem_stride_bytes);

@@ -40,10 +40,11 @@ def test_oracle_libraries_export_their_api():
             assert hasattr(r, n), n
 
 
-def test_status_strings():
+def test_status_strings_and_capacity():
     lib = L.lib()
     for code in range(0, -8, -1):
         assert lib.dg_status_string(code)
+    assert lib.dg_static_scratch_capacity() == 4 << 20
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 5])
