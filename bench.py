@@ -133,13 +133,18 @@ def kernel_bytes(name, P, ncell, nface, nqf):
         return state + nface * face_rec + nface * nqf * 5 * 8
     if name == "element_fp64":           # stage state + U^n read, new stage written, face fluxes read
         return 3 * state + ncell * elem_rec + nface * nqf * 5 * 8
-    fj = nface * (nqf * 5 * 4 + 2 * 5 * 8)  # FP32 face fluxes + FP64 face means and mode-0 sums
-    if name == "face_flux_mixed":
+    kf = (nqf + 15) // 16 * 16
+    fj = nface * (5 * kf * 4 + 2 * 5 * 8)  # BF16 hi/lo flux deviations + FP64 face means and mode-0 sums
+    rv = state                             # FP64 volume part of the residual
+    grp = ncell * 76 // 3                  # element-group records
+    if name == "face_flux_mixed":          # state read once, face records, face data written
         return state + nface * face_rec + fj
-    if name == "element_mixed":
-        return 3 * state + ncell * elem_rec + fj
-    if name == "stage_persistent_mixed":  # both phases, the face data round trip included
-        return 3 * state + nface * face_rec + ncell * elem_rec + 2 * fj
+    if name == "volume_mixed":             # state + geometry read, R_v written
+        return state + ncell * 80 + grp + rv
+    if name == "lift_mixed":               # face data + R_v + stage state + U^n read, new stage written
+        return fj + rv + 3 * state + ncell * 8 + grp
+    if name == "stage_persistent_mixed":   # all three phases, each intermediate written and read once
+        return 4 * state + nface * face_rec + ncell * 88 + 2 * grp + 2 * fj + 2 * rv
     return None
 
 
@@ -330,7 +335,7 @@ def main():
 
 
 KNAMES = {("fp64", "two-launch"): {0: "face_flux_fp64", 1: "element_fp64"},
-          ("mixed", "two-launch"): {0: "face_flux_mixed", 1: "element_mixed"},
+          ("mixed", "two-launch"): {0: "face_flux_mixed", 3: "volume_mixed", 1: "lift_mixed"},
           ("mixed", "persistent"): {2: "stage_persistent_mixed"}}
 
 

@@ -283,13 +283,13 @@ int step(dg_ctx* c, double dt, cudaStream_t s) {
     if (c->cfg.precision == DG_PREC_MIXED) {
         if (c->cfg.schedule == 1)
             return step_persistent(c->mixed, c->d_queue, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm);
-        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm);
+        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm, !c->timing);
     }
     return step_fp64(c, dt, s);
 }
 
 int launches_per_step(const dg_ctx* c) {
-    if (c->cfg.precision == DG_PREC_MIXED && c->cfg.schedule == 1) return 3;
+    if (c->cfg.precision == DG_PREC_MIXED) return c->cfg.schedule == 1 ? 3 : mixed_launches_per_step(c->mixed);
     return 6;
 }
 
@@ -623,6 +623,9 @@ int dg_set_state(dg_ctx* c, const double* U, size_t stride) {
     DG_CUDA(cudaSetDevice(c->cfg.device));
     int rc = copy_in(c, c->d_Un, U, stride, c->stream);
     if (rc) return rc;
+    // the mixed form reads U^n's split deviation coefficients from a mirror the steps keep current
+    if (c->cfg.precision == DG_PREC_MIXED && (rc = mixed_mirror(c->mixed, c->d_Un, 0, c->stream, &g_launches)))
+        return rc;
     c->have_state = true;
     return cuda_ok(cudaStreamSynchronize(c->stream));
 }
@@ -755,6 +758,7 @@ int dg_autotune(dg_ctx* c, double dt, char* report, size_t len) {
           std::to_string(bestp.tile_e) + ", \"max_blocks_per_sm\": " + std::to_string(bestp.max_blocks) +
           ", \"ms_per_step\": " + std::to_string(best) + "}}";
     cudaMemcpyAsync(c->d_Un, save, nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    mixed_mirror(c->mixed, c->d_Un, 0, c->stream, &g_launches);
     cudaStreamSynchronize(c->stream);
     cudaFree(save);
     cudaEventDestroy(e0);

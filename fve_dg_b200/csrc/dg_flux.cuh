@@ -11,6 +11,13 @@
 
 namespace fvedg {
 
+// Division and square root: IEEE in FP64 (the plain form's parity), the fast hardware
+// approximations in FP32 (a few ulp; the mixed form's flux is FP32 by design).
+__device__ __forceinline__ double dg_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float dg_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double dg_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float dg_sqrt(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
+
 template <typename T>
 struct Phys {
     static __device__ __forceinline__ T positive(T v) { return v > T(1e-16) ? v : T(1e-16); }
@@ -20,7 +27,7 @@ struct Phys {
     static __device__ __forceinline__ void flux_n(const T U[5], const T n[3], T gm1, T Fn[5], T& rho,
                                                   T vel[3], T& p) {
         rho = positive(U[0]);
-        const T ir = T(1) / rho;
+        const T ir = dg_div(T(1), rho);
         vel[0] = U[1] * ir;
         vel[1] = U[2] * ir;
         vel[2] = U[3] * ir;
@@ -37,7 +44,7 @@ struct Phys {
     // Full 5x3 flux, row = variable, column = direction (EulerPhysicalFlux.cpp:8-18).
     static __device__ __forceinline__ void flux(const T U[5], T gm1, T F[5][3]) {
         const T rho = positive(U[0]);
-        const T ir = T(1) / rho;
+        const T ir = dg_div(T(1), rho);
         const T u = U[1] * ir, v = U[2] * ir, w = U[3] * ir, e = U[4] * ir;
         const T p = gm1 * (rho * e - T(0.5) * rho * (u * u + v * v + w * w));
         F[0][0] = rho * u;         F[0][1] = rho * v;         F[0][2] = rho * w;
@@ -49,8 +56,8 @@ struct Phys {
     }
 
     static __device__ __forceinline__ T wave_speed(T rho, const T vel[3], T p, T gam) {
-        const T c = sqrt(gam * positive(p / rho));
-        return sqrt(vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]) + c;
+        const T c = dg_sqrt(gam * positive(dg_div(p, rho)));
+        return dg_sqrt(vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]) + c;
     }
 
     static __device__ __forceinline__ void lax_friedrichs(const T UL[5], const T UR[5], const T n[3],
@@ -69,15 +76,16 @@ struct Phys {
         const T gm1 = gam - T(1);
         flux_n(UL, n, gm1, FL, rL, uL, pL);
         flux_n(UR, n, gm1, FR, rR, uR, pR);
-        const T HL = (UL[4] + pL) / rL, HR = (UR[4] + pR) / rR;
-        const T sL = sqrt(rL), sR = sqrt(rR), iden = T(1) / (sL + sR);
+        const T HL = dg_div(UL[4] + pL, rL), HR = dg_div(UR[4] + pR, rR);
+        const T sL = dg_sqrt(rL), sR = dg_sqrt(rR), iden = dg_div(T(1), sL + sR);
         T ut[3];
         #pragma unroll
         for (int i = 0; i < 3; ++i) ut[i] = (sL * uL[i] + sR * uR[i]) * iden;
         const T Ht = (sL * HL + sR * HR) * iden;
         const T q2 = ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2];
         const T c2 = positive(gm1 * (Ht - T(0.5) * q2));
-        const T ct = sqrt(c2);
+        const T ct = dg_sqrt(c2);
+        const T ic2 = dg_div(T(1), c2);
         const T rt = sL * sR;
         const T unt = ut[0] * n[0] + ut[1] * n[1] + ut[2] * n[2];
         const T dr = rR - rL, dp = pR - pL;
@@ -87,11 +95,11 @@ struct Phys {
         const T dun = du[0] * n[0] + du[1] * n[1] + du[2] * n[2];
         T l1 = fabs(unt - ct), l2 = fabs(unt), l5 = fabs(unt + ct);
         const T delta = T(0.1) * ct;
-        if (l1 < delta) l1 = (l1 * l1 + delta * delta) / (T(2) * delta);
-        if (l5 < delta) l5 = (l5 * l5 + delta * delta) / (T(2) * delta);
-        const T a1 = (dp - rt * ct * dun) / (T(2) * c2);
-        const T a5 = (dp + rt * ct * dun) / (T(2) * c2);
-        const T a2 = dr - dp / c2;
+        if (l1 < delta) l1 = dg_div(l1 * l1 + delta * delta, T(2) * delta);
+        if (l5 < delta) l5 = dg_div(l5 * l5 + delta * delta, T(2) * delta);
+        const T a1 = (dp - rt * ct * dun) * (T(0.5) * ic2);
+        const T a5 = (dp + rt * ct * dun) * (T(0.5) * ic2);
+        const T a2 = dr - dp * ic2;
         const T w1 = l1 * a1, w5 = l5 * a5, w2 = l2 * a2;
         T D[5];
         D[0] = w1 + w5 + w2;
