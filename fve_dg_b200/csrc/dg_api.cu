@@ -283,7 +283,7 @@ int step(dg_ctx* c, double dt, cudaStream_t s) {
     if (c->cfg.precision == DG_PREC_MIXED) {
         if (c->cfg.schedule == 1)
             return step_persistent(c->mixed, c->d_queue, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm);
-        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm, !c->timing);
+        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm);
     }
     return step_fp64(c, dt, s);
 }

@@ -1,8 +1,9 @@
 // Mixed-precision form of the explicit DG operator.
 //
 // The four dense contractions of a stage run on the tensor cores as BF16 MMAs with FP32
-// accumulation (mma.sync.m16n8k16). Both operands are split into hi + lo BF16 parts and the three
-// products hi*hi + hi*lo + lo*hi are accumulated (about 16 significant bits per product):
+// accumulation (mma.sync m16n8k16, plus an m16n8k8 tail so every K is padded to 8, not 16). Both
+// operands are split into hi + lo BF16 parts and the three products hi*hi + hi*lo + lo*hi are
+// accumulated (about 16 significant bits per product):
 //   face traces      U'(x_g) = sum_{b>=1} phi_b(xi_g^perm) c_b          B = face-map table
 //   volume values    U'(x_g) = sum_{b>=1} phi_b(x_g) c_b                B = volume table
 //   volume integral  R_v[j]  = -sum_{g,d} w_g dphi_j,d(x_g) G'_d(x_g)   B = weighted gradients
@@ -10,19 +11,25 @@
 // The MMA's 16 rows hold (item, variable) pairs of three items (faces or elements) that share their
 // face maps, so one table fragment serves three items. Items are grouped that way on the host.
 //
-// Three kernels per RK stage: face fluxes, volume integrals (independent of the faces, so the two
-// run side by side), and the face integrals with the RK update. The face kernel writes its flux
-// deviations already split into BF16 hi/lo in the order the lift's MMA fragments read them.
+// Two kernels per RK stage. The face kernel interpolates both traces, evaluates the Riemann flux
+// and stores the flux deviations already split and in the element kernel's fragment order. The
+// element kernel does the volume term (values, flux, integral) and the four face integrals into
+// the same accumulators, then the FP64 parts and the RK update, and writes the new stage's split
+// coefficients for the next stage's MMAs.
+//
+// Operands in memory are kept in fragment order ("A rows", "B fragments" below): a lane fetches
+// its MMA registers for one 16-wide K tile, hi and lo, with one 128-bit load.
 //
 // Only deviations go through the tensor cores: the mode-0 coefficient c_0 (phi_0 = 1) is added to
-// the traces exactly; the volume flux is taken relative to the flux of the element mean state and
-// the face flux relative to its face mean, and those references are integrated exactly in FP64
-// against precomputed moments (sum_g w_g dphi_j and sum_g w_g phi_j). The mode-0 face integral
-// is summed in FP64 in one fixed order per face, so both sides receive exactly opposite amounts
-// and the element means (mass, momentum, energy) are conserved to round-off. Large constant
-// backgrounds (the p0 ~ 71 of a Mach 0.1 flow) never meet BF16 rounding. The pointwise flux and
-// the Riemann solvers run in FP32; the RK stage update, the inverse mass and the state are FP64.
-// The terms follow ExplicitConvection.cpp:144-272 one for one.
+// the traces in FP32 after the MMA; the volume flux is taken relative to the flux of the element
+// mean state and the face flux relative to a per-face reference (the physical flux of the
+// cells[0] mean state), and those references are integrated in FP64 against precomputed moments
+// (sum_g w_g dphi_j and sum_g w_g phi_j). The mode-0 face integral of each face is formed once, in
+// the face kernel, so both sides receive exactly opposite amounts and the element means (mass,
+// momentum, energy) are conserved to round-off. Large constant backgrounds (the p0 ~ 71 of a Mach
+// 0.1 flow) never meet BF16 rounding. The pointwise flux and the Riemann solvers run in FP32; the
+// RK stage update, the inverse mass and the state are FP64. The terms follow
+// ExplicitConvection.cpp:144-272 one for one.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -38,19 +45,51 @@
 
 namespace fvedg {
 
-__host__ __device__ constexpr int pad16(int x) { return (x + 15) / 16 * 16; }
 __host__ __device__ constexpr int pad8(int x) { return (x + 7) / 8 * 8; }
+__host__ __device__ constexpr int pad16(int x) { return (x + 15) / 16 * 16; }
+// A shared-memory row stride >= n that is 8 (mod 32) floats: 64-bit accesses of the MMA fragment
+// pattern (8 rows x 4 column pairs) then touch 32 distinct banks per half warp.
+__host__ __device__ constexpr int frag_ld(int n) { return n + ((8 - n % 32) + 32) % 32; }
 
-struct MixedTables {  // device pointers; every table row-major [n][k] (the MMA's B operand)
-    const __nv_bfloat16 *tfa_hi, *tfa_lo;  // [24][MF][KB]   face traces:  n = face point, k = mode-1
-    const __nv_bfloat16 *tva_hi, *tva_lo;  // [MV][KB]       volume values: n = volume point
-    const __nv_bfloat16 *tvp_hi, *tvp_lo;  // [MJ][KV]       volume integral: n = mode, k = (point, dir)
-    const __nv_bfloat16 *tfl_hi, *tfl_lo;  // [24][MJ][KF]   face integral: n = mode, k = face point
-    const double* mv;                      // [NB][3]  sum_g w_g dphi_j
-    const double* mf;                      // [24][NB] sum_g w_g phi_j(xi_g^perm)
-    const double* wf;                      // [NQF]
-    const float* wf32;                     // [NQF]
-    const double* inv_mass;                // [NB] 1 / sum_g w_g phi_j^2
+// K tiling of one contraction: K / 16 full tiles and, when K = 8 (mod 16), one 8-wide tail.
+template <int K>
+struct KTiles {
+    static_assert(K % 8 == 0, "K is padded to a multiple of 8");
+    static constexpr int N16 = K / 16;
+    static constexpr bool TAIL = (K % 16) != 0;
+    static constexpr int NT_U32 = N16 * 128 + (TAIL ? 64 : 0);  // 32-bit words of one n-tile of a B table
+};
+
+// ---- A rows ---------------------------------------------------------------------------------------
+// One MMA row of K values split into BF16 hi/lo, stored as K 32-bit words in fragment order: in a
+// full 16-column tile, lane quad t (columns 2t, 2t+1, 2t+8, 2t+9) owns the 4 words
+// {hi(2t,2t+1), hi(2t+8,2t+9), lo(2t,2t+1), lo(2t+8,2t+9)}; in the 8-column tail, quad t owns
+// {hi(2t,2t+1), lo(2t,2t+1)}. Each word holds the lower column in its low half.
+template <int K>
+__host__ __device__ __forceinline__ int arow_hi_word(int x) {
+    constexpr int N16 = K / 16;
+    const int t = x >> 4;
+    if (t < N16) {
+        const int w = x & 15;
+        return t * 16 + ((w & 7) >> 1) * 4 + (w >> 3);
+    }
+    return N16 * 16 + ((x - N16 * 16) >> 1) * 2;
+}
+template <int K>
+__host__ __device__ __forceinline__ int arow_lo_word(int x) {
+    return arow_hi_word<K>(x) + ((x >> 4) < K / 16 ? 2 : 1);
+}
+
+struct MixedTables {  // device pointers
+    const uint32_t* tfa;     // [24 maps] B fragments of the face traces: n = face point, k = mode - 1
+    const uint32_t* tva;     // B fragments of the volume values: n = volume point, k = mode - 1
+    const uint32_t* tvp;     // B fragments of the volume integral: n = mode, k = (point, dir), w dphi
+    const uint32_t* tfl;     // [24 maps] B fragments of the face integral: n = mode, k = face point, w phi
+    const double* mv;        // [NB][3]  sum_g w_g dphi_j
+    const double* mf;        // [24][NB] sum_g w_g phi_j(xi_g^perm)
+    const float* wf32;       // [NQF] face weights
+    const double* inv_mass;  // [NB] 1 / sum_g w_g phi_j^2
+    double wsum;             // sum_g w_g of the face rule
 };
 
 struct FaceGroup {   // up to three faces with equal (perm0, perm1, kind)
@@ -66,15 +105,13 @@ struct ElemGroup {   // up to three elements with equal face maps in canonical f
 
 struct MixedFaceArgs {
     const double* U;
-    const __nv_bfloat16* mir_hi;  // U's deviation coefficients c_b (b >= 1), split, [ncell][5][KB]
-    const __nv_bfloat16* mir_lo;
+    const uint32_t* mir;    // U's deviation coefficients c_b (b >= 1) as A rows, [ncell][5][KB]
     const FaceInfo* fi;
     const FaceGroup* groups;
     const double* UD;
-    __nv_bfloat16* dev_hi;  // [nface][5][KF] flux deviation from the face mean, 2A * (F - mean)
-    __nv_bfloat16* dev_lo;
-    double* Fmean;          // [nface][5] face mean of 2A * F
-    double* S0;             // [nface][5] sum_g w_g 2A F (the exact mode-0 face integral)
+    uint32_t* dev;          // [nface][5][KF] A rows: 2A F(x_g) - Fref, the element kernel's operand
+    double* Fref;           // [nface][5] reference flux 2A F(c0 of cells[0]) . n
+    double* S0;             // [nface][5] sum_g w_g 2A F (the mode-0 face integral)
     MixedTables t;
     int ngroups;
     float gamma;
@@ -82,149 +119,159 @@ struct MixedFaceArgs {
     int faces_mask;
 };
 
-struct MixedVolArgs {
-    const double* U;
-    const __nv_bfloat16* mir_hi;
-    const __nv_bfloat16* mir_lo;
-    const double* geo;
-    const ElemGroup* groups;
-    double* Rv;             // [ncell][5*NB] volume part of the residual
-    MixedTables t;
-    int ngroups;
-    float gamma;
-};
-
-struct MixedLiftArgs {
+struct MixedElemArgs {
     const double* U;
     const double* U0;
     double* out;
-    const double* Rv;       // null when the volume term is left out (residual parts 2 and 3)
-    const __nv_bfloat16* dev_hi;
-    const __nv_bfloat16* dev_lo;
-    const double* Fmean;
+    const uint32_t* mir;     // U's split deviation coefficients
+    uint32_t* mir_out;       // RK mode: the new stage's split deviation coefficients
+    const uint32_t* dev;     // face flux deviations (written by the face kernel)
+    const double* Fref;
     const double* S0;
-    const double* inv_detj; // [ncell]
+    const double* geo;       // [ncell][10] J^-T row-major, detJ
+    const double* inv_detj;  // [ncell]
     const ElemGroup* groups;
     MixedTables t;
     int ngroups;
+    float gamma;
+    int volume;              // 0: leave the volume term out (residual parts 2 and 3)
     double dt, a0, a1;
-    int mode;
-    const double* dt_inst;  // optional per-instance time step (ensembles), indexed by elem_inst
-    const int* elem_inst;   // [ncell] instance of each element
-    __nv_bfloat16* out_mir_hi;  // RK mode: the new stage's split deviation coefficients
-    __nv_bfloat16* out_mir_lo;
+    int mode;                // 0: out = R; 1: out = a0 U0 + a1 (U - dt M^-1 R)
+    const double* dt_inst;   // optional per-instance time step (ensembles), indexed by elem_inst
+    const int* elem_inst;    // [ncell] instance of each element
 };
 
-__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo_k, __nv_bfloat16 hi_k) {
-    return (uint32_t)__bfloat16_as_ushort(lo_k) | ((uint32_t)__bfloat16_as_ushort(hi_k) << 16);
-}
-
-// x = hi + lo with hi, lo in BF16
-__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-    hi = __float2bfloat16_rn(x);
-    lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-}
-
-__device__ __forceinline__ void mma16816(float d[4], const uint32_t a[4], const uint32_t b[2]) {
+// ---- MMA helpers ----------------------------------------------------------------------------------
+__device__ __forceinline__ void mma16816(float d[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
     asm volatile(
         "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
         "{%0,%1,%2,%3};\n"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ void mma1688(float d[4], const uint32_t a[2], uint32_t b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(b));
 }
 
-// A fragment (16 x 16, row-major) of k-tile kt from a value functor v(row, col) -> float, split.
-template <class V>
-__device__ __forceinline__ void build_a(V v, int kt, int lane, uint32_t ah[4], uint32_t al[4]) {
-    const int gid = lane >> 2, tig = lane & 3;
-    __nv_bfloat16 h[8], l[8];
+__device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
+
+// (x0, x1) = hi + lo, both pairs packed BF16 (x0 in the low half)
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+    hi = bf2_bits(h);
+    lo = bf2_bits(__floats2bfloat162_rn(x0 - __low2float(h), x1 - __high2float(h)));
+}
+__device__ __forceinline__ void split1(float x, unsigned short& hi, unsigned short& lo) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(__float2bfloat16_rn(x - __bfloat162float(h)));
+}
+
+// A operand registers of a K-wide contraction (per full tile: the 4 hi and 4 lo MMA registers).
+template <int K>
+struct AFrag {
+    static constexpr int N = KTiles<K>::N16 > 0 ? KTiles<K>::N16 : 1;
+    uint32_t h[N][4], l[N][4];
+    uint32_t th[2], tl[2];
+};
+
+// Rows gid and gid + 8 from A rows in global memory (null: a zero row). `Coherent` reads through
+// L2 only, for data written earlier in the same launch (the persistent schedule).
+template <int K, bool Coherent>
+__device__ __forceinline__ void load_afrag(AFrag<K>& A, const uint32_t* r0, const uint32_t* r1, int lane,
+                                           uint32_t flip = 0u) {
+    const int tq = lane & 3;
     #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const int row = gid + ((r >> 1) & 1) * 8;
-        const int col = kt * 16 + tig * 2 + (r & 1) + (r >> 2) * 8;
-        split_bf16(v(row, col), h[r], l[r]);
+    for (int t = 0; t < KTiles<K>::N16; ++t) {
+        uint4 v0 = make_uint4(0u, 0u, 0u, 0u), v1 = v0;
+        if (r0) v0 = Coherent ? __ldcg(reinterpret_cast<const uint4*>(r0 + t * 16 + tq * 4))
+                              : __ldg(reinterpret_cast<const uint4*>(r0 + t * 16 + tq * 4));
+        if (r1) v1 = Coherent ? __ldcg(reinterpret_cast<const uint4*>(r1 + t * 16 + tq * 4))
+                              : __ldg(reinterpret_cast<const uint4*>(r1 + t * 16 + tq * 4));
+        A.h[t][0] = v0.x ^ flip; A.h[t][1] = v1.x ^ flip; A.h[t][2] = v0.y ^ flip; A.h[t][3] = v1.y ^ flip;
+        A.l[t][0] = v0.z ^ flip; A.l[t][1] = v1.z ^ flip; A.l[t][2] = v0.w ^ flip; A.l[t][3] = v1.w ^ flip;
     }
+    if constexpr (KTiles<K>::TAIL) {
+        constexpr int o = KTiles<K>::N16 * 16;
+        uint2 u0 = make_uint2(0u, 0u), u1 = u0;
+        if (r0) u0 = Coherent ? __ldcg(reinterpret_cast<const uint2*>(r0 + o + tq * 2))
+                              : __ldg(reinterpret_cast<const uint2*>(r0 + o + tq * 2));
+        if (r1) u1 = Coherent ? __ldcg(reinterpret_cast<const uint2*>(r1 + o + tq * 2))
+                              : __ldg(reinterpret_cast<const uint2*>(r1 + o + tq * 2));
+        A.th[0] = u0.x ^ flip; A.th[1] = u1.x ^ flip;
+        A.tl[0] = u0.y ^ flip; A.tl[1] = u1.y ^ flip;
+    }
+}
+
+// acc += A(full tile t) * B(n-tile at tbn, tile t): three products
+__device__ __forceinline__ void mma3_tile(float acc[4], const uint32_t h[4], const uint32_t l[4], const uint32_t* tbn,
+                                          int t, int lane) {
+    const uint4 b = __ldg(reinterpret_cast<const uint4*>(tbn + t * 128 + lane * 4));
+    mma16816(acc, h, b.x, b.y);
+    mma16816(acc, h, b.z, b.w);
+    mma16816(acc, l, b.x, b.y);
+}
+template <int K>
+__device__ __forceinline__ void mma3_tail(float acc[4], const uint32_t h[2], const uint32_t l[2], const uint32_t* tbn,
+                                          int lane) {
+    const uint2 b = __ldg(reinterpret_cast<const uint2*>(tbn + KTiles<K>::N16 * 128 + lane * 2));
+    mma1688(acc, h, b.x);
+    mma1688(acc, h, b.y);
+    mma1688(acc, l, b.x);
+}
+
+// acc += A * B(n-tile nt) over the whole K of a fragment-ordered table tb
+template <int K>
+__device__ __forceinline__ void mma_bt(float acc[4], const AFrag<K>& A, const uint32_t* tb, int nt, int lane) {
+    const uint32_t* tbn = tb + nt * KTiles<K>::NT_U32;
     #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        ah[i] = pack_bf16(h[2 * i], h[2 * i + 1]);
-        al[i] = pack_bf16(l[2 * i], l[2 * i + 1]);
-    }
+    for (int t = 0; t < KTiles<K>::N16; ++t) mma3_tile(acc, A.h[t], A.l[t], tbn, t, lane);
+    if constexpr (KTiles<K>::TAIL) mma3_tail<K>(acc, A.th, A.tl, tbn, lane);
 }
 
-// A fragment of k-tile kt straight from a split mirror [item][5][KB]: row r = (slot, var) of the
-// 16 rows reads mirror row base[r / 5] * 5 + r % 5; rows >= nrows are zero.
-template <int KB>
-__device__ __forceinline__ void load_a_mirror(const __nv_bfloat16* hi, const __nv_bfloat16* lo, const int* item,
-                                              int nrows, int kt, int lane, uint32_t ah[4], uint32_t al[4]) {
-    const int gid = lane >> 2, tig = lane & 3;
-    const int r0 = gid, r1 = gid + 8;
-    const bool v0 = r0 < nrows, v1 = r1 < nrows;
-    const int64_t o0 = v0 ? ((int64_t)item[r0 / 5] * 5 + r0 % 5) * KB + kt * 16 + tig * 2 : 0;
-    const int64_t o1 = v1 ? ((int64_t)item[r1 / 5] * 5 + r1 % 5) * KB + kt * 16 + tig * 2 : 0;
-    ah[0] = v0 ? __ldg((const unsigned int*)(hi + o0)) : 0u;
-    ah[1] = v1 ? __ldg((const unsigned int*)(hi + o1)) : 0u;
-    ah[2] = v0 ? __ldg((const unsigned int*)(hi + o0 + 8)) : 0u;
-    ah[3] = v1 ? __ldg((const unsigned int*)(hi + o1 + 8)) : 0u;
-    al[0] = v0 ? __ldg((const unsigned int*)(lo + o0)) : 0u;
-    al[1] = v1 ? __ldg((const unsigned int*)(lo + o1)) : 0u;
-    al[2] = v0 ? __ldg((const unsigned int*)(lo + o0 + 8)) : 0u;
-    al[3] = v1 ? __ldg((const unsigned int*)(lo + o1 + 8)) : 0u;
-}
-
-// Writes the split deviation coefficients of a state into a mirror (after an upload, or for a
-// residual of an arbitrary state): one thread per (element, var, column).
+// Writes the split deviation coefficients of a state as A rows (after an upload, or for a residual
+// of an arbitrary state): one thread per (element, var, column pair).
 template <int NB>
-__global__ void mirror_split(const double* __restrict__ U, __nv_bfloat16* __restrict__ hi,
-                             __nv_bfloat16* __restrict__ lo, int64_t ncell) {
-    constexpr int KB = pad16(NB - 1);
+__global__ void mirror_split(const double* __restrict__ U, uint32_t* __restrict__ mir, int64_t ncell) {
+    constexpr int KB = pad8(NB - 1), NP = KB / 2;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ncell * 5 * KB) return;
-    const int64_t row = i / KB;
-    const int col = (int)(i - row * KB);
+    if (i >= ncell * 5 * NP) return;
+    const int64_t row = i / NP;
+    const int x = 2 * (int)(i - row * NP);
     const int64_t e = row / 5;
     const int k = (int)(row - e * 5);
-    const float v = col + 1 < NB ? (float)U[e * (5 * NB) + 5 * (col + 1) + k] : 0.f;
-    __nv_bfloat16 h, l;
-    split_bf16(v, h, l);
-    hi[i] = h;
-    lo[i] = l;
-}
-
-// acc(16 x 8 tile nt) += A * B(nt, kt) with B read from a row-major [n][k] BF16 table of leading
-// dimension ld; three products hi*hi + hi*lo + lo*hi.
-__device__ __forceinline__ void mma3_b(float acc[4], const uint32_t ah[4], const uint32_t al[4],
-                                       const __nv_bfloat16* Th, const __nv_bfloat16* Tl, int ld, int nt, int kt,
-                                       int lane) {
-    const int gid = lane >> 2, tig = lane & 3;
-    const int off = (nt * 8 + gid) * ld + kt * 16 + tig * 2;
-    uint32_t bh[2], bl[2];
-    bh[0] = __ldg((const unsigned int*)(Th + off));
-    bh[1] = __ldg((const unsigned int*)(Th + off + 8));
-    bl[0] = __ldg((const unsigned int*)(Tl + off));
-    bl[1] = __ldg((const unsigned int*)(Tl + off + 8));
-    mma16816(acc, ah, bh);
-    mma16816(acc, ah, bl);
-    mma16816(acc, al, bh);
+    const double* u = U + e * (5 * NB) + k;
+    const float v0 = x + 1 < NB ? (float)u[5 * (x + 1)] : 0.f;
+    const float v1 = x + 2 < NB ? (float)u[5 * (x + 2)] : 0.f;
+    uint32_t hi, lo;
+    split2(v0, v1, hi, lo);
+    mir[row * KB + arow_hi_word<KB>(x)] = hi;
+    mir[row * KB + arow_lo_word<KB>(x)] = lo;
 }
 
 // ------------------------------------------------------------------------------------------------
 // Face fluxes: one warp per face group. Trace deviations of each side for the three faces (rows
-// (face, var)) on the tensor cores; one lane per face point adds c_0 and evaluates the FP32 flux;
-// then the face mean, the exact mode-0 sum and the split deviations are written.
+// (face, var)) on the tensor cores, c_0 added in FP32; one lane per face point evaluates the FP32
+// Riemann flux and writes 2A F - Fref, split, into the element kernel's A rows; then the mode-0
+// integral of each face.
 // ------------------------------------------------------------------------------------------------
 template <int NQF>
-struct FaceMixedSmem {
-    double sC0[2][3][5];  // mode-0 coefficients of both sides of the three faces
-    float sN[3][4];       // unit normal and 2A of the three faces
-    float sU[2][16][pad8(NQF) + 1];
-    float sFb[3][5];
+struct alignas(16) FaceMixedSmem {
+    static constexpr int MF = pad8(NQF), LD = frag_ld(MF);
+    float sU[2][16][LD];  // traces of side 0 / 1, rows (face, var), cols face point
+    float sC0[2][16];     // c_0 of the rows
+    float sRef[3][5];     // reference flux of each face
+    float sN[3][4];       // unit normal and 2A
 };
 
 template <int NB, int NQF>
 __device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi, FaceMixedSmem<NQF>& sm, int lane) {
-    constexpr int KB = pad16(NB - 1), MF = pad8(NQF), KF = pad16(NQF);
-    auto& sU = sm.sU;
-    const int gid = lane >> 2, tig = lane & 3;
+    using S = FaceMixedSmem<NQF>;
+    constexpr int KB = pad8(NB - 1), MF = S::MF, KF = pad8(NQF);
+    const int gid = lane >> 2, tq = lane & 3;
     const FaceGroup grp = a.groups[gi];
     const FaceInfo f0 = a.fi[grp.f[0]];  // shares perms and kind with the others
     const int perm[2] = {f0.meta & 0xff, (f0.meta >> 8) & 0xff};
@@ -233,47 +280,61 @@ __device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi,
     const bool active = interior ? (a.faces_mask & 1)
                                  : ((a.faces_mask & 2) && ((bc == 0 && a.UD != nullptr) || bc == 5));
     if (!active) {
-        const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
-        for (int i = lane; i < grp.n * 5 * NQF; i += 32) {
-            const int fl = i / (5 * NQF), r = i - fl * 5 * NQF, k = r / NQF, g = r - k * NQF;
-            const int64_t o = ((int64_t)grp.f[fl] * 5 + k) * KF + g;
-            a.dev_hi[o] = z;
-            a.dev_lo[o] = z;
+        for (int i = lane; i < grp.n * 5 * KF; i += 32) {
+            const int fl = i / (5 * KF);
+            a.dev[(int64_t)grp.f[fl] * 5 * KF + (i - fl * 5 * KF)] = 0u;
         }
         for (int i = lane; i < grp.n * 5; i += 32) {
-            a.Fmean[(int64_t)grp.f[i / 5] * 5 + i % 5] = 0.0;
+            a.Fref[(int64_t)grp.f[i / 5] * 5 + i % 5] = 0.0;
             a.S0[(int64_t)grp.f[i / 5] * 5 + i % 5] = 0.0;
         }
         return;
     }
     const int nside = interior ? 2 : 1;
-    if (lane < 3 * nside * 5) {  // per-face data of the point loop, staged once
-        const int s = lane / 15, r = lane - 15 * s, fl = r / 5, k = r - 5 * fl;
-        const FaceInfo& F = a.fi[grp.f[fl]];
-        sm.sC0[s][fl][k] = __ldg(a.U + (int64_t)(s ? F.c1 : F.c0) * (5 * NB) + k);
-        if (s == 0 && k < 4) sm.sN[fl][k] = k < 3 ? (float)F.n[k] : (float)F.jw;
-    }
-    for (int s = 0; s < nside; ++s) {
-        int cell[3];
-        #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const FaceInfo& F = a.fi[grp.f[i]];
-            cell[i] = s ? F.c1 : F.c0;
+    if (lane < 16 * nside) {
+        const int s = lane >> 4, r = lane & 15;
+        float v = 0.f;
+        if (r < 5 * grp.n) {
+            const FaceInfo& F = a.fi[grp.f[r / 5]];
+            v = (float)__ldg(a.U + (int64_t)(s ? F.c1 : F.c0) * (5 * NB) + r % 5);
         }
-        uint32_t ah[KB / 16][4], al[KB / 16][4];
+        sm.sC0[s][r] = v;
+    }
+    if (lane < grp.n) {  // normal, 2A and the reference flux 2A F(c_0 of cells[0]) . n of each face
+        const FaceInfo& F = a.fi[grp.f[lane]];
+        float c0[5], n[3], Fn[5], rho, vel[3], p;
         #pragma unroll
-        for (int kt = 0; kt < KB / 16; ++kt) load_a_mirror<KB>(a.mir_hi, a.mir_lo, cell, 5 * grp.n, kt, lane, ah[kt], al[kt]);
-        const __nv_bfloat16* th = a.t.tfa_hi + perm[s] * MF * KB;
-        const __nv_bfloat16* tl = a.t.tfa_lo + perm[s] * MF * KB;
+        for (int k = 0; k < 5; ++k) c0[k] = (float)__ldg(a.U + (int64_t)F.c0 * (5 * NB) + k);
+        #pragma unroll
+        for (int i = 0; i < 3; ++i) n[i] = (float)F.n[i];
+        const float jw = (float)F.jw;
+        Phys<float>::flux_n(c0, n, a.gamma - 1.f, Fn, rho, vel, p);
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) sm.sRef[lane][k] = Fn[k] * jw;
+        sm.sN[lane][0] = n[0]; sm.sN[lane][1] = n[1]; sm.sN[lane][2] = n[2]; sm.sN[lane][3] = jw;
+    }
+    __syncwarp();
+    for (int s = 0; s < nside; ++s) {
+        const uint32_t* p0 = nullptr;
+        const uint32_t* p1 = nullptr;
+        if (gid < 5 * grp.n) {
+            const FaceInfo& F = a.fi[grp.f[gid / 5]];
+            p0 = a.mir + ((int64_t)(s ? F.c1 : F.c0) * 5 + gid % 5) * KB;
+        }
+        if (gid + 8 < 5 * grp.n) {
+            const FaceInfo& F = a.fi[grp.f[(gid + 8) / 5]];
+            p1 = a.mir + ((int64_t)(s ? F.c1 : F.c0) * 5 + (gid + 8) % 5) * KB;
+        }
+        AFrag<KB> A;
+        load_afrag<KB, false>(A, p0, p1, lane);
+        const uint32_t* tb = a.t.tfa + perm[s] * (MF / 8) * KTiles<KB>::NT_U32;
+        const float c00 = sm.sC0[s][gid], c01 = sm.sC0[s][gid + 8];
         #pragma unroll
         for (int nt = 0; nt < MF / 8; ++nt) {
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            #pragma unroll
-            for (int kt = 0; kt < KB / 16; ++kt) mma3_b(acc, ah[kt], al[kt], th, tl, KB, nt, kt, lane);
-            sU[s][gid][nt * 8 + tig * 2] = acc[0];
-            sU[s][gid][nt * 8 + tig * 2 + 1] = acc[1];
-            sU[s][gid + 8][nt * 8 + tig * 2] = acc[2];
-            sU[s][gid + 8][nt * 8 + tig * 2 + 1] = acc[3];
+            mma_bt<KB>(acc, A, tb, nt, lane);
+            *reinterpret_cast<float2*>(&sm.sU[s][gid][nt * 8 + 2 * tq]) = make_float2(acc[0] + c00, acc[1] + c00);
+            *reinterpret_cast<float2*>(&sm.sU[s][gid + 8][nt * 8 + 2 * tq]) = make_float2(acc[2] + c01, acc[3] + c01);
         }
     }
     __syncwarp();
@@ -282,10 +343,10 @@ __device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi,
         const int f = grp.f[fl];
         float UL[5], UR[5];
         #pragma unroll
-        for (int k = 0; k < 5; ++k) UL[k] = (float)(sm.sC0[0][fl][k] + (double)sU[0][fl * 5 + k][g]);
+        for (int k = 0; k < 5; ++k) UL[k] = sm.sU[0][fl * 5 + k][g];
         if (interior) {
             #pragma unroll
-            for (int k = 0; k < 5; ++k) UR[k] = (float)(sm.sC0[1][fl][k] + (double)sU[1][fl * 5 + k][g]);
+            for (int k = 0; k < 5; ++k) UR[k] = sm.sU[1][fl * 5 + k][g];
         } else if (bc == 0) {
             const double* ud = a.UD + ((int64_t)f * NQF + g) * 5;
             #pragma unroll
@@ -299,37 +360,38 @@ __device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi,
         float Fh[5];
         if (a.flux == 1) Phys<float>::roe(UL, UR, n, a.gamma, Fh);
         else Phys<float>::lax_friedrichs(UL, UR, n, a.gamma, Fh);
-        const float jw = sm.sN[fl][3];
-        // side-1 deviations are no longer needed: keep the face flux there
+        const float jw = sm.sN[fl][3], w = __ldg(a.t.wf32 + g);
+        unsigned short* drow = reinterpret_cast<unsigned short*>(a.dev + (int64_t)f * 5 * KF);
+        const int hw = 2 * arow_hi_word<KF>(g) + (g & 1), lw = 2 * arow_lo_word<KF>(g) + (g & 1);
         #pragma unroll
-        for (int k = 0; k < 5; ++k) sU[1][fl * 5 + k][g] = Fh[k] * jw;
-    }
-    __syncwarp();
-    if (lane < 5 * grp.n) {
-        // face mean (any per-face constant serves as the reference) and the mode-0 integral
-        // sum_g w_g F, in one fixed order: both sides of the face then use the same number, which
-        // is what makes the element means conserved exactly
-        const int fl = lane / 5, k = lane - 5 * fl;
-        float s[2] = {0.f, 0.f}, s0[2] = {0.f, 0.f};
-        #pragma unroll
-        for (int g = 0; g < NQF; ++g) {
-            const float v = sU[1][fl * 5 + k][g];
-            s[g & 1] += v;
-            s0[g & 1] += __ldg(a.t.wf32 + g) * v;
+        for (int k = 0; k < 5; ++k) {
+            const float d = Fh[k] * jw - sm.sRef[fl][k];
+            unsigned short h, l;
+            split1(d, h, l);
+            drow[2 * k * KF + hw] = h;
+            drow[2 * k * KF + lw] = l;
+            sm.sU[0][fl * 5 + k][g] = w * d;  // side 0 is no longer needed: keep w_g d_g for the sums
         }
-        const float mean = (s[0] + s[1]) * (1.f / NQF);
-        a.Fmean[(int64_t)grp.f[fl] * 5 + k] = (double)mean;
-        a.S0[(int64_t)grp.f[fl] * 5 + k] = (double)(s0[0] + s0[1]);
-        sm.sFb[fl][k] = mean;
     }
     __syncwarp();
-    for (int i = lane; i < grp.n * 5 * NQF; i += 32) {  // deviations, split, in [face][var][point] order
-        const int fl = i / (5 * NQF), r = i - fl * 5 * NQF, k = r / NQF, g = r - k * NQF;
-        __nv_bfloat16 h, l;
-        split_bf16(sU[1][fl * 5 + k][g] - sm.sFb[fl][k], h, l);
-        const int64_t o = ((int64_t)grp.f[fl] * 5 + k) * KF + g;
-        a.dev_hi[o] = h;
-        a.dev_lo[o] = l;
+    {   // mode-0 integral sum_g w_g 2A F = Fref sum_g w_g + sum_g w_g d_g, summed in one fixed order
+        // per face: both sides of the face then use the same number, which is what makes the
+        // element means conserved exactly
+        constexpr int NH = (NQF + 1) / 2;
+        const int r = lane >> 1, h = lane & 1;
+        float s = 0.f;
+        if (r < 5 * grp.n) {
+            const int g1 = h ? NQF : NH;
+            for (int g = h ? NH : 0; g < g1; ++g) s += sm.sU[0][r][g];
+        }
+        const float tot = s + __shfl_xor_sync(0xffffffffu, s, 1);
+        if (h == 0 && r < 5 * grp.n) {
+            const int fl = r / 5, k = r - 5 * fl;
+            const int64_t o = (int64_t)grp.f[fl] * 5 + k;
+            const double ref = (double)sm.sRef[fl][k];
+            a.Fref[o] = ref;
+            a.S0[o] = ref * a.t.wsum + (double)tot;
+        }
     }
     __syncwarp();
 }
@@ -343,34 +405,43 @@ __global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// Volume integrals: one warp per element group. Volume values on the tensor cores, FP32 flux,
-// deviations from the flux of the element mean state, the integral on the tensor cores, and the
-// FP64 mean part; writes R_v.
+// Elements: one warp per element group. Volume values on the tensor cores, FP32 flux, deviations
+// from the flux of the element mean state, the volume integral and the four face integrals into
+// one set of accumulators; then the FP64 parts, the RK update and the new stage's A rows.
 // ------------------------------------------------------------------------------------------------
-template <int NB, int NQV>
-struct VolMixedSmem {
-    static constexpr int MV = pad8(NQV), KV = pad16(3 * NQV);
-    double sGb[3][15];               // flux of the element mean state, times detJ J^-T
-    float sJ[3][10];                 // J^-T and detJ, FP32
-    float sU[16][MV + 1];            // volume deviations, rows (element, var), cols point
-    float sG[16][KV + 2];            // G - G(c_0), rows (element, var), cols (point, dir)
+template <int NB, int NQV, int NQF>
+struct alignas(16) ElemMixedSmem {
+    static constexpr int MV = pad8(NQV), KV = pad8(3 * NQV), MJ = pad8(NB);
+    static constexpr int LDU = frag_ld(MV), LDG = frag_ld(KV);
+    static_assert(MJ <= LDU, "the accumulator transpose reuses sU");
+    float sU[16][LDU];    // volume values (c_0 added), rows (element, var), cols point; then R
+    float sG[16][LDG];    // Gb - G, rows (element, var), cols (point, dir); padding columns zero
+    double sGb[3][15];    // detJ F(c_0) J^-T of each element (FP64)
+    double sFr[3][4][5];  // face reference fluxes
+    double sS0[3][5];     // +-sum_q S0 (the mode-0 face integrals, in a fixed order)
+    double sMF[4][NB];    // +-mf of the group's four face maps
+    float sJ[3][10];      // J^-T and detJ
+    float sGbf[3][15];
+    float sC0[16];
 };
 
-template <int NB, int NQV>
-__device__ __forceinline__ void volume_group_mixed(const MixedVolArgs& a, int gi, VolMixedSmem<NB, NQV>& sm, int lane) {
-    using S = VolMixedSmem<NB, NQV>;
-    constexpr int KB = pad16(NB - 1), MV = S::MV, MJ = pad8(NB), KV = S::KV;
-    const int gid = lane >> 2, tig = lane & 3;
-    const ElemGroup grp = a.groups[gi];
+template <int NB, int NQV, int NQF>
+__device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int gi, ElemMixedSmem<NB, NQV, NQF>& sm,
+                                                    int lane) {
+    using S = ElemMixedSmem<NB, NQV, NQF>;
+    constexpr int KB = pad8(NB - 1), MV = S::MV, KV = S::KV, MJ = S::MJ, KF = pad8(NQF), NT = MJ / 8;
+    const int gid = lane >> 2, tq = lane & 3;
+    const ElemGroup& grp = a.groups[gi];  // read in place (a copy would live in local memory)
     const int ne = grp.n;
-    const double* coef[3];
-    #pragma unroll
-    for (int i = 0; i < 3; ++i) coef[i] = a.U + (int64_t)grp.e[i] * (5 * NB);
-    if (lane < ne) {  // G(c_0), FP64
-        const double* geo = a.geo + (int64_t)grp.e[lane] * 10;
+    const int r0 = gid, r1 = gid + 8;
+    const bool v0 = r0 < 5 * ne, v1 = r1 < 5 * ne;
+    if (lane < 16) sm.sC0[lane] = lane < 5 * ne ? (float)__ldg(a.U + (int64_t)grp.e[lane / 5] * (5 * NB) + lane % 5) : 0.f;
+    if (a.volume && lane < ne) {  // G(c_0), FP64
+        const int64_t e = grp.e[lane];
+        const double* geo = a.geo + e * 10;
         double c0[5], F[5][3], J[9];
         #pragma unroll
-        for (int k = 0; k < 5; ++k) c0[k] = __ldg(coef[lane] + k);
+        for (int k = 0; k < 5; ++k) c0[k] = __ldg(a.U + e * (5 * NB) + k);
         #pragma unroll
         for (int i = 0; i < 9; ++i) J[i] = __ldg(geo + i);
         const double dj = __ldg(geo + 9);
@@ -378,194 +449,180 @@ __device__ __forceinline__ void volume_group_mixed(const MixedVolArgs& a, int gi
         #pragma unroll
         for (int k = 0; k < 5; ++k)
             #pragma unroll
-            for (int d = 0; d < 3; ++d)
-                sm.sGb[lane][3 * k + d] = dj * (F[k][0] * J[d] + F[k][1] * J[3 + d] + F[k][2] * J[6 + d]);
+            for (int d = 0; d < 3; ++d) {
+                const double gb = dj * (F[k][0] * J[d] + F[k][1] * J[3 + d] + F[k][2] * J[6 + d]);
+                sm.sGb[lane][3 * k + d] = gb;
+                sm.sGbf[lane][3 * k + d] = (float)gb;
+            }
         #pragma unroll
         for (int i = 0; i < 9; ++i) sm.sJ[lane][i] = (float)J[i];
         sm.sJ[lane][9] = (float)dj;
     }
-    {
-        uint32_t ah[KB / 16][4], al[KB / 16][4];
-        #pragma unroll
-        for (int kt = 0; kt < KB / 16; ++kt) load_a_mirror<KB>(a.mir_hi, a.mir_lo, grp.e, 5 * ne, kt, lane, ah[kt], al[kt]);
-        #pragma unroll
-        for (int nt = 0; nt < MV / 8; ++nt) {
-            float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            #pragma unroll
-            for (int kt = 0; kt < KB / 16; ++kt) mma3_b(acc, ah[kt], al[kt], a.t.tva_hi, a.t.tva_lo, KB, nt, kt, lane);
-            sm.sU[gid][nt * 8 + tig * 2] = acc[0];
-            sm.sU[gid][nt * 8 + tig * 2 + 1] = acc[1];
-            sm.sU[gid + 8][nt * 8 + tig * 2] = acc[2];
-            sm.sU[gid + 8][nt * 8 + tig * 2 + 1] = acc[3];
-        }
-    }
-    __syncwarp();
-    for (int p = lane; p < ne * NQV; p += 32) {
-        const int el = p / NQV, g = p - el * NQV;
-        float U[5], F[5][3];
-        #pragma unroll
-        for (int k = 0; k < 5; ++k) U[k] = (float)(__ldg(coef[el] + k) + (double)sm.sU[el * 5 + k][g]);
-        Phys<float>::flux(U, a.gamma - 1.f, F);
-        const float* J = sm.sJ[el];
-        #pragma unroll
-        for (int k = 0; k < 5; ++k)
-            #pragma unroll
-            for (int d = 0; d < 3; ++d)
-                sm.sG[el * 5 + k][3 * g + d] =
-                    J[9] * (F[k][0] * J[d] + F[k][1] * J[3 + d] + F[k][2] * J[6 + d]) - (float)sm.sGb[el][3 * k + d];
-    }
-    __syncwarp();
-    float accv[MJ / 8][4];
-    #pragma unroll
-    for (int nt = 0; nt < MJ / 8; ++nt)
-        #pragma unroll
-        for (int r = 0; r < 4; ++r) accv[nt][r] = 0.f;
-    #pragma unroll
-    for (int kt = 0; kt < KV / 16; ++kt) {
-        uint32_t ah[4], al[4];
-        build_a([&](int row, int col) { return (row < 5 * ne && col < 3 * NQV) ? sm.sG[row][col] : 0.f; },
-                kt, lane, ah, al);
-        #pragma unroll
-        for (int nt = 0; nt < MJ / 8; ++nt) mma3_b(accv[nt], ah, al, a.t.tvp_hi, a.t.tvp_lo, KV, nt, kt, lane);
-    }
-    #pragma unroll
-    for (int nt = 0; nt < MJ / 8; ++nt) {
-        #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int row = gid + (r >> 1) * 8;
-            const int j = nt * 8 + tig * 2 + (r & 1);
-            if (row >= 5 * ne || j >= NB) continue;
-            const int el = row / 5, k = row - 5 * el;
-            double R = 0.0;  // grad phi_0 = 0
-            if (j > 0) {
-                const double* gb = sm.sGb[el] + 3 * k;
-                const double* mv = a.t.mv + 3 * j;
-                R = -(double)accv[nt][r] - (gb[0] * __ldg(mv) + gb[1] * __ldg(mv + 1) + gb[2] * __ldg(mv + 2));
-            }
-            a.Rv[(int64_t)grp.e[el] * (5 * NB) + 5 * j + k] = R;
-        }
-    }
-    __syncwarp();
-}
-
-template <int NB, int NQV, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) volume_mixed(MixedVolArgs a) {
-    using S = VolMixedSmem<NB, NQV>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    S& sm = reinterpret_cast<S*>(smem_raw)[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    for (int gi = blockIdx.x * WARPS + (threadIdx.x >> 5); gi < a.ngroups; gi += gridDim.x * WARPS)
-        volume_group_mixed<NB, NQV>(a, gi, sm, lane);
-}
-
-// ------------------------------------------------------------------------------------------------
-// Face integrals and the RK update: one warp per element group. The flux deviations arrive split,
-// in fragment order, so the four face integrals are MMAs straight from memory; then the FP64 mean
-// parts, the volume part and the stage combination.
-// ------------------------------------------------------------------------------------------------
-struct LiftMixedSmem {
-    double sFb[3][4][5];   // face means
-    double sS0[3][4][5];   // exact mode-0 face sums
-};
-
-template <int NB, int NQF>
-__device__ __forceinline__ void lift_group_mixed(const MixedLiftArgs& a, int gi, LiftMixedSmem& sm, int lane) {
-    constexpr int MJ = pad8(NB), KF = pad16(NQF);
-    const int gid = lane >> 2, tig = lane & 3;
-    const ElemGroup grp = a.groups[gi];
-    const int ne = grp.n;
     for (int i = lane; i < ne * 20; i += 32) {
         const int el = i / 20, r = i - el * 20, q = r / 5, k = r - 5 * q;
-        const int f = grp.face[el][q];
-        sm.sFb[el][q][k] = __ldcg(a.Fmean + (int64_t)f * 5 + k);
-        sm.sS0[el][q][k] = __ldcg(a.S0 + (int64_t)f * 5 + k);
+        sm.sFr[el][q][k] = __ldcg(a.Fref + (int64_t)grp.face[el][q] * 5 + k);
     }
-    float accf[MJ / 8][4];
-    #pragma unroll
-    for (int nt = 0; nt < MJ / 8; ++nt)
+    if (lane < 5 * ne) {
+        const int el = lane / 5, k = lane - 5 * el;
+        double s = 0.0;
         #pragma unroll
-        for (int r = 0; r < 4; ++r) accf[nt][r] = 0.f;
-    // rows gid and gid + 8 of the A fragments: (element, var) -> the face's deviation row
-    const int r0 = gid, r1 = gid + 8;
-    const int el0 = r0 / 5, k0 = r0 - 5 * el0, el1 = r1 / 5, k1 = r1 - 5 * el1;
-    const bool v0 = r0 < 5 * ne, v1 = r1 < 5 * ne;
+        for (int q = 0; q < 4; ++q) {
+            const double v = __ldcg(a.S0 + (int64_t)grp.face[el][q] * 5 + k);
+            s += (grp.meta[q] >> 8) ? -v : v;
+        }
+        sm.sS0[el][k] = s;
+    }
+    for (int i = lane; i < 4 * NB; i += 32) {
+        const int q = i / NB, j = i - q * NB;
+        const double v = __ldg(a.t.mf + (grp.meta[q] & 0xff) * NB + j);
+        sm.sMF[q][j] = (grp.meta[q] >> 8) ? -v : v;
+    }
+    __syncwarp();
+    float acc[NT][4];
+    #pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+        #pragma unroll
+        for (int r = 0; r < 4; ++r) acc[nt][r] = 0.f;
+    if (a.volume) {
+        {   // values at the volume points
+            AFrag<KB> A;
+            load_afrag<KB, false>(A, v0 ? a.mir + ((int64_t)grp.e[r0 / 5] * 5 + r0 % 5) * KB : nullptr,
+                                  v1 ? a.mir + ((int64_t)grp.e[r1 / 5] * 5 + r1 % 5) * KB : nullptr, lane);
+            const float c00 = sm.sC0[r0], c01 = sm.sC0[r1];
+            #pragma unroll
+            for (int nt = 0; nt < MV / 8; ++nt) {
+                float o[4] = {0.f, 0.f, 0.f, 0.f};
+                mma_bt<KB>(o, A, a.t.tva, nt, lane);
+                *reinterpret_cast<float2*>(&sm.sU[r0][nt * 8 + 2 * tq]) = make_float2(o[0] + c00, o[1] + c00);
+                *reinterpret_cast<float2*>(&sm.sU[r1][nt * 8 + 2 * tq]) = make_float2(o[2] + c01, o[3] + c01);
+            }
+        }
+        __syncwarp();
+        const float gm1 = a.gamma - 1.f;
+        for (int p = lane; p < ne * NQV; p += 32) {
+            const int el = p / NQV, g = p - el * NQV;
+            float U[5], F[5][3];
+            #pragma unroll
+            for (int k = 0; k < 5; ++k) U[k] = sm.sU[el * 5 + k][g];
+            Phys<float>::flux(U, gm1, F);
+            const float* J = sm.sJ[el];
+            #pragma unroll
+            for (int k = 0; k < 5; ++k)
+                #pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    sm.sG[el * 5 + k][3 * g + d] =
+                        sm.sGbf[el][3 * k + d] - J[9] * (F[k][0] * J[d] + F[k][1] * J[3 + d] + F[k][2] * J[6 + d]);
+        }
+        __syncwarp();
+        // volume integral: acc += (Gb - G) * (w dphi), split on the fly
+        #pragma unroll
+        for (int t = 0; t < KTiles<KV>::N16; ++t) {
+            const int c = t * 16 + 2 * tq;
+            uint32_t h[4] = {0u, 0u, 0u, 0u}, l[4] = {0u, 0u, 0u, 0u};
+            if (v0) {
+                const float2 x = *reinterpret_cast<const float2*>(&sm.sG[r0][c]);
+                const float2 y = *reinterpret_cast<const float2*>(&sm.sG[r0][c + 8]);
+                split2(x.x, x.y, h[0], l[0]);
+                split2(y.x, y.y, h[2], l[2]);
+            }
+            if (v1) {
+                const float2 x = *reinterpret_cast<const float2*>(&sm.sG[r1][c]);
+                const float2 y = *reinterpret_cast<const float2*>(&sm.sG[r1][c + 8]);
+                split2(x.x, x.y, h[1], l[1]);
+                split2(y.x, y.y, h[3], l[3]);
+            }
+            #pragma unroll
+            for (int nt = 0; nt < NT; ++nt) mma3_tile(acc[nt], h, l, a.t.tvp + nt * KTiles<KV>::NT_U32, t, lane);
+        }
+        if constexpr (KTiles<KV>::TAIL) {
+            const int c = KTiles<KV>::N16 * 16 + 2 * tq;
+            uint32_t h[2] = {0u, 0u}, l[2] = {0u, 0u};
+            if (v0) {
+                const float2 x = *reinterpret_cast<const float2*>(&sm.sG[r0][c]);
+                split2(x.x, x.y, h[0], l[0]);
+            }
+            if (v1) {
+                const float2 x = *reinterpret_cast<const float2*>(&sm.sG[r1][c]);
+                split2(x.x, x.y, h[1], l[1]);
+            }
+            #pragma unroll
+            for (int nt = 0; nt < NT; ++nt) mma3_tail<KV>(acc[nt], h, l, a.t.tvp + nt * KTiles<KV>::NT_U32, lane);
+        }
+    }
+    // face integrals: the flux deviations arrive split, in fragment order; side 1 negated exactly
     #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int perm = grp.meta[q] & 0xff;
-        const uint32_t flip = (grp.meta[q] >> 8) ? 0x80008000u : 0u;  // exact negation of both halves
-        const int64_t o0 = v0 ? ((int64_t)grp.face[el0][q] * 5 + k0) * KF : 0;
-        const int64_t o1 = v1 ? ((int64_t)grp.face[el1][q] * 5 + k1) * KF : 0;
-        const __nv_bfloat16* th = a.t.tfl_hi + perm * MJ * KF;
-        const __nv_bfloat16* tl = a.t.tfl_lo + perm * MJ * KF;
+        const uint32_t flip = (grp.meta[q] >> 8) ? 0x80008000u : 0u;
+        AFrag<KF> A;
+        load_afrag<KF, true>(A, v0 ? a.dev + ((int64_t)grp.face[r0 / 5][q] * 5 + r0 % 5) * KF : nullptr,
+                             v1 ? a.dev + ((int64_t)grp.face[r1 / 5][q] * 5 + r1 % 5) * KF : nullptr, lane, flip);
+        const uint32_t* tb = a.t.tfl + perm * NT * KTiles<KF>::NT_U32;
         #pragma unroll
-        for (int kt = 0; kt < KF / 16; ++kt) {
-            const int c = kt * 16 + tig * 2;
-            uint32_t ah[4], al[4];
-            ah[0] = v0 ? (__ldcg((const unsigned int*)(a.dev_hi + o0 + c)) ^ flip) : 0u;
-            ah[1] = v1 ? (__ldcg((const unsigned int*)(a.dev_hi + o1 + c)) ^ flip) : 0u;
-            ah[2] = v0 ? (__ldcg((const unsigned int*)(a.dev_hi + o0 + c + 8)) ^ flip) : 0u;
-            ah[3] = v1 ? (__ldcg((const unsigned int*)(a.dev_hi + o1 + c + 8)) ^ flip) : 0u;
-            al[0] = v0 ? (__ldcg((const unsigned int*)(a.dev_lo + o0 + c)) ^ flip) : 0u;
-            al[1] = v1 ? (__ldcg((const unsigned int*)(a.dev_lo + o1 + c)) ^ flip) : 0u;
-            al[2] = v0 ? (__ldcg((const unsigned int*)(a.dev_lo + o0 + c + 8)) ^ flip) : 0u;
-            al[3] = v1 ? (__ldcg((const unsigned int*)(a.dev_lo + o1 + c + 8)) ^ flip) : 0u;
-            #pragma unroll
-            for (int nt = 0; nt < MJ / 8; ++nt) mma3_b(accf[nt], ah, al, th, tl, KF, nt, kt, lane);
-        }
+        for (int nt = 0; nt < NT; ++nt) mma_bt<KF>(acc[nt], A, tb, nt, lane);
+    }
+    __syncwarp();  // sU is free: transpose the accumulators through it
+    #pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+        *reinterpret_cast<float2*>(&sm.sU[r0][nt * 8 + 2 * tq]) = make_float2(acc[nt][0], acc[nt][1]);
+        *reinterpret_cast<float2*>(&sm.sU[r1][nt * 8 + 2 * tq]) = make_float2(acc[nt][2], acc[nt][3]);
     }
     __syncwarp();
-    // epilogue: this lane owns rows (element, var) gid and gid + 8, modes nt*8 + 2 tig (+1)
-    #pragma unroll
-    for (int nt = 0; nt < MJ / 8; ++nt) {
-        #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int row = gid + (r >> 1) * 8;
-            const int j = nt * 8 + tig * 2 + (r & 1);
-            if (row >= 5 * ne || j >= NB) continue;
-            const int el = row / 5, k = row - 5 * el;
-            double R;
-            if (j == 0) {  // only the exact face sums
-                R = 0.0;
-                #pragma unroll
-                for (int q = 0; q < 4; ++q) R += (grp.meta[q] >> 8) ? -sm.sS0[el][q][k] : sm.sS0[el][q][k];
-            } else {
-                R = (double)accf[nt][r];
-                #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const double m = __ldg(a.t.mf + (grp.meta[q] & 0xff) * NB + j) * sm.sFb[el][q][k];
-                    R += (grp.meta[q] >> 8) ? -m : m;
-                }
+    // epilogue over the group's DOFs in memory order (coalesced FP64 traffic)
+    for (int i = lane; i < ne * 5 * NB; i += 32) {
+        const int el = i / (5 * NB), r = i - el * (5 * NB), j = r / 5, k = r - 5 * j;
+        const int e = grp.e[el];
+        double R;
+        if (j == 0) {
+            R = sm.sS0[el][k];  // grad phi_0 = 0: only the exact face sums
+        } else {
+            R = (double)sm.sU[el * 5 + k][j];
+            #pragma unroll
+            for (int q = 0; q < 4; ++q) R += sm.sMF[q][j] * sm.sFr[el][q][k];
+            if (a.volume) {
+                const double* mv = a.t.mv + 3 * j;
+                const double* gb = sm.sGb[el] + 3 * k;
+                R -= gb[0] * __ldg(mv) + gb[1] * __ldg(mv + 1) + gb[2] * __ldg(mv + 2);
             }
-            const int e = grp.e[el];
-            const int64_t idx = (int64_t)e * (5 * NB) + 5 * j + k;
-            if (a.Rv) R += __ldcg(a.Rv + idx);
-            if (a.mode == 0) {
-                a.out[idx] = R;
-            } else {
-                const double ib = __ldg(a.inv_detj + e) * __ldg(a.t.inv_mass + j);
-                const double dt = a.dt_inst ? __ldg(a.dt_inst + __ldg(a.elem_inst + e)) : a.dt;
-                const double un = a.a0 * a.U0[idx] + a.a1 * (__ldg(a.U + idx) + dt * (-R * ib));
-                a.out[idx] = un;
-                if (j > 0) {
-                    constexpr int KBm = pad16(NB - 1);
-                    __nv_bfloat16 h, l;
-                    split_bf16((float)un, h, l);
-                    const int64_t mo = ((int64_t)e * 5 + k) * KBm + (j - 1);
-                    a.out_mir_hi[mo] = h;
-                    a.out_mir_lo[mo] = l;
-                }
+        }
+        const int64_t idx = (int64_t)e * (5 * NB) + r;
+        if (a.mode == 0) {
+            a.out[idx] = R;
+        } else {
+            const double ib = __ldg(a.inv_detj + e) * __ldg(a.t.inv_mass + j);
+            const double dt = a.dt_inst ? __ldg(a.dt_inst + __ldg(a.elem_inst + e)) : a.dt;
+            const double un = a.a0 * a.U0[idx] + a.a1 * (__ldg(a.U + idx) + dt * (-R * ib));
+            a.out[idx] = un;
+            if (j > 0) {
+                unsigned short h, l;
+                split1((float)un, h, l);
+                unsigned short* mrow = reinterpret_cast<unsigned short*>(a.mir_out + ((int64_t)e * 5 + k) * KB);
+                mrow[2 * arow_hi_word<KB>(j - 1) + ((j - 1) & 1)] = h;
+                mrow[2 * arow_lo_word<KB>(j - 1) + ((j - 1) & 1)] = l;
             }
         }
     }
     __syncwarp();
 }
 
-template <int NB, int NQF, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 4) lift_mixed(MixedLiftArgs a) {
-    __shared__ LiftMixedSmem sm[WARPS];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int gi = blockIdx.x * WARPS + warp; gi < a.ngroups; gi += gridDim.x * WARPS)
-        lift_group_mixed<NB, NQF>(a, gi, sm[warp], lane);
+// Columns 3 NQV .. LDG of sG stay zero for the kernel's lifetime (the flux loop never writes them).
+template <int NB, int NQV, int NQF>
+__device__ __forceinline__ void element_smem_init(ElemMixedSmem<NB, NQV, NQF>& sm, int lane) {
+    using S = ElemMixedSmem<NB, NQV, NQF>;
+    constexpr int c0 = 3 * NQV, w = S::LDG - c0;
+    for (int i = lane; i < 16 * w; i += 32) sm.sG[i / w][c0 + i % w] = 0.f;
+    __syncwarp();
+}
+
+template <int NB, int NQV, int NQF, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) element_mixed(MixedElemArgs a) {
+    using S = ElemMixedSmem<NB, NQV, NQF>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    S& sm = reinterpret_cast<S*>(smem_raw)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    element_smem_init(sm, lane);
+    for (int gi = blockIdx.x * WARPS + (threadIdx.x >> 5); gi < a.ngroups; gi += gridDim.x * WARPS)
+        element_group_mixed<NB, NQV, NQF>(a, gi, sm, lane);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -587,36 +644,31 @@ struct MixedData {
     const double* geo = nullptr;
     const double* inv_detj = nullptr;
     const double* UD = nullptr;
-    __nv_bfloat16* dev_hi = nullptr;
-    __nv_bfloat16* dev_lo = nullptr;
-    double* Fmean = nullptr;
+    uint32_t* dev = nullptr;
+    double* Fref = nullptr;
     double* S0 = nullptr;
-    double* Rv = nullptr;
     const double* dt_inst = nullptr;  // ensembles: per-instance dt (device), else null
     const int* elem_inst = nullptr;
-    // split deviation coefficients of the states Un, Ua, Ub and of a residual input, [ncell][5][KB]
-    __nv_bfloat16* mir_hi[4] = {nullptr, nullptr, nullptr, nullptr};
-    __nv_bfloat16* mir_lo[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaStream_t side = nullptr;      // second stream: the volume kernel beside the face kernel
-    cudaEvent_t fork = nullptr, join = nullptr;
+    // A rows of the deviation coefficients of the states Un, Ua, Ub and of a residual input
+    uint32_t* mir[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
-// X(order, qv, qf, NB, NQV, NQF)
+// X(order, qv, qf, NB, NQV, NQF, W): W warps per block of the element kernel
 #define FVEDG_MIXED_COMBOS(X)      \
-    X(1, 0, 1, 4, 4, 6)            \
-    X(1, 0, 0, 4, 4, 4)            \
-    X(1, 0, 2, 4, 4, 7)            \
-    X(1, 2, 2, 4, 15, 7)           \
-    X(2, 1, 2, 10, 11, 7)          \
-    X(2, 1, 3, 10, 11, 24)         \
-    X(2, 2, 3, 10, 15, 24)         \
-    X(3, 3, 3, 20, 23, 24)         \
-    X(3, 4, 3, 20, 31, 24)         \
-    X(4, 5, 3, 35, 44, 24)         \
-    X(4, 6, 3, 35, 57, 24)
+    X(1, 0, 1, 4, 4, 6, 8)         \
+    X(1, 0, 0, 4, 4, 4, 8)         \
+    X(1, 0, 2, 4, 4, 7, 8)         \
+    X(1, 2, 2, 4, 15, 7, 8)        \
+    X(2, 1, 2, 10, 11, 7, 8)       \
+    X(2, 1, 3, 10, 11, 24, 8)      \
+    X(2, 2, 3, 10, 15, 24, 8)      \
+    X(3, 3, 3, 20, 23, 24, 8)      \
+    X(3, 4, 3, 20, 31, 24, 8)      \
+    X(4, 5, 3, 35, 44, 24, 4)      \
+    X(4, 6, 3, 35, 57, 24, 4)
 
 inline bool mixed_supported(int order, int qv, int qf) {
-#define X(P, QV, QF, NB, NQV, NQF) \
+#define X(P, QV, QF, NB, NQV, NQF, W) \
     if (order == P && qv == QV && qf == QF) return true;
     FVEDG_MIXED_COMBOS(X)
 #undef X
@@ -644,13 +696,33 @@ inline int mixed_alloc(MixedData& m, T** dst, size_t n) {
     return DG_OK;
 }
 
-inline void split_table(const std::vector<double>& x, std::vector<__nv_bfloat16>& hi, std::vector<__nv_bfloat16>& lo) {
-    hi.resize(x.size());
-    lo.resize(x.size());
-    for (size_t i = 0; i < x.size(); ++i) {
-        const float f = (float)x[i];
-        hi[i] = __float2bfloat16_rn(f);
-        lo[i] = __float2bfloat16_rn(f - __bfloat162float(hi[i]));
+// B operand of one contraction in fragment order. T is N x K row-major (N, K multiples of 8). Per
+// n-tile: for each full K tile, 32 lanes x {hi(c,c+1), hi(c+8,c+9), lo(c,c+1), lo(c+8,c+9)} of
+// row n = 8 nt + lane / 4, c = 16 t + 2 (lane % 4); then the tail, 32 lanes x {hi(c,c+1), lo(c,c+1)}.
+inline void append_frag_table(const std::vector<double>& T, int N, int K, std::vector<uint32_t>& out) {
+    const int n16 = K / 16;
+    const bool tail = (K % 16) != 0;
+    auto half = [&](int n, int k, bool lo) -> uint32_t {
+        const float f = (float)T[(size_t)n * K + k];
+        const __nv_bfloat16 h = __float2bfloat16_rn(f);
+        return (uint32_t)__bfloat16_as_ushort(lo ? __float2bfloat16_rn(f - __bfloat162float(h)) : h);
+    };
+    auto word = [&](int n, int c, bool lo) { return half(n, c, lo) | (half(n, c + 1, lo) << 16); };
+    for (int nt = 0; nt < N / 8; ++nt) {
+        for (int t = 0; t < n16; ++t)
+            for (int lane = 0; lane < 32; ++lane) {
+                const int n = nt * 8 + lane / 4, c = t * 16 + 2 * (lane % 4);
+                out.push_back(word(n, c, false));
+                out.push_back(word(n, c + 8, false));
+                out.push_back(word(n, c, true));
+                out.push_back(word(n, c + 8, true));
+            }
+        if (tail)
+            for (int lane = 0; lane < 32; ++lane) {
+                const int n = nt * 8 + lane / 4, c = n16 * 16 + 2 * (lane % 4);
+                out.push_back(word(n, c, false));
+                out.push_back(word(n, c, true));
+            }
     }
 }
 
@@ -707,15 +779,25 @@ inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>
                       const FaceInfo* d_fi, const ElemFace*, const double*) {
     if (!mixed_supported(tab.order, qv, qf)) return DG_E_ARG;
     const int NB = tab.nb, NQV = tab.nqv, NQF = tab.nqf;
-    const int KB = pad16(NB - 1), MF = pad8(NQF), MV = pad8(NQV), MJ = pad8(NB), KV = pad16(3 * NQV),
-              KF = pad16(NQF);
+    const int KB = pad8(NB - 1), MF = pad8(NQF), MV = pad8(NQV), MJ = pad8(NB), KV = pad8(3 * NQV), KF = pad8(NQF);
     m.order = tab.order; m.qv = qv; m.qf = qf; m.nb = NB; m.nqv = NQV; m.nqf = NQF;
     m.ncell = ncell; m.nface = nface; m.gamma = (float)gamma; m.flux = flux;
-    std::vector<double> tfa(24 * MF * KB, 0.0), tva(MV * KB, 0.0), tvp(MJ * KV, 0.0), tfl(24 * MJ * KF, 0.0);
+    std::vector<double> tva(MV * KB, 0.0), tvp(MJ * KV, 0.0);
     std::vector<double> mv(NB * 3, 0.0), mf(24 * NB, 0.0), inv_mass(NB, 0.0), inv_detj(ncell, 0.0);
-    for (int p = 0; p < 24; ++p)
+    std::vector<uint32_t> ftfa, ftva, ftvp, ftfl;
+    for (int p = 0; p < 24; ++p) {
+        std::vector<double> tfa(MF * KB, 0.0), tfl(MJ * KF, 0.0);
         for (int g = 0; g < NQF; ++g)
-            for (int b = 1; b < NB; ++b) tfa[(p * MF + g) * KB + (b - 1)] = tab.phi_f[((size_t)p * NQF + g) * NB + b];
+            for (int b = 1; b < NB; ++b) tfa[g * KB + (b - 1)] = tab.phi_f[((size_t)p * NQF + g) * NB + b];
+        for (int j = 0; j < NB; ++j)
+            for (int g = 0; g < NQF; ++g) {
+                const double v = tab.w_f[g] * tab.phi_f[((size_t)p * NQF + g) * NB + j];
+                tfl[j * KF + g] = v;
+                mf[p * NB + j] += v;
+            }
+        append_frag_table(tfa, MF, KB, ftfa);
+        append_frag_table(tfl, MJ, KF, ftfl);
+    }
     for (int g = 0; g < NQV; ++g)
         for (int b = 1; b < NB; ++b) tva[g * KB + (b - 1)] = tab.phi_v[g * NB + b];
     for (int j = 0; j < NB; ++j)
@@ -725,27 +807,19 @@ inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>
                 tvp[j * KV + 3 * g + d] = v;
                 mv[j * 3 + d] += v;
             }
-    for (int p = 0; p < 24; ++p)
-        for (int j = 0; j < NB; ++j)
-            for (int g = 0; g < NQF; ++g) {
-                const double v = tab.w_f[g] * tab.phi_f[((size_t)p * NQF + g) * NB + j];
-                tfl[(p * MJ + j) * KF + g] = v;
-                mf[p * NB + j] += v;
-            }
+    append_frag_table(tva, MV, KB, ftva);
+    append_frag_table(tvp, MJ, KV, ftvp);
     for (int j = 0; j < NB; ++j) inv_mass[j] = 1.0 / tab.mass_ref[j];
     for (int64_t e = 0; e < ncell; ++e) inv_detj[e] = 1.0 / hgeo[10 * e + 9];
-    std::vector<__nv_bfloat16> h, l;
+    double wsum = 0.0;
+    for (int g = 0; g < NQF; ++g) wsum += tab.w_f[g];
+    m.t.wsum = wsum;
     int rc;
-    split_table(tfa, h, l);
-    if ((rc = mixed_upload(m, &m.t.tfa_hi, h)) || (rc = mixed_upload(m, &m.t.tfa_lo, l))) return rc;
-    split_table(tva, h, l);
-    if ((rc = mixed_upload(m, &m.t.tva_hi, h)) || (rc = mixed_upload(m, &m.t.tva_lo, l))) return rc;
-    split_table(tvp, h, l);
-    if ((rc = mixed_upload(m, &m.t.tvp_hi, h)) || (rc = mixed_upload(m, &m.t.tvp_lo, l))) return rc;
-    split_table(tfl, h, l);
-    if ((rc = mixed_upload(m, &m.t.tfl_hi, h)) || (rc = mixed_upload(m, &m.t.tfl_lo, l))) return rc;
+    if ((rc = mixed_upload(m, &m.t.tfa, ftfa)) || (rc = mixed_upload(m, &m.t.tva, ftva)) ||
+        (rc = mixed_upload(m, &m.t.tvp, ftvp)) || (rc = mixed_upload(m, &m.t.tfl, ftfl)))
+        return rc;
     if ((rc = mixed_upload(m, &m.t.mv, mv)) || (rc = mixed_upload(m, &m.t.mf, mf)) ||
-        (rc = mixed_upload(m, &m.t.wf, tab.w_f)) || (rc = mixed_upload(m, &m.t.inv_mass, inv_mass)) ||
+        (rc = mixed_upload(m, &m.t.inv_mass, inv_mass)) ||
         (rc = mixed_upload(m, &m.t.wf32, std::vector<float>(tab.w_f.begin(), tab.w_f.end()))) ||
         (rc = mixed_upload(m, &m.inv_detj, inv_detj)))
         return rc;
@@ -755,23 +829,16 @@ inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>
     m.nfgroups = (int)fg.size();
     m.negroups = (int)eg.size();
     if ((rc = mixed_upload(m, &m.fgroups, fg)) || (rc = mixed_upload(m, &m.egroups, eg))) return rc;
-    // the deviation buffers' padding columns stay zero: allocation clears them, kernels never write them
-    if ((rc = mixed_alloc(m, &m.dev_hi, (size_t)nface * 5 * KF)) || (rc = mixed_alloc(m, &m.dev_lo, (size_t)nface * 5 * KF)) ||
-        (rc = mixed_alloc(m, &m.Fmean, (size_t)nface * 5)) || (rc = mixed_alloc(m, &m.S0, (size_t)nface * 5)) ||
-        (rc = mixed_alloc(m, &m.Rv, (size_t)ncell * 5 * NB)))
+    // padding columns of the A rows stay zero: allocation clears them and no kernel writes them
+    if ((rc = mixed_alloc(m, &m.dev, (size_t)nface * 5 * KF)) || (rc = mixed_alloc(m, &m.Fref, (size_t)nface * 5)) ||
+        (rc = mixed_alloc(m, &m.S0, (size_t)nface * 5)))
         return rc;
     for (int i = 0; i < 4; ++i)
-        if ((rc = mixed_alloc(m, &m.mir_hi[i], (size_t)ncell * 5 * KB)) ||
-            (rc = mixed_alloc(m, &m.mir_lo[i], (size_t)ncell * 5 * KB)))
-            return rc;
+        if ((rc = mixed_alloc(m, &m.mir[i], (size_t)ncell * 5 * KB))) return rc;
     m.fi = d_fi; m.geo = d_geo;
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&m.sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaStreamCreateWithFlags(&m.side, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&m.fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&m.join, cudaEventDisableTiming) != cudaSuccess)
-        return DG_E_CUDA;
     m.ready = true;
     return DG_OK;
 }
@@ -779,97 +846,94 @@ inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>
 inline void free_mixed(MixedData& m) {
     for (void* p : m.bufs) cudaFree(p);
     m.bufs.clear();
-    if (m.side) cudaStreamDestroy(m.side);
-    if (m.fork) cudaEventDestroy(m.fork);
-    if (m.join) cudaEventDestroy(m.join);
-    m.side = nullptr;
-    m.fork = m.join = nullptr;
     m.ready = false;
 }
 
 inline void set_mixed_dirichlet(MixedData& m, const double* UD) { m.UD = UD; }
 
-// Launch classes used for timing: 0 face fluxes, 3 volume integrals, 1 face integrals + update.
-template <int NB, int NQV, int NQF, int W = 8>
+inline MixedFaceArgs face_args(const MixedData& m, const double* U, int mir_in, int face_mask) {
+    MixedFaceArgs fa;
+    fa.U = U; fa.mir = m.mir[mir_in]; fa.fi = m.fi; fa.groups = m.fgroups; fa.UD = m.UD; fa.dev = m.dev;
+    fa.Fref = m.Fref; fa.S0 = m.S0; fa.t = m.t; fa.ngroups = m.nfgroups; fa.gamma = m.gamma; fa.flux = m.flux;
+    fa.faces_mask = face_mask;
+    return fa;
+}
+
+inline MixedElemArgs elem_args(const MixedData& m, const double* U, const double* U0, double* out, int mode,
+                               double dt, double a0, double a1, int with_volume, int mir_in, int mir_out) {
+    MixedElemArgs ea;
+    ea.U = U; ea.U0 = U0; ea.out = out; ea.mir = m.mir[mir_in]; ea.mir_out = mir_out >= 0 ? m.mir[mir_out] : nullptr;
+    ea.dev = m.dev; ea.Fref = m.Fref; ea.S0 = m.S0; ea.geo = m.geo; ea.inv_detj = m.inv_detj; ea.groups = m.egroups;
+    ea.t = m.t; ea.ngroups = m.negroups; ea.gamma = m.gamma; ea.volume = with_volume;
+    ea.dt = dt; ea.a0 = a0; ea.a1 = a1; ea.mode = mode;
+    ea.dt_inst = mode == 1 ? m.dt_inst : nullptr; ea.elem_inst = m.elem_inst;
+    return ea;
+}
+
+// Opt a kernel into `smem` bytes of dynamic shared memory once per device.
+template <class Kernel>
+inline int ensure_smem(Kernel k, size_t smem, unsigned long long& done_mask) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DG_E_CUDA;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done_mask & bit) return DG_OK;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return DG_E_CUDA;
+    done_mask |= bit;
+    return DG_OK;
+}
+
+// which: 0 = face fluxes, 1 = element kernel (volume + face integrals + update), 4 = mirror split.
+template <int NB, int NQV, int NQF, int WE>
 inline int mixed_launch(MixedData& m, int which, const double* U, const double* U0, double* out, int mode,
                         double dt, double a0, double a1, int face_mask, int with_volume, cudaStream_t s,
                         int mir_in, int mir_out) {
-    if (which == 4) {  // split U into mirror mir_in
-        const int64_t n = m.ncell * 5 * pad16(NB - 1);
-        mirror_split<NB><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(U, m.mir_hi[mir_in], m.mir_lo[mir_in], m.ncell);
+    if (which == 4) {
+        const int64_t n = m.ncell * 5 * (pad8(NB - 1) / 2);
+        mirror_split<NB><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(U, m.mir[mir_in], m.ncell);
     } else if (which == 0) {
-        MixedFaceArgs fa;
-        fa.U = U; fa.mir_hi = m.mir_hi[mir_in]; fa.mir_lo = m.mir_lo[mir_in]; fa.fi = m.fi; fa.groups = m.fgroups; fa.UD = m.UD; fa.dev_hi = m.dev_hi; fa.dev_lo = m.dev_lo;
-        fa.Fmean = m.Fmean; fa.S0 = m.S0; fa.t = m.t; fa.ngroups = m.nfgroups; fa.gamma = m.gamma; fa.flux = m.flux;
-        fa.faces_mask = face_mask;
+        constexpr int W = 8;
         const int g = (int)std::min<int64_t>((m.nfgroups + W - 1) / W, (int64_t)m.sms * 32);
-        face_flux_mixed<NB, NQF, W><<<g, W * 32, 0, s>>>(fa);
-    } else if (which == 3) {
-        constexpr size_t smem = sizeof(VolMixedSmem<NB, NQV>) * W;
-        static bool attr = false;
-        if (!attr) {
-            if (cudaFuncSetAttribute(volume_mixed<NB, NQV, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem) != cudaSuccess)
-                return DG_E_CUDA;
-            attr = true;
-        }
-        MixedVolArgs va;
-        va.U = U; va.mir_hi = m.mir_hi[mir_in]; va.mir_lo = m.mir_lo[mir_in]; va.geo = m.geo; va.groups = m.egroups; va.Rv = m.Rv; va.t = m.t; va.ngroups = m.negroups;
-        va.gamma = m.gamma;
-        const int g = (int)std::min<int64_t>((m.negroups + W - 1) / W, (int64_t)m.sms * 32);
-        volume_mixed<NB, NQV, W><<<g, W * 32, smem, s>>>(va);
+        face_flux_mixed<NB, NQF, W><<<g, W * 32, 0, s>>>(face_args(m, U, mir_in, face_mask));
     } else {
-        MixedLiftArgs la;
-        la.U = U; la.U0 = U0; la.out = out; la.Rv = with_volume ? m.Rv : nullptr; la.dev_hi = m.dev_hi;
-        la.dev_lo = m.dev_lo; la.Fmean = m.Fmean; la.S0 = m.S0; la.inv_detj = m.inv_detj; la.groups = m.egroups;
-        la.t = m.t; la.ngroups = m.negroups; la.dt = dt; la.a0 = a0; la.a1 = a1; la.mode = mode;
-        la.dt_inst = mode == 1 ? m.dt_inst : nullptr; la.elem_inst = m.elem_inst;
-        la.out_mir_hi = mir_out >= 0 ? m.mir_hi[mir_out] : nullptr;
-        la.out_mir_lo = mir_out >= 0 ? m.mir_lo[mir_out] : nullptr;
-        const int g = (int)std::min<int64_t>((m.negroups + W - 1) / W, (int64_t)m.sms * 32);
-        lift_mixed<NB, NQF, W><<<g, W * 32, 0, s>>>(la);
+        constexpr size_t smem = sizeof(ElemMixedSmem<NB, NQV, NQF>) * WE;
+        static unsigned long long done = 0;
+        int rc = ensure_smem(element_mixed<NB, NQV, NQF, WE>, smem, done);
+        if (rc) return rc;
+        const int g = (int)std::min<int64_t>((m.negroups + WE - 1) / WE, (int64_t)m.sms * 32);
+        element_mixed<NB, NQV, NQF, WE><<<g, WE * 32, smem, s>>>(
+            elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out));
     }
     return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;
 }
 
-// which: 0 = face fluxes, 3 = volume integrals, 1 = face integrals + update, 4 = mirror split.
 // mir_in: mirror of U (0..3); mir_out: mirror the update writes (RK mode), or -1.
 inline int mixed_kernel(MixedData& m, int which, const double* U, const double* U0, double* out, int mode,
                         double dt, double a0, double a1, int face_mask, int with_volume, cudaStream_t s,
                         std::atomic<int64_t>* launches, int mir_in, int mir_out) {
     if (!m.ready) return DG_E_ARG;
     ++*launches;
-#define X(P, QV, QF, NB, NQV, NQF)                                                                          \
-    if (m.order == P && m.qv == QV && m.qf == QF)                                                           \
-        return mixed_launch<NB, NQV, NQF>(m, which, U, U0, out, mode, dt, a0, a1, face_mask, with_volume, s, \
-                                          mir_in, mir_out);
+#define X(P, QV, QF, NB, NQV, NQF, W)                                                                           \
+    if (m.order == P && m.qv == QV && m.qf == QF)                                                               \
+        return mixed_launch<NB, NQV, NQF, W>(m, which, U, U0, out, mode, dt, a0, a1, face_mask, with_volume, s, \
+                                             mir_in, mir_out);
     FVEDG_MIXED_COMBOS(X)
 #undef X
     return DG_E_ARG;
 }
 
-// One stage: face fluxes on s, volume integrals on the side stream (forked from and joined back to
-// s, which a CUDA graph capture turns into two parallel branches), then face integrals + update.
+// One stage: face fluxes, then the element kernel.
 template <class Timed>
 inline int mixed_stage(MixedData& m, const double* U, const double* U0, double* out, int mode, double dt, double a0,
                        double a1, int face_mask, int with_volume, cudaStream_t s, std::atomic<int64_t>* launches,
-                       Timed&& timed, bool overlap, int mir_in, int mir_out) {
-    int rc;
-    auto K = [&](int which, int wv, cudaStream_t st) {
-        return mixed_kernel(m, which, U, U0, out, mode, dt, a0, a1, face_mask, wv, st, launches, mir_in, mir_out);
+                       Timed&& timed, int mir_in, int mir_out) {
+    auto K = [&](int which) {
+        return mixed_kernel(m, which, U, U0, out, mode, dt, a0, a1, face_mask, with_volume, s, launches, mir_in,
+                            mir_out);
     };
-    if (with_volume && overlap) {
-        if (cudaEventRecord(m.fork, s) != cudaSuccess || cudaStreamWaitEvent(m.side, m.fork, 0) != cudaSuccess)
-            return DG_E_CUDA;
-        if ((rc = K(3, 1, m.side))) return rc;
-        if (cudaEventRecord(m.join, m.side) != cudaSuccess) return DG_E_CUDA;
-        if ((rc = timed(0, [&] { return K(0, 1, s); }))) return rc;
-        if (cudaStreamWaitEvent(s, m.join, 0) != cudaSuccess) return DG_E_CUDA;
-    } else {
-        if ((rc = timed(0, [&] { return K(0, 1, s); }))) return rc;
-        if (with_volume && (rc = timed(3, [&] { return K(3, 1, s); }))) return rc;
-    }
-    return timed(1, [&] { return K(1, with_volume, s); });
+    const int rc = timed(0, [&] { return K(0); });
+    if (rc) return rc;
+    return timed(1, [&] { return K(1); });
 }
 
 // The mirror of an arbitrary state (the upload, the residual input) is written by a split kernel.
@@ -883,25 +947,24 @@ inline int residual_mixed(MixedData& m, const double* U, double* R, int part, cu
     int rc = mixed_mirror(m, U, 3, s, launches);
     if (rc) return rc;
     return mixed_stage(m, U, U, R, 0, 0.0, 0.0, 0.0, mask, part == 0 || part == 1, s, launches,
-                       [](int, auto&& fn) { return fn(); }, false, 3, -1);
+                       [](int, auto&& fn) { return fn(); }, 3, -1);
 }
 
-inline int mixed_launches_per_step(const MixedData&) { return 9; }
+inline int mixed_launches_per_step(const MixedData&) { return 6; }
 
-// SSP-RK3 step; `timed(cls, fn)` runs fn (one launch) and may bracket it with timing events. When
-// timing, the volume kernel runs in line so each launch has its own interval. The mirror of Un
-// must be current (the upload writes it, and stage 3 of every step rewrites it).
+// SSP-RK3 step; `timed(cls, fn)` runs fn (one launch) and may bracket it with timing events. The
+// mirror of Un must be current (the upload writes it, and stage 3 of every step rewrites it).
 template <class Timed>
 inline int step_mixed(MixedData& m, double* Un, double* Ua, double* Ub, double dt, cudaStream_t s,
-                      std::atomic<int64_t>* launches, Timed&& timed, bool overlap = true) {
+                      std::atomic<int64_t>* launches, Timed&& timed) {
     const double A0[3] = {0.0, 0.75, 1.0 / 3.0};
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
     const double* in[3] = {Un, Ua, Ub};
     double* out[3] = {Ua, Ub, Un};
     const int mi[3] = {0, 1, 2}, mo[3] = {1, 2, 0};
     for (int st = 0; st < 3; ++st) {
-        const int rc = mixed_stage(m, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches, timed, overlap,
-                                   mi[st], mo[st]);
+        const int rc =
+            mixed_stage(m, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches, timed, mi[st], mo[st]);
         if (rc) return rc;
     }
     return DG_OK;

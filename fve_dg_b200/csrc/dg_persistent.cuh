@@ -50,48 +50,40 @@ __device__ __forceinline__ void grid_barrier(QueueState* q, unsigned int nblocks
 
 template <int NB, int NQV, int NQF>
 __host__ __device__ constexpr size_t persistent_warp_smem() {
-    constexpr size_t a = sizeof(FaceMixedSmem<NQF>), b = sizeof(VolMixedSmem<NB, NQV>), c = sizeof(LiftMixedSmem);
-    return ((a > b ? (a > c ? a : c) : (b > c ? b : c)) + 15) / 16 * 16;
+    constexpr size_t a = sizeof(FaceMixedSmem<NQF>), b = sizeof(ElemMixedSmem<NB, NQV, NQF>);
+    return ((a > b ? a : b) + 15) / 16 * 16;
 }
 
-// Phase 1 takes tickets over face-group tiles followed by volume-group tiles (independent work);
-// phase 2 takes tickets over element-group tiles for the face integrals and the update.
+// Phase 1 takes tickets over face-group tiles; phase 2 takes tickets over element-group tiles
+// (volume term, face integrals and the update).
 template <int NB, int NQV, int NQF, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
-    stage_persistent_mixed(MixedFaceArgs fa, MixedVolArgs va, MixedLiftArgs la, QueueState* q, int tile_f,
-                           int tile_e) {
+    stage_persistent_mixed(MixedFaceArgs fa, MixedElemArgs ea, QueueState* q, int tile_f, int tile_e) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_tile;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* wsm = smem_raw + persistent_warp_smem<NB, NQV, NQF>() * warp;
-    const int nft = (fa.ngroups + tile_f - 1) / tile_f;
-    const int nvt = va.Rv ? (va.ngroups + tile_e - 1) / tile_e : 0;
     for (;;) {
         if (threadIdx.x == 0) s_tile = (int)atomicAdd(&q->ctr[0], 1u);
         __syncthreads();
-        const int t = s_tile;
+        const int g0 = s_tile * tile_f;
         __syncthreads();
-        if (t >= nft + nvt) break;
-        if (t < nft) {
-            const int g0 = t * tile_f, g1 = min(g0 + tile_f, fa.ngroups);
-            for (int gi = g0 + warp; gi < g1; gi += WARPS)
-                face_group_mixed<NB, NQF>(fa, gi, *reinterpret_cast<FaceMixedSmem<NQF>*>(wsm), lane);
-        } else {
-            const int g0 = (t - nft) * tile_e, g1 = min(g0 + tile_e, va.ngroups);
-            for (int gi = g0 + warp; gi < g1; gi += WARPS)
-                volume_group_mixed<NB, NQV>(va, gi, *reinterpret_cast<VolMixedSmem<NB, NQV>*>(wsm), lane);
-        }
+        if (g0 >= fa.ngroups) break;
+        const int g1 = min(g0 + tile_f, fa.ngroups);
+        for (int gi = g0 + warp; gi < g1; gi += WARPS)
+            face_group_mixed<NB, NQF>(fa, gi, *reinterpret_cast<FaceMixedSmem<NQF>*>(wsm), lane);
     }
     grid_barrier(q, gridDim.x);
+    auto& esm = *reinterpret_cast<ElemMixedSmem<NB, NQV, NQF>*>(wsm);
+    element_smem_init(esm, lane);
     for (;;) {
         if (threadIdx.x == 0) s_tile = (int)atomicAdd(&q->ctr[1], 1u);
         __syncthreads();
         const int g0 = s_tile * tile_e;
         __syncthreads();
-        if (g0 >= la.ngroups) break;
-        const int g1 = min(g0 + tile_e, la.ngroups);
-        for (int gi = g0 + warp; gi < g1; gi += WARPS)
-            lift_group_mixed<NB, NQF>(la, gi, *reinterpret_cast<LiftMixedSmem*>(wsm), lane);
+        if (g0 >= ea.ngroups) break;
+        const int g1 = min(g0 + tile_e, ea.ngroups);
+        for (int gi = g0 + warp; gi < g1; gi += WARPS) element_group_mixed<NB, NQV, NQF>(ea, gi, esm, lane);
     }
     grid_barrier(q, gridDim.x);
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // every CTA is past both queues: rearm them
@@ -113,27 +105,22 @@ inline int persistent_launch(MixedData& m, QueueState* q, const PersistentParams
                              int with_volume, cudaStream_t s, int mir_in, int mir_out) {
     auto kern = stage_persistent_mixed<NB, NQV, NQF, W>;
     constexpr size_t smem = persistent_warp_smem<NB, NQV, NQF>() * W;
-    static int per_sm = -1;
-    if (per_sm < 0) {
+    static unsigned long long done = 0;
+    static int per_sm[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DG_E_CUDA;
+    if (!(done & (1ull << (dev & 63)))) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return DG_E_CUDA;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem) != cudaSuccess || per_sm < 1)
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, W * 32, smem) != cudaSuccess || n < 1)
             return DG_E_CUDA;
+        per_sm[dev & 63] = n;
+        done |= 1ull << (dev & 63);
     }
-    const int bps = pp.max_blocks > 0 ? std::min(per_sm, pp.max_blocks) : per_sm;
-    MixedFaceArgs fa;
-    fa.U = U; fa.mir_hi = m.mir_hi[mir_in]; fa.mir_lo = m.mir_lo[mir_in]; fa.fi = m.fi; fa.groups = m.fgroups; fa.UD = m.UD; fa.dev_hi = m.dev_hi; fa.dev_lo = m.dev_lo;
-    fa.Fmean = m.Fmean; fa.S0 = m.S0; fa.t = m.t; fa.ngroups = m.nfgroups; fa.gamma = m.gamma; fa.flux = m.flux;
-    fa.faces_mask = face_mask;
-    MixedVolArgs va;
-    va.U = U; va.mir_hi = m.mir_hi[mir_in]; va.mir_lo = m.mir_lo[mir_in]; va.geo = m.geo; va.groups = m.egroups; va.Rv = with_volume ? m.Rv : nullptr; va.t = m.t;
-    va.ngroups = m.negroups; va.gamma = m.gamma;
-    MixedLiftArgs la;
-    la.U = U; la.U0 = U0; la.out = out; la.Rv = with_volume ? m.Rv : nullptr; la.dev_hi = m.dev_hi;
-    la.dev_lo = m.dev_lo; la.Fmean = m.Fmean; la.S0 = m.S0; la.inv_detj = m.inv_detj; la.groups = m.egroups;
-    la.t = m.t; la.ngroups = m.negroups; la.dt = dt; la.a0 = a0; la.a1 = a1; la.mode = mode;
-    la.dt_inst = mode == 1 ? m.dt_inst : nullptr; la.elem_inst = m.elem_inst;
-    la.out_mir_hi = m.mir_hi[mir_out]; la.out_mir_lo = m.mir_lo[mir_out];
+    const int bps = pp.max_blocks > 0 ? std::min(per_sm[dev & 63], pp.max_blocks) : per_sm[dev & 63];
+    const MixedFaceArgs fa = face_args(m, U, mir_in, face_mask);
+    const MixedElemArgs ea = elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out);
     int tf = pp.tile_f, te = pp.tile_e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(m.sms * bps);
@@ -145,7 +132,7 @@ inline int persistent_launch(MixedData& m, QueueState* q, const PersistentParams
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, kern, fa, va, la, q, tf, te) != cudaSuccess) return DG_E_CUDA;
+    if (cudaLaunchKernelEx(&cfg, kern, fa, ea, q, tf, te) != cudaSuccess) return DG_E_CUDA;
     return DG_OK;
 }
 
@@ -154,7 +141,7 @@ inline int persistent_kernel(MixedData& m, QueueState* q, const PersistentParams
                              int with_volume, cudaStream_t s, std::atomic<int64_t>* launches, int mir_in, int mir_out) {
     if (!m.ready) return DG_E_ARG;
     ++*launches;
-#define X(P, QV, QF, NB, NQV, NQF)                                                                                \
+#define X(P, QV, QF, NB, NQV, NQF, W)                                                                             \
     if (m.order == P && m.qv == QV && m.qf == QF)                                                                 \
         return persistent_launch<NB, NQV, NQF>(m, q, pp, U, U0, out, mode, dt, a0, a1, face_mask, with_volume, s, \
                                                mir_in, mir_out);
