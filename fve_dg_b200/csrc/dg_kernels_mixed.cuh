@@ -413,50 +413,104 @@ template <int NB, int NQV, int NQF>
 struct alignas(16) ElemMixedSmem {
     static constexpr int MV = pad8(NQV), KV = pad8(3 * NQV), MJ = pad8(NB);
     static constexpr int LDU = frag_ld(MV), LDG = frag_ld(KV);
-    static_assert(MJ <= LDU, "the accumulator transpose reuses sU");
-    float sU[16][LDU];    // volume values (c_0 added), rows (element, var), cols point; then R
-    float sG[16][LDG];    // Gb - G, rows (element, var), cols (point, dir); padding columns zero
-    double sGb[3][15];    // detJ F(c_0) J^-T of each element (FP64)
-    double sFr[3][4][5];  // face reference fluxes
-    double sS0[3][5];     // +-sum_q S0 (the mode-0 face integrals, in a fixed order)
-    double sMF[4][NB];    // +-mf of the group's four face maps
-    float sJ[3][10];      // J^-T and detJ
+    // FP64 residual rows: stride = 8 (mod 16) doubles, so the 16-byte stores of the accumulator
+    // pattern (two rows x four column pairs per quarter warp) hit 32 distinct banks
+    static constexpr int LDR = MJ + ((8 - MJ % 16) + 16) % 16;
+    static constexpr int GROWS = 16 * LDG >= 32 * LDR ? 16 : (32 * LDR + LDG - 1) / LDG;
+    float sU[16][LDU];       // volume values (c_0 added), rows (element, var), cols point
+    float sG[GROWS][LDG];    // Gb - G, rows (element, var), cols (point, dir), padding columns zero;
+                             // afterwards the FP64 residual [16][LDR]
+    double sGb[3][15];       // detJ F(c_0) J^-T of each element (FP64)
+    double sFr[3][4][5];     // face reference fluxes
+    double sS0[3][5];        // +-sum_q S0 (the mode-0 face integrals, in a fixed order)
+    double sMF[4][NB];       // +-mf of the group's four face maps
+    double sDT[3];           // dt / detJ of each element
+    float sJ[3][9];          // detJ J^-T, FP32
     float sGbf[3][15];
     float sC0[16];
+    int sE[3];
 };
+
+// Per-block tables of the element kernel's epilogue: for DOF r = 5 j + k of an element, (j, k) and
+// the BF16 offsets of its hi/lo parts in the element's A rows; and the inverse reference mass.
+template <int NB>
+struct ElemTables {
+    int4 dof[5 * NB];
+    double inv_mass[NB];
+};
+
+template <int NB>
+__device__ __forceinline__ void element_tables_init(ElemTables<NB>& T, const double* inv_mass) {
+    constexpr int KB = pad8(NB - 1);
+    for (int r = threadIdx.x; r < 5 * NB; r += blockDim.x) {
+        const int j = r / 5, k = r - 5 * j;
+        int hw = 0, lw = 0;
+        if (j > 0) {
+            hw = 2 * (k * KB + arow_hi_word<KB>(j - 1)) + ((j - 1) & 1);
+            lw = 2 * (k * KB + arow_lo_word<KB>(j - 1)) + ((j - 1) & 1);
+        }
+        T.dof[r] = make_int4(j, k, hw, lw);
+    }
+    for (int j = threadIdx.x; j < NB; j += blockDim.x) T.inv_mass[j] = inv_mass[j];
+    __syncthreads();
+}
+
+__device__ __forceinline__ void dmma884(double d[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
 
 template <int NB, int NQV, int NQF>
 __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int gi, ElemMixedSmem<NB, NQV, NQF>& sm,
-                                                    int lane) {
+                                                    const ElemTables<NB>& T, int lane) {
     using S = ElemMixedSmem<NB, NQV, NQF>;
-    constexpr int KB = pad8(NB - 1), MV = S::MV, KV = S::KV, MJ = S::MJ, KF = pad8(NQF), NT = MJ / 8;
+    constexpr int KB = pad8(NB - 1), MV = S::MV, KV = S::KV, MJ = S::MJ, KF = pad8(NQF), NT = MJ / 8, LDR = S::LDR;
     const int gid = lane >> 2, tq = lane & 3;
     const ElemGroup& grp = a.groups[gi];  // read in place (a copy would live in local memory)
     const int ne = grp.n;
     const int r0 = gid, r1 = gid + 8;
     const bool v0 = r0 < 5 * ne, v1 = r1 < 5 * ne;
     if (lane < 16) sm.sC0[lane] = lane < 5 * ne ? (float)__ldg(a.U + (int64_t)grp.e[lane / 5] * (5 * NB) + lane % 5) : 0.f;
-    if (a.volume && lane < ne) {  // G(c_0), FP64
-        const int64_t e = grp.e[lane];
+    if (lane < ne) {
+        const int e = grp.e[lane];
+        sm.sE[lane] = e;
+        const double dt = a.dt_inst ? __ldg(a.dt_inst + __ldg(a.elem_inst + e)) : a.dt;
+        sm.sDT[lane] = dt * __ldg(a.inv_detj + e);
+    }
+    if (a.volume && lane < 5 * ne) {  // row k of G(c_0) = detJ F(c_0) J^-T, FP64, one lane per (element, var)
+        const int el = lane / 5, k = lane - 5 * el;
+        const int64_t e = grp.e[el];
         const double* geo = a.geo + e * 10;
-        double c0[5], F[5][3], J[9];
+        double c[5], J[9];
         #pragma unroll
-        for (int k = 0; k < 5; ++k) c0[k] = __ldg(a.U + e * (5 * NB) + k);
+        for (int i = 0; i < 5; ++i) c[i] = __ldg(a.U + e * (5 * NB) + i);
         #pragma unroll
         for (int i = 0; i < 9; ++i) J[i] = __ldg(geo + i);
         const double dj = __ldg(geo + 9);
-        Phys<double>::flux(c0, (double)a.gamma - 1.0, F);
-        #pragma unroll
-        for (int k = 0; k < 5; ++k)
+        const double rho = c[0] > 1e-16 ? c[0] : 1e-16, ir = 1.0 / rho;
+        const double u[3] = {c[1] * ir, c[2] * ir, c[3] * ir}, en = c[4] * ir;
+        const double p = ((double)a.gamma - 1.0) * (rho * en - 0.5 * rho * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]));
+        double F[3];
+        if (k == 0) {
+            F[0] = rho * u[0]; F[1] = rho * u[1]; F[2] = rho * u[2];
+        } else if (k < 4) {
             #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const double gb = dj * (F[k][0] * J[d] + F[k][1] * J[3 + d] + F[k][2] * J[6 + d]);
-                sm.sGb[lane][3 * k + d] = gb;
-                sm.sGbf[lane][3 * k + d] = (float)gb;
-            }
+            for (int i = 0; i < 3; ++i) F[i] = rho * u[i] * u[k - 1] + (i == k - 1 ? p : 0.0);
+        } else {
+            #pragma unroll
+            for (int i = 0; i < 3; ++i) F[i] = u[i] * (rho * en + p);
+        }
         #pragma unroll
-        for (int i = 0; i < 9; ++i) sm.sJ[lane][i] = (float)J[i];
-        sm.sJ[lane][9] = (float)dj;
+        for (int d = 0; d < 3; ++d) {
+            const double gb = dj * (F[0] * J[d] + F[1] * J[3 + d] + F[2] * J[6 + d]);
+            sm.sGb[el][3 * k + d] = gb;
+            sm.sGbf[el][3 * k + d] = (float)gb;
+        }
+        if (k == 0) {
+            #pragma unroll
+            for (int i = 0; i < 9; ++i) sm.sJ[el][i] = (float)(dj * J[i]);
+        }
     }
     for (int i = lane; i < ne * 20; i += 32) {
         const int el = i / 20, r = i - el * 20, q = r / 5, k = r - 5 * q;
@@ -497,6 +551,12 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
                 *reinterpret_cast<float2*>(&sm.sU[r1][nt * 8 + 2 * tq]) = make_float2(o[2] + c01, o[3] + c01);
             }
         }
+        // the MMA reads columns up to KV: the padding past 3 NQV must be zero (the FP64 residual of
+        // the previous group shares this memory)
+        if constexpr (KV > 3 * NQV) {
+            constexpr int w = KV - 3 * NQV;
+            for (int i = lane; i < 16 * w; i += 32) sm.sG[i / w][3 * NQV + i % w] = 0.f;
+        }
         __syncwarp();
         const float gm1 = a.gamma - 1.f;
         for (int p = lane; p < ne * NQV; p += 32) {
@@ -511,7 +571,7 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
                 #pragma unroll
                 for (int d = 0; d < 3; ++d)
                     sm.sG[el * 5 + k][3 * g + d] =
-                        sm.sGbf[el][3 * k + d] - J[9] * (F[k][0] * J[d] + F[k][1] * J[3 + d] + F[k][2] * J[6 + d]);
+                        fmaf(-F[k][0], J[d], fmaf(-F[k][1], J[3 + d], fmaf(-F[k][2], J[6 + d], sm.sGbf[el][3 * k + d])));
         }
         __syncwarp();
         // volume integral: acc += (Gb - G) * (w dphi), split on the fly
@@ -561,56 +621,60 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
         #pragma unroll
         for (int nt = 0; nt < NT; ++nt) mma_bt<KF>(acc[nt], A, tb, nt, lane);
     }
-    __syncwarp();  // sU is free: transpose the accumulators through it
-    #pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-        *reinterpret_cast<float2*>(&sm.sU[r0][nt * 8 + 2 * tq]) = make_float2(acc[nt][0], acc[nt][1]);
-        *reinterpret_cast<float2*>(&sm.sU[r1][nt * 8 + 2 * tq]) = make_float2(acc[nt][2], acc[nt][3]);
+    __syncwarp();  // sG is free
+    // FP64 parts on the FP64 tensor cores, in the accumulators' own layout (rows gid / gid + 8,
+    // columns 2 tq, 2 tq + 1 of each n-tile): R = acc + [Fr_q, Gb_d] x [+-mf_q(j), -mv_d(j)], K = 8
+    // (four face references, three volume reference components, one zero)
+    {
+        double* sR = reinterpret_cast<double*>(&sm.sG[0][0]);
+        double am[2][2];  // A(row gid + 8 mt, column 4 kt + tq)
+        #pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            const int row = gid + 8 * mt, el = row / 5, k = row - 5 * el;
+            const bool ok = row < 5 * ne;
+            am[mt][0] = ok ? sm.sFr[el][tq][k] : 0.0;
+            am[mt][1] = (ok && a.volume && tq < 3) ? sm.sGb[el][3 * k + tq] : 0.0;
+        }
+        #pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+            const int jb = nt * 8 + gid;  // B(k = 4 kt + tq, n = jb)
+            const double b0 = jb < NB ? sm.sMF[tq][jb] : 0.0;
+            const double b1 = (jb < NB && tq < 3) ? -__ldg(a.t.mv + 3 * jb + tq) : 0.0;
+            #pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                double d[2] = {(double)acc[nt][2 * mt], (double)acc[nt][2 * mt + 1]};
+                dmma884(d, am[mt][0], b0);
+                dmma884(d, am[mt][1], b1);
+                const int row = gid + 8 * mt;
+                if (nt == 0 && tq == 0 && row < 5 * ne) d[0] = sm.sS0[row / 5][row % 5];  // mode 0: exact face sums
+                *reinterpret_cast<double2*>(sR + row * LDR + nt * 8 + 2 * tq) = make_double2(d[0], d[1]);
+            }
+        }
     }
     __syncwarp();
     // epilogue over the group's DOFs in memory order (coalesced FP64 traffic)
+    const double* sR = reinterpret_cast<const double*>(&sm.sG[0][0]);
+    unsigned short* mir16 = reinterpret_cast<unsigned short*>(a.mir_out);
     for (int i = lane; i < ne * 5 * NB; i += 32) {
-        const int el = i / (5 * NB), r = i - el * (5 * NB), j = r / 5, k = r - 5 * j;
-        const int e = grp.e[el];
-        double R;
-        if (j == 0) {
-            R = sm.sS0[el][k];  // grad phi_0 = 0: only the exact face sums
-        } else {
-            R = (double)sm.sU[el * 5 + k][j];
-            #pragma unroll
-            for (int q = 0; q < 4; ++q) R += sm.sMF[q][j] * sm.sFr[el][q][k];
-            if (a.volume) {
-                const double* mv = a.t.mv + 3 * j;
-                const double* gb = sm.sGb[el] + 3 * k;
-                R -= gb[0] * __ldg(mv) + gb[1] * __ldg(mv + 1) + gb[2] * __ldg(mv + 2);
-            }
-        }
-        const int64_t idx = (int64_t)e * (5 * NB) + r;
+        const int el = i / (5 * NB), r = i - el * (5 * NB);
+        const int4 d = T.dof[r];  // j, k, hi offset, lo offset
+        const int64_t e = sm.sE[el];
+        const double R = sR[(el * 5 + d.y) * LDR + d.x];
+        const int64_t idx = e * (5 * NB) + r;
         if (a.mode == 0) {
             a.out[idx] = R;
         } else {
-            const double ib = __ldg(a.inv_detj + e) * __ldg(a.t.inv_mass + j);
-            const double dt = a.dt_inst ? __ldg(a.dt_inst + __ldg(a.elem_inst + e)) : a.dt;
-            const double un = a.a0 * a.U0[idx] + a.a1 * (__ldg(a.U + idx) + dt * (-R * ib));
+            const double un = a.a0 * a.U0[idx] + a.a1 * (__ldg(a.U + idx) - sm.sDT[el] * T.inv_mass[d.x] * R);
             a.out[idx] = un;
-            if (j > 0) {
+            if (d.x > 0) {
                 unsigned short h, l;
                 split1((float)un, h, l);
-                unsigned short* mrow = reinterpret_cast<unsigned short*>(a.mir_out + ((int64_t)e * 5 + k) * KB);
-                mrow[2 * arow_hi_word<KB>(j - 1) + ((j - 1) & 1)] = h;
-                mrow[2 * arow_lo_word<KB>(j - 1) + ((j - 1) & 1)] = l;
+                unsigned short* mrow = mir16 + e * (10 * KB);
+                mrow[d.z] = h;
+                mrow[d.w] = l;
             }
         }
     }
-    __syncwarp();
-}
-
-// Columns 3 NQV .. LDG of sG stay zero for the kernel's lifetime (the flux loop never writes them).
-template <int NB, int NQV, int NQF>
-__device__ __forceinline__ void element_smem_init(ElemMixedSmem<NB, NQV, NQF>& sm, int lane) {
-    using S = ElemMixedSmem<NB, NQV, NQF>;
-    constexpr int c0 = 3 * NQV, w = S::LDG - c0;
-    for (int i = lane; i < 16 * w; i += 32) sm.sG[i / w][c0 + i % w] = 0.f;
     __syncwarp();
 }
 
@@ -618,11 +682,12 @@ template <int NB, int NQV, int NQF, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) element_mixed(MixedElemArgs a) {
     using S = ElemMixedSmem<NB, NQV, NQF>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ ElemTables<NB> tabs;
+    element_tables_init(tabs, a.t.inv_mass);
     S& sm = reinterpret_cast<S*>(smem_raw)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
-    element_smem_init(sm, lane);
     for (int gi = blockIdx.x * WARPS + (threadIdx.x >> 5); gi < a.ngroups; gi += gridDim.x * WARPS)
-        element_group_mixed<NB, NQV, NQF>(a, gi, sm, lane);
+        element_group_mixed<NB, NQV, NQF>(a, gi, sm, tabs, lane);
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -75,7 +75,8 @@ __global__ void __launch_bounds__(WARPS * 32)
     }
     grid_barrier(q, gridDim.x);
     auto& esm = *reinterpret_cast<ElemMixedSmem<NB, NQV, NQF>*>(wsm);
-    element_smem_init(esm, lane);
+    __shared__ ElemTables<NB> tabs;
+    element_tables_init(tabs, ea.t.inv_mass);
     for (;;) {
         if (threadIdx.x == 0) s_tile = (int)atomicAdd(&q->ctr[1], 1u);
         __syncthreads();
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(WARPS * 32)
         __syncthreads();
         if (g0 >= ea.ngroups) break;
         const int g1 = min(g0 + tile_e, ea.ngroups);
-        for (int gi = g0 + warp; gi < g1; gi += WARPS) element_group_mixed<NB, NQV, NQF>(ea, gi, esm, lane);
+        for (int gi = g0 + warp; gi < g1; gi += WARPS) element_group_mixed<NB, NQV, NQF>(ea, gi, esm, tabs, lane);
     }
     grid_barrier(q, gridDim.x);
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // every CTA is past both queues: rearm them
