@@ -47,9 +47,9 @@ namespace fvedg {
 
 __host__ __device__ constexpr int pad8(int x) { return (x + 7) / 8 * 8; }
 __host__ __device__ constexpr int pad16(int x) { return (x + 15) / 16 * 16; }
-// A shared-memory row stride >= n that is 8 (mod 32) floats: 64-bit accesses of the MMA fragment
-// pattern (8 rows x 4 column pairs) then touch 32 distinct banks per half warp.
-__host__ __device__ constexpr int frag_ld(int n) { return n + ((8 - n % 32) + 32) % 32; }
+// A shared-memory row stride >= n that is 8 (mod 16) floats: the 64-bit accesses of the MMA
+// fragment pattern (4 rows x 4 column pairs per half warp) then touch 32 distinct banks.
+__host__ __device__ constexpr int frag_ld(int n) { return n + ((8 - n % 16) + 16) % 16; }
 
 // K tiling of one contraction: K / 16 full tiles and, when K = 8 (mod 16), one 8-wide tail.
 template <int K>
@@ -416,14 +416,12 @@ struct alignas(16) ElemMixedSmem {
     // FP64 residual rows: stride = 8 (mod 16) doubles, so the 16-byte stores of the accumulator
     // pattern (two rows x four column pairs per quarter warp) hit 32 distinct banks
     static constexpr int LDR = MJ + ((8 - MJ % 16) + 16) % 16;
-    static constexpr int GROWS = 16 * LDG >= 32 * LDR ? 16 : (32 * LDR + LDG - 1) / LDG;
+    // 15 rows hold (element, var) pairs (row 15 is never a valid row); the FP64 residual [16][LDR]
+    // reuses the space once the volume integral is done
+    static constexpr int GROWS = 15 * LDG >= 32 * LDR ? 15 : (32 * LDR + LDG - 1) / LDG;
     float sU[16][LDU];       // volume values (c_0 added), rows (element, var), cols point
-    float sG[GROWS][LDG];    // Gb - G, rows (element, var), cols (point, dir), padding columns zero;
-                             // afterwards the FP64 residual [16][LDR]
+    float sG[GROWS][LDG];    // Gb - G, rows (element, var), cols (point, dir), padding columns zero
     double sGb[3][15];       // detJ F(c_0) J^-T of each element (FP64)
-    double sFr[3][4][5];     // face reference fluxes
-    double sS0[3][5];        // +-sum_q S0 (the mode-0 face integrals, in a fixed order)
-    double sMF[4][NB];       // +-mf of the group's four face maps
     double sDT[3];           // dt / detJ of each element
     float sJ[3][9];          // detJ J^-T, FP32
     float sGbf[3][15];
@@ -512,25 +510,6 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
             for (int i = 0; i < 9; ++i) sm.sJ[el][i] = (float)(dj * J[i]);
         }
     }
-    for (int i = lane; i < ne * 20; i += 32) {
-        const int el = i / 20, r = i - el * 20, q = r / 5, k = r - 5 * q;
-        sm.sFr[el][q][k] = __ldcg(a.Fref + (int64_t)grp.face[el][q] * 5 + k);
-    }
-    if (lane < 5 * ne) {
-        const int el = lane / 5, k = lane - 5 * el;
-        double s = 0.0;
-        #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const double v = __ldcg(a.S0 + (int64_t)grp.face[el][q] * 5 + k);
-            s += (grp.meta[q] >> 8) ? -v : v;
-        }
-        sm.sS0[el][k] = s;
-    }
-    for (int i = lane; i < 4 * NB; i += 32) {
-        const int q = i / NB, j = i - q * NB;
-        const double v = __ldg(a.t.mf + (grp.meta[q] & 0xff) * NB + j);
-        sm.sMF[q][j] = (grp.meta[q] >> 8) ? -v : v;
-    }
     __syncwarp();
     float acc[NT][4];
     #pragma unroll
@@ -555,7 +534,7 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
         // the previous group shares this memory)
         if constexpr (KV > 3 * NQV) {
             constexpr int w = KV - 3 * NQV;
-            for (int i = lane; i < 16 * w; i += 32) sm.sG[i / w][3 * NQV + i % w] = 0.f;
+            for (int i = lane; i < 15 * w; i += 32) sm.sG[i / w][3 * NQV + i % w] = 0.f;
         }
         __syncwarp();
         const float gm1 = a.gamma - 1.f;
@@ -627,18 +606,27 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
     // (four face references, three volume reference components, one zero)
     {
         double* sR = reinterpret_cast<double*>(&sm.sG[0][0]);
-        double am[2][2];  // A(row gid + 8 mt, column 4 kt + tq)
+        const int mq = grp.meta[tq];  // face q = tq: its map and side
+        const double sq = (mq >> 8) ? -1.0 : 1.0;
+        double am[2][2], s0[2] = {0.0, 0.0};  // A(row gid + 8 mt, column 4 kt + tq); mode-0 sums
         #pragma unroll
         for (int mt = 0; mt < 2; ++mt) {
             const int row = gid + 8 * mt, el = row / 5, k = row - 5 * el;
             const bool ok = row < 5 * ne;
-            am[mt][0] = ok ? sm.sFr[el][tq][k] : 0.0;
+            am[mt][0] = ok ? __ldcg(a.Fref + (int64_t)grp.face[el][tq] * 5 + k) : 0.0;
             am[mt][1] = (ok && a.volume && tq < 3) ? sm.sGb[el][3 * k + tq] : 0.0;
+            if (ok && tq == 0) {  // the exact mode-0 face sums, in a fixed order
+                #pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const double v = __ldcg(a.S0 + (int64_t)grp.face[el][q] * 5 + k);
+                    s0[mt] += (grp.meta[q] >> 8) ? -v : v;
+                }
+            }
         }
         #pragma unroll
         for (int nt = 0; nt < NT; ++nt) {
             const int jb = nt * 8 + gid;  // B(k = 4 kt + tq, n = jb)
-            const double b0 = jb < NB ? sm.sMF[tq][jb] : 0.0;
+            const double b0 = jb < NB ? sq * __ldg(a.t.mf + (mq & 0xff) * NB + jb) : 0.0;
             const double b1 = (jb < NB && tq < 3) ? -__ldg(a.t.mv + 3 * jb + tq) : 0.0;
             #pragma unroll
             for (int mt = 0; mt < 2; ++mt) {
@@ -646,7 +634,7 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
                 dmma884(d, am[mt][0], b0);
                 dmma884(d, am[mt][1], b1);
                 const int row = gid + 8 * mt;
-                if (nt == 0 && tq == 0 && row < 5 * ne) d[0] = sm.sS0[row / 5][row % 5];  // mode 0: exact face sums
+                if (nt == 0 && tq == 0) d[0] = s0[mt];  // mode 0 (grad phi_0 = 0): the exact face sums only
                 *reinterpret_cast<double2*>(sR + row * LDR + nt * 8 + 2 * tq) = make_double2(d[0], d[1]);
             }
         }
@@ -678,8 +666,9 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
     __syncwarp();
 }
 
+// 8 warps: four CTAs per SM (64 registers a thread); 4 warps (P4): six, at most 85 registers
 template <int NB, int NQV, int NQF, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) element_mixed(MixedElemArgs a) {
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 8 ? 4 : 6) element_mixed(MixedElemArgs a) {
     using S = ElemMixedSmem<NB, NQV, NQF>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ ElemTables<NB> tabs;
