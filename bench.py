@@ -268,7 +268,9 @@ def main():
     P, qv, qf = cfg["P"], cfg["qv"], cfg["qf"]
     m = box_mesh(cfg["n"], hi=(cfg["L"],) * 3, jitter=cfg["jitter"])
     U0 = problems.project(m, P, problem_fn(cfg["problem"], problems))
-    schedule = args.schedule or ("persistent" if args.precision == "mixed" else "two-launch")
+    # one instance: two launches per stage (face fluxes, elements) is the faster schedule; the
+    # persistent tile queue serves ensembles of uneven meshes (--config ensemble)
+    schedule = args.schedule or "two-launch"
     conv = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf,
                               precision=args.precision, device=local, schedule=schedule)
     conv.set_state(U0)
