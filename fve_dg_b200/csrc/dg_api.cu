@@ -83,6 +83,7 @@ struct dg_ctx {
     // persistent schedule (mixed form): queue state and tile parameters (chosen by dg_autotune)
     QueueState* d_queue = nullptr;
     PersistentParams pp;
+    QueueSchedule qs;
     // ensembles: instance element offsets, per-instance dt on the device, instance of each element
     int ninst = 1;
     std::vector<int64_t> inst_off;
@@ -282,7 +283,8 @@ int step(dg_ctx* c, double dt, cudaStream_t s) {
     auto tm = [&](int cls, auto&& fn) { return timed(c, cls, s, fn); };
     if (c->cfg.precision == DG_PREC_MIXED) {
         if (c->cfg.schedule == 1)
-            return step_persistent(c->mixed, c->d_queue, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm);
+            return step_persistent(c->mixed, c->d_queue, c->qs, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches,
+                                   tm);
         return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm);
     }
     return step_fp64(c, dt, s);
@@ -329,6 +331,7 @@ void free_ctx(dg_ctx* c) {
                     c->d_red, c->d_red_out};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    free_schedule(c->qs);
     free_mixed(c->mixed);
     if (c->d_queue) cudaFree(c->d_queue);
     if (c->d_dt_inst) cudaFree(c->d_dt_inst);
@@ -443,6 +446,7 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
         c->mixed.elem_inst = c->d_elem_inst;
         if (cudaMalloc((void**)&c->d_queue, sizeof(QueueState)) != cudaSuccess) return fail(c, DG_E_NOMEM);
         if (cudaMemset(c->d_queue, 0, sizeof(QueueState)) != cudaSuccess) return fail(c, DG_E_CUDA);
+        if ((rc = build_schedule(c->mixed, c->qs, c->pp))) return fail(c, rc);
     }
     if (err) *err = DG_OK;
     return c;
@@ -722,8 +726,10 @@ int dg_autotune(dg_ctx* c, double dt, char* report, size_t len) {
     double* save = nullptr;
     if (dev_alloc(&save, nstate)) return DG_E_NOMEM;
     DG_CUDA(cudaMemcpyAsync(save, c->d_Un, nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    static const int cand[][3] = {{4, 2, 0},  {8, 4, 0},  {16, 8, 0},  {32, 16, 0}, {64, 32, 0},
-                                  {16, 4, 0}, {32, 8, 0}, {8, 4, 1},   {16, 8, 1},  {32, 16, 1}};
+    // {face groups per tile, element groups per tile, CTAs per SM cap, regions, lag}
+    static const int cand[][5] = {{32, 16, 0, 32, 1}, {16, 8, 0, 32, 1}, {64, 32, 0, 32, 1}, {32, 16, 0, 16, 1},
+                                  {32, 16, 0, 64, 1}, {64, 32, 0, 64, 1}, {32, 16, 0, 32, 2}, {32, 16, 0, 64, 2},
+                                  {16, 8, 0, 64, 1},  {128, 64, 0, 64, 1}, {32, 16, 0, 8, 1}, {32, 16, 0, 1, 0}};
     const int ncand = (int)(sizeof(cand) / sizeof(cand[0]));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -739,7 +745,10 @@ int dg_autotune(dg_ctx* c, double dt, char* report, size_t len) {
         c->pp.tile_f = cand[i][0];
         c->pp.tile_e = cand[i][1];
         c->pp.max_blocks = cand[i][2];
-        rc = step(c, dt, c->stream);  // warm-up
+        c->pp.regions = cand[i][3];
+        c->pp.lag = cand[i][4];
+        rc = build_schedule(c->mixed, c->qs, c->pp);
+        if (rc == DG_OK) rc = step(c, dt, c->stream);  // warm-up
         cudaEventRecord(e0, c->stream);
         for (int r = 0; r < 2 && rc == DG_OK; ++r) rc = step(c, dt, c->stream);
         cudaEventRecord(e1, c->stream);
@@ -750,12 +759,18 @@ int dg_autotune(dg_ctx* c, double dt, char* report, size_t len) {
         ms *= 0.5f;
         js += std::string(i ? ", " : "") + "{\"tile_f\": " + std::to_string(cand[i][0]) + ", \"tile_e\": " +
               std::to_string(cand[i][1]) + ", \"max_blocks_per_sm\": " + std::to_string(cand[i][2]) +
+              ", \"regions\": " + std::to_string(c->qs.nregions) + ", \"lag\": " + std::to_string(cand[i][4]) +
               ", \"ms_per_step\": " + std::to_string(ms) + "}";
         if (rc == DG_OK && ms < best) { best = ms; bestp = c->pp; }
     }
     c->pp = bestp;
+    {
+        const int brc = build_schedule(c->mixed, c->qs, c->pp);
+        if (rc == DG_OK) rc = brc;
+    }
     js += "], \"chosen\": {\"tile_f\": " + std::to_string(bestp.tile_f) + ", \"tile_e\": " +
           std::to_string(bestp.tile_e) + ", \"max_blocks_per_sm\": " + std::to_string(bestp.max_blocks) +
+          ", \"regions\": " + std::to_string(c->qs.nregions) + ", \"lag\": " + std::to_string(bestp.lag) +
           ", \"ms_per_step\": " + std::to_string(best) + "}}";
     cudaMemcpyAsync(c->d_Un, save, nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
     mixed_mirror(c->mixed, c->d_Un, 0, c->stream, &g_launches);

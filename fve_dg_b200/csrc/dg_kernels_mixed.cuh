@@ -705,6 +705,10 @@ struct MixedData {
     const int* elem_inst = nullptr;
     // A rows of the deviation coefficients of the states Un, Ua, Ub and of a residual input
     uint32_t* mir[4] = {nullptr, nullptr, nullptr, nullptr};
+    // host copies the tile schedule of the persistent form is built from
+    std::vector<FaceGroup> hfg;
+    std::vector<ElemGroup> heg;
+    std::vector<int> hface_cells;  // [nface][2]
 };
 
 // X(order, qv, qf, NB, NQV, NQF, W): W warps per block of the element kernel
@@ -883,6 +887,13 @@ inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>
     m.nfgroups = (int)fg.size();
     m.negroups = (int)eg.size();
     if ((rc = mixed_upload(m, &m.fgroups, fg)) || (rc = mixed_upload(m, &m.egroups, eg))) return rc;
+    m.hfg = fg;
+    m.heg = eg;
+    m.hface_cells.resize(2 * hfi.size());
+    for (size_t f = 0; f < hfi.size(); ++f) {
+        m.hface_cells[2 * f] = hfi[f].c0;
+        m.hface_cells[2 * f + 1] = hfi[f].c1;
+    }
     // padding columns of the A rows stay zero: allocation clears them and no kernel writes them
     if ((rc = mixed_alloc(m, &m.dev, (size_t)nface * 5 * KF)) || (rc = mixed_alloc(m, &m.Fref, (size_t)nface * 5)) ||
         (rc = mixed_alloc(m, &m.S0, (size_t)nface * 5)))

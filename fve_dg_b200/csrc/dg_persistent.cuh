@@ -1,52 +1,56 @@
-// Persistent form of one RK stage: a single cooperative launch whose CTAs pull tiles of work from
-// two queues — face groups first, then element groups — separated by a grid-wide barrier. The
-// queues are plain atomic tickets, so CTAs that finish early take more tiles and uneven work (an
-// ensemble of meshes of different sizes laid end to end) balances itself. Each RK stage is one
-// launch; a CUDA graph captures the three launches of a step.
+// Persistent, dependency-driven form of one RK stage: one launch whose CTAs take tickets over a
+// single list of tiles in which face tiles and element tiles are interleaved region by region, so
+// the face work (instruction-bound: traces, Riemann solver) and the element work (bound by memory
+// latency: face data, state, update) share the SMs instead of running one after the other.
 //
-// Every wait is bounded: a CTA that spins at the barrier longer than kSpinLimit polls records
-// DG_E_WATCHDOG in the queue state and continues, the host reads that word after the step and
-// reports the error. The launch is cooperative, so all CTAs are co-resident by construction.
+// The element groups are cut into R regions of consecutive groups. A face group belongs to the
+// lowest region among the cells of its faces. An element tile of region r may start once every
+// face region its elements read is complete; the host places it in the list `lag` face regions
+// after the last of those, so by the time a CTA takes it the faces are normally done. Face tiles
+// wait for nothing. Since a tile is taken only by a running CTA and every tile an element tile
+// waits for was taken before it, every wait ends; no cooperative launch is needed, and uneven work
+// (an ensemble of meshes of different sizes laid end to end) balances itself.
+//
+// Every wait is bounded: a CTA that spins longer than kSpinLimit polls records DG_E_WATCHDOG in
+// the queue state and goes on; the host reads that word after the step and reports the error. The
+// last CTA to leave re-arms the ticket and the completion counters for the next launch, so a CUDA
+// graph replays the three launches of a step as they are.
 #pragma once
 #include "dg_kernels_mixed.cuh"
 
 namespace fvedg {
 
+constexpr int kMaxRegions = 64;
+
 struct QueueState {
-    unsigned int ctr[2];     // tickets of the face and element queues
-    unsigned int bar_count;  // grid barrier: arrivals
-    unsigned int bar_gen;    // grid barrier: generation
-    int error;               // DG_OK or DG_E_WATCHDOG
-    int pad[3];
+    unsigned int ticket;              // next tile of the list
+    unsigned int exits;               // CTAs that have left this launch
+    int error;                        // DG_OK or DG_E_WATCHDOG
+    int pad;
+    unsigned int done[kMaxRegions];   // face groups completed, per region
 };
 
 constexpr long long kSpinLimit = 1ll << 24;  // about a second of 64 ns naps
 
-__device__ __forceinline__ void grid_barrier(QueueState* q, unsigned int nblocks) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int* vgen = &q->bar_gen;
-        const unsigned int gen = *vgen;
-        __threadfence();
-        const unsigned int arrived = atomicAdd(&q->bar_count, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(&q->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&q->bar_gen, 1u);
-        } else {
-            long long spins = 0;
-            while (*vgen == gen) {
-                __nanosleep(64);
-                if (++spins > kSpinLimit) {
-                    atomicExch(&q->error, DG_E_WATCHDOG);
-                    break;
-                }
-            }
-        }
-        __threadfence();
+struct PersistentParams {
+    int tile_f = 32;     // face groups per tile
+    int tile_e = 16;     // element groups per tile
+    int max_blocks = 0;  // CTAs per SM cap (0 = as many as fit)
+    int regions = 32;    // element regions (1 .. kMaxRegions)
+    int lag = 1;         // face regions between an element tile's last dependency and its place
+    bool operator==(const PersistentParams& o) const {
+        return tile_f == o.tile_f && tile_e == o.tile_e && regions == o.regions && lag == o.lag;
     }
-    __syncthreads();
-}
+};
+
+struct QueueSchedule {
+    int4* tiles = nullptr;              // {kind (0 face, 1 element), first group, end group, region}
+    unsigned long long* deps = nullptr; // [R] face regions each element region reads
+    unsigned int* total = nullptr;      // [R] face groups per region
+    int ntiles = 0, nregions = 0;
+    PersistentParams built{};
+    bool ready = false;
+};
 
 template <int NB, int NQV, int NQF>
 __host__ __device__ constexpr size_t persistent_warp_smem() {
@@ -54,56 +58,164 @@ __host__ __device__ constexpr size_t persistent_warp_smem() {
     return ((a > b ? a : b) + 15) / 16 * 16;
 }
 
-// Phase 1 takes tickets over face-group tiles; phase 2 takes tickets over element-group tiles
-// (volume term, face integrals and the update).
 template <int NB, int NQV, int NQF, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32)
-    stage_persistent_mixed(MixedFaceArgs fa, MixedElemArgs ea, QueueState* q, int tile_f, int tile_e) {
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 8 ? 4 : 6)
+    stage_persistent_mixed(MixedFaceArgs fa, MixedElemArgs ea, QueueState* q, const int4* __restrict__ tiles,
+                           int ntiles, const unsigned long long* __restrict__ deps,
+                           const unsigned int* __restrict__ total) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int s_tile;
+    __shared__ ElemTables<NB> tabs;
+    __shared__ int4 s_tile;
+    element_tables_init(tabs, ea.t.inv_mass);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* wsm = smem_raw + persistent_warp_smem<NB, NQV, NQF>() * warp;
     for (;;) {
-        if (threadIdx.x == 0) s_tile = (int)atomicAdd(&q->ctr[0], 1u);
+        if (threadIdx.x == 0) {
+            const unsigned int t = atomicAdd(&q->ticket, 1u);
+            int4 tl = t < (unsigned int)ntiles ? tiles[t] : make_int4(-1, 0, 0, 0);
+            if (tl.x == 1) {  // element tile: wait until the face regions it reads are complete
+                unsigned long long need = deps[tl.w];
+                while (need) {
+                    const int f = __ffsll((long long)need) - 1;
+                    const volatile unsigned int* d = &q->done[f];
+                    long long spins = 0;
+                    while (*d < total[f]) {
+                        __nanosleep(64);
+                        if (++spins > kSpinLimit) {
+                            atomicExch(&q->error, DG_E_WATCHDOG);
+                            break;
+                        }
+                    }
+                    need &= need - 1;
+                }
+                __threadfence();
+            }
+            s_tile = tl;
+        }
         __syncthreads();
-        const int g0 = s_tile * tile_f;
-        __syncthreads();
-        if (g0 >= fa.ngroups) break;
-        const int g1 = min(g0 + tile_f, fa.ngroups);
-        for (int gi = g0 + warp; gi < g1; gi += WARPS)
-            face_group_mixed<NB, NQF>(fa, gi, *reinterpret_cast<FaceMixedSmem<NQF>*>(wsm), lane);
+        const int4 tl = s_tile;
+        if (tl.x < 0) break;
+        if (tl.x == 0) {
+            for (int gi = tl.y + warp; gi < tl.z; gi += WARPS)
+                face_group_mixed<NB, NQF>(fa, gi, *reinterpret_cast<FaceMixedSmem<NQF>*>(wsm), lane);
+            __threadfence();  // this CTA's face data is visible before the region count moves
+            __syncthreads();
+            if (threadIdx.x == 0) atomicAdd(&q->done[tl.w], (unsigned int)(tl.z - tl.y));
+        } else {
+            auto& esm = *reinterpret_cast<ElemMixedSmem<NB, NQV, NQF>*>(wsm);
+            for (int gi = tl.y + warp; gi < tl.z; gi += WARPS) element_group_mixed<NB, NQV, NQF>(ea, gi, esm, tabs, lane);
+            __syncthreads();
+        }
     }
-    grid_barrier(q, gridDim.x);
-    auto& esm = *reinterpret_cast<ElemMixedSmem<NB, NQV, NQF>*>(wsm);
-    __shared__ ElemTables<NB> tabs;
-    element_tables_init(tabs, ea.t.inv_mass);
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = (int)atomicAdd(&q->ctr[1], 1u);
-        __syncthreads();
-        const int g0 = s_tile * tile_e;
-        __syncthreads();
-        if (g0 >= ea.ngroups) break;
-        const int g1 = min(g0 + tile_e, ea.ngroups);
-        for (int gi = g0 + warp; gi < g1; gi += WARPS) element_group_mixed<NB, NQV, NQF>(ea, gi, esm, tabs, lane);
-    }
-    grid_barrier(q, gridDim.x);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {  // every CTA is past both queues: rearm them
-        q->ctr[0] = 0u;
-        q->ctr[1] = 0u;
+    if (threadIdx.x == 0) {  // the last CTA out re-arms the queue
         __threadfence();
+        if (atomicAdd(&q->exits, 1u) == gridDim.x - 1) {
+            q->ticket = 0u;
+            for (int r = 0; r < kMaxRegions; ++r) q->done[r] = 0u;
+            __threadfence();
+            q->exits = 0u;
+        }
     }
 }
 
-struct PersistentParams {
-    int tile_f = 16;     // face groups per ticket
-    int tile_e = 8;      // element groups per ticket
-    int max_blocks = 0;  // CTAs per SM cap (0 = as many as fit)
-};
+// Builds the tile list for `pp`: reorders the face groups by region (the face kernel of the
+// two-launch form does not depend on their order) and uploads the list. Synchronous: call outside
+// any stream capture (context creation, the autotuner).
+inline int build_schedule(MixedData& m, QueueSchedule& qs, const PersistentParams& pp) {
+    const int ne = m.negroups, nf = m.nfgroups;
+    if (ne < 1 || nf < 1) return DG_E_ARG;
+    const int R = std::max(1, std::min({pp.regions, kMaxRegions, ne}));
+    const int tf = std::max(1, pp.tile_f), te = std::max(1, pp.tile_e), lag = std::max(0, pp.lag);
+    std::vector<int> ereg(m.ncell, 0), greg(ne);
+    for (int g = 0; g < ne; ++g) {
+        greg[g] = (int)((int64_t)g * R / ne);
+        for (int i = 0; i < m.heg[g].n; ++i) ereg[m.heg[g].e[i]] = greg[g];
+    }
+    // face groups by region (lowest region among their cells), stable within a region
+    std::vector<int> freg(nf);
+    for (int g = 0; g < nf; ++g) {
+        int r = R;
+        for (int i = 0; i < m.hfg[g].n; ++i) {
+            const int f = m.hfg[g].f[i];
+            r = std::min(r, ereg[m.hface_cells[2 * f]]);
+            if (m.hface_cells[2 * f + 1] >= 0) r = std::min(r, ereg[m.hface_cells[2 * f + 1]]);
+        }
+        freg[g] = r;
+    }
+    std::vector<int> order(nf);
+    for (int g = 0; g < nf; ++g) order[g] = g;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return freg[x] < freg[y]; });
+    std::vector<FaceGroup> fg(nf);
+    std::vector<int> fg_reg(nf), face_reg(m.nface, 0);
+    std::vector<unsigned int> total(R, 0u);
+    for (int i = 0; i < nf; ++i) {
+        fg[i] = m.hfg[order[i]];
+        fg_reg[i] = freg[order[i]];
+        ++total[fg_reg[i]];
+        for (int k = 0; k < fg[i].n; ++k) face_reg[fg[i].f[k]] = fg_reg[i];
+    }
+    std::vector<unsigned long long> deps(R, 0ull);
+    for (int g = 0; g < ne; ++g)
+        for (int i = 0; i < m.heg[g].n; ++i)
+            for (int q = 0; q < 4; ++q) deps[greg[g]] |= 1ull << face_reg[m.heg[g].face[i][q]];
+    // element region r goes after face region min(last dependency + lag, R - 1)
+    std::vector<std::vector<int>> after(R);
+    for (int r = 0; r < R; ++r) {
+        int last = 0;
+        for (int b = 0; b < R; ++b)
+            if (deps[r] >> b & 1ull) last = b;
+        after[std::min(last + lag, R - 1)].push_back(r);
+    }
+    std::vector<int> ebeg(R + 1, ne), fbeg(R + 1, nf);
+    for (int g = ne - 1; g >= 0; --g) ebeg[greg[g]] = g;
+    for (int i = nf - 1; i >= 0; --i) fbeg[fg_reg[i]] = i;
+    for (int r = R - 1; r >= 0; --r) {
+        ebeg[r] = std::min(ebeg[r], ebeg[r + 1]);
+        fbeg[r] = std::min(fbeg[r], fbeg[r + 1]);
+    }
+    std::vector<int4> tiles;
+    for (int x = 0; x < R; ++x) {
+        for (int g = fbeg[x]; g < fbeg[x + 1]; g += tf) tiles.push_back(make_int4(0, g, std::min(g + tf, fbeg[x + 1]), x));
+        for (int r : after[x])
+            for (int g = ebeg[r]; g < ebeg[r + 1]; g += te)
+                tiles.push_back(make_int4(1, g, std::min(g + te, ebeg[r + 1]), r));
+    }
+    // upload: the reordered face groups into the existing buffer, the schedule into fresh ones
+    if (cudaMemcpy((void*)m.fgroups, fg.data(), sizeof(FaceGroup) * nf, cudaMemcpyHostToDevice) != cudaSuccess)
+        return DG_E_CUDA;
+    m.hfg = fg;
+    if (qs.tiles) cudaFree(qs.tiles);
+    if (qs.deps) cudaFree(qs.deps);
+    if (qs.total) cudaFree(qs.total);
+    qs.tiles = nullptr; qs.deps = nullptr; qs.total = nullptr;
+    qs.ready = false;
+    if (cudaMalloc((void**)&qs.tiles, sizeof(int4) * tiles.size()) != cudaSuccess ||
+        cudaMalloc((void**)&qs.deps, sizeof(unsigned long long) * R) != cudaSuccess ||
+        cudaMalloc((void**)&qs.total, sizeof(unsigned int) * R) != cudaSuccess)
+        return DG_E_NOMEM;
+    if (cudaMemcpy(qs.tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(qs.deps, deps.data(), sizeof(unsigned long long) * R, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(qs.total, total.data(), sizeof(unsigned int) * R, cudaMemcpyHostToDevice) != cudaSuccess)
+        return DG_E_CUDA;
+    qs.ntiles = (int)tiles.size();
+    qs.nregions = R;
+    qs.built = pp;
+    qs.ready = true;
+    return DG_OK;
+}
+
+inline void free_schedule(QueueSchedule& qs) {
+    if (qs.tiles) cudaFree(qs.tiles);
+    if (qs.deps) cudaFree(qs.deps);
+    if (qs.total) cudaFree(qs.total);
+    qs = QueueSchedule{};
+}
 
 template <int NB, int NQV, int NQF, int W = 8>
-inline int persistent_launch(MixedData& m, QueueState* q, const PersistentParams& pp, const double* U,
-                             const double* U0, double* out, int mode, double dt, double a0, double a1, int face_mask,
-                             int with_volume, cudaStream_t s, int mir_in, int mir_out) {
+inline int persistent_launch(MixedData& m, QueueState* q, const QueueSchedule& qs, const PersistentParams& pp,
+                             const double* U, const double* U0, double* out, int mode, double dt, double a0, double a1,
+                             int face_mask, int with_volume, cudaStream_t s, int mir_in, int mir_out) {
+    if (!qs.ready || !(qs.built == pp)) return DG_E_STATE;
     auto kern = stage_persistent_mixed<NB, NQV, NQF, W>;
     constexpr size_t smem = persistent_warp_smem<NB, NQV, NQF>() * W;
     static unsigned long long done = 0;
@@ -122,38 +234,29 @@ inline int persistent_launch(MixedData& m, QueueState* q, const PersistentParams
     const int bps = pp.max_blocks > 0 ? std::min(per_sm[dev & 63], pp.max_blocks) : per_sm[dev & 63];
     const MixedFaceArgs fa = face_args(m, U, mir_in, face_mask);
     const MixedElemArgs ea = elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out);
-    int tf = pp.tile_f, te = pp.tile_e;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(m.sms * bps);
-    cfg.blockDim = dim3(W * 32);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, kern, fa, ea, q, tf, te) != cudaSuccess) return DG_E_CUDA;
-    return DG_OK;
+    kern<<<m.sms * bps, W * 32, smem, s>>>(fa, ea, q, qs.tiles, qs.ntiles, qs.deps, qs.total);
+    return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;
 }
 
-inline int persistent_kernel(MixedData& m, QueueState* q, const PersistentParams& pp, const double* U,
-                             const double* U0, double* out, int mode, double dt, double a0, double a1, int face_mask,
-                             int with_volume, cudaStream_t s, std::atomic<int64_t>* launches, int mir_in, int mir_out) {
+inline int persistent_kernel(MixedData& m, QueueState* q, const QueueSchedule& qs, const PersistentParams& pp,
+                             const double* U, const double* U0, double* out, int mode, double dt, double a0, double a1,
+                             int face_mask, int with_volume, cudaStream_t s, std::atomic<int64_t>* launches, int mir_in,
+                             int mir_out) {
     if (!m.ready) return DG_E_ARG;
     ++*launches;
-#define X(P, QV, QF, NB, NQV, NQF, W)                                                                             \
-    if (m.order == P && m.qv == QV && m.qf == QF)                                                                 \
-        return persistent_launch<NB, NQV, NQF>(m, q, pp, U, U0, out, mode, dt, a0, a1, face_mask, with_volume, s, \
-                                               mir_in, mir_out);
+#define X(P, QV, QF, NB, NQV, NQF, W)                                                                              \
+    if (m.order == P && m.qv == QV && m.qf == QF)                                                                  \
+        return persistent_launch<NB, NQV, NQF, W>(m, q, qs, pp, U, U0, out, mode, dt, a0, a1, face_mask,           \
+                                                  with_volume, s, mir_in, mir_out);
     FVEDG_MIXED_COMBOS(X)
 #undef X
     return DG_E_ARG;
 }
 
 template <class Timed>
-inline int step_persistent(MixedData& m, QueueState* q, const PersistentParams& pp, double* Un, double* Ua,
-                           double* Ub, double dt, cudaStream_t s, std::atomic<int64_t>* launches, Timed&& timed) {
+inline int step_persistent(MixedData& m, QueueState* q, const QueueSchedule& qs, const PersistentParams& pp,
+                           double* Un, double* Ua, double* Ub, double dt, cudaStream_t s,
+                           std::atomic<int64_t>* launches, Timed&& timed) {
     const double A0[3] = {0.0, 0.75, 1.0 / 3.0};
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
     const double* in[3] = {Un, Ua, Ub};
@@ -161,8 +264,8 @@ inline int step_persistent(MixedData& m, QueueState* q, const PersistentParams& 
     const int mi[3] = {0, 1, 2}, mo[3] = {1, 2, 0};
     for (int st = 0; st < 3; ++st) {
         const int rc = timed(2, [&] {
-            return persistent_kernel(m, q, pp, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches, mi[st],
-                                     mo[st]);
+            return persistent_kernel(m, q, qs, pp, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches,
+                                     mi[st], mo[st]);
         });
         if (rc) return rc;
     }
