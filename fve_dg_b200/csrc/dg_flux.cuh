@@ -116,4 +116,107 @@ struct Phys {
     }
 };
 
+// FP32 forms for the mixed-precision kernels: the same fluxes as Phys<float>, reorganised for fewer
+// instructions. The momenta are used directly (rho u = m, rho u.n = m.n, rho e = E), each state
+// costs one reciprocal, square roots come from the hardware reciprocal square root (the arguments
+// are clamped positive), and the Roe dissipation shares its subexpressions:
+//   D_0 = W, D_{1+i} = W u~_i + c~ (w5 - w1) n_i + |u~.n| r~ (du_i - du.n n_i),
+//   D_4 = (w1 + w5) H~ + c~ (w5 - w1) u~.n + w2 |u~|^2 / 2 + |u~.n| r~ u~.(du - du.n n),
+// with W = w1 + w2 + w5, which is the wave sum of Phys::roe term by term.
+struct StateF32 {
+    float r, ir, u[3], p, e, un, mn;  // clamped density, 1/rho, velocity, pressure, E + p, u.n, m.n
+};
+
+__device__ __forceinline__ float rcp_f32(float x) { return __fdividef(1.f, x); }
+
+__device__ __forceinline__ StateF32 state_f32(const float U[5], const float n[3], float gm1) {
+    StateF32 s;
+    s.r = fmaxf(U[0], 1e-16f);
+    s.ir = rcp_f32(s.r);
+    #pragma unroll
+    for (int i = 0; i < 3; ++i) s.u[i] = U[1 + i] * s.ir;
+    const float k = s.u[0] * U[1] + s.u[1] * U[2] + s.u[2] * U[3];  // rho |u|^2
+    s.p = gm1 * fmaf(-0.5f, k, U[4]);
+    s.e = U[4] + s.p;
+    s.mn = U[1] * n[0] + U[2] * n[1] + U[3] * n[2];
+    s.un = s.mn * s.ir;
+    return s;
+}
+
+__device__ __forceinline__ void roe_f32(const float UL[5], const float UR[5], const float n[3], float gam, float Fh[5]) {
+    const float gm1 = gam - 1.f;
+    const StateF32 L = state_f32(UL, n, gm1), R = state_f32(UR, n, gm1);
+    const float qL = rsqrtf(L.r), qR = rsqrtf(R.r);
+    const float sL = L.r * qL, sR = R.r * qR;  // sqrt(rho)
+    const float iden = rcp_f32(sL + sR);
+    const float wL = sL * iden, wR = sR * iden;
+    float ut[3];
+    #pragma unroll
+    for (int i = 0; i < 3; ++i) ut[i] = fmaf(wL, L.u[i], wR * R.u[i]);
+    const float Ht = fmaf(wL, L.e * L.ir, wR * (R.e * R.ir));
+    const float q2 = ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2];
+    const float c2 = fmaxf(gm1 * fmaf(-0.5f, q2, Ht), 1e-16f);
+    const float qc = rsqrtf(c2);
+    const float ct = c2 * qc, ic2 = qc * qc;
+    const float rt = sL * sR;
+    const float unt = ut[0] * n[0] + ut[1] * n[1] + ut[2] * n[2];
+    const float dr = R.r - L.r, dp = R.p - L.p, dun = R.un - L.un;
+    float l1 = fabsf(unt - ct), l5 = fabsf(unt + ct);
+    const float l2 = fabsf(unt);
+    const float delta = 0.1f * ct, d2 = delta * delta, ihd = __fdividef(0.5f, delta);
+    if (l1 < delta) l1 = fmaf(l1, l1, d2) * ihd;
+    if (l5 < delta) l5 = fmaf(l5, l5, d2) * ihd;
+    const float rcd = rt * ct * dun, h2 = 0.5f * ic2;
+    const float w1 = l1 * ((dp - rcd) * h2), w5 = l5 * ((dp + rcd) * h2), w2 = l2 * fmaf(-dp, ic2, dr);
+    const float W = w1 + w5 + w2, cw = ct * (w5 - w1), lrt = l2 * rt;
+    float uds = 0.f, D[5];
+    D[0] = W;
+    #pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float sh = fmaf(-dun, n[i], R.u[i] - L.u[i]);
+        uds = fmaf(ut[i], sh, uds);
+        D[1 + i] = fmaf(W, ut[i], fmaf(cw, n[i], lrt * sh));
+    }
+    D[4] = fmaf(w1 + w5, Ht, fmaf(cw, unt, fmaf(0.5f * w2, q2, lrt * uds)));
+    const float ps = L.p + R.p;
+    Fh[0] = 0.5f * (L.mn + R.mn - D[0]);
+    #pragma unroll
+    for (int i = 0; i < 3; ++i) Fh[1 + i] = 0.5f * (fmaf(UL[1 + i], L.un, fmaf(UR[1 + i], R.un, ps * n[i])) - D[1 + i]);
+    Fh[4] = 0.5f * (fmaf(L.un, L.e, R.un * R.e) - D[4]);
+}
+
+__device__ __forceinline__ void lax_friedrichs_f32(const float UL[5], const float UR[5], const float n[3], float gam,
+                                                   float Fh[5]) {
+    const float gm1 = gam - 1.f;
+    const StateF32 L = state_f32(UL, n, gm1), R = state_f32(UR, n, gm1);
+    auto speed = [&](const StateF32& s) {
+        const float v2 = s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2];
+        const float c2 = fmaxf(gam * fmaxf(s.p * s.ir, 1e-16f), 1e-16f);
+        const float v = v2 > 0.f ? v2 * rsqrtf(v2) : 0.f;
+        return v + c2 * rsqrtf(c2);
+    };
+    const float lam = fmaxf(speed(L), speed(R));
+    Fh[0] = 0.5f * fmaf(lam, UL[0] - UR[0], L.mn + R.mn);
+    const float ps = L.p + R.p;
+    #pragma unroll
+    for (int i = 0; i < 3; ++i)
+        Fh[1 + i] = 0.5f * fmaf(lam, UL[1 + i] - UR[1 + i], fmaf(UL[1 + i], L.un, fmaf(UR[1 + i], R.un, ps * n[i])));
+    Fh[4] = 0.5f * fmaf(lam, UL[4] - UR[4], fmaf(L.un, L.e, R.un * R.e));
+}
+
+// Full 5 x 3 flux in FP32 (row = variable, column = direction), momenta used directly.
+__device__ __forceinline__ void flux_f32(const float U[5], float gm1, float F[5][3]) {
+    const float r = fmaxf(U[0], 1e-16f), ir = rcp_f32(r);
+    const float u[3] = {U[1] * ir, U[2] * ir, U[3] * ir};
+    const float p = gm1 * fmaf(-0.5f, u[0] * U[1] + u[1] * U[2] + u[2] * U[3], U[4]);
+    const float e = U[4] + p;
+    #pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        F[0][d] = U[1 + d];
+        #pragma unroll
+        for (int i = 0; i < 3; ++i) F[1 + i][d] = U[1 + i] * u[d] + (i == d ? p : 0.f);
+        F[4][d] = u[d] * e;
+    }
+}
+
 }  // namespace fvedg

@@ -358,8 +358,8 @@ __device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi,
         }
         const float n[3] = {sm.sN[fl][0], sm.sN[fl][1], sm.sN[fl][2]};
         float Fh[5];
-        if (a.flux == 1) Phys<float>::roe(UL, UR, n, a.gamma, Fh);
-        else Phys<float>::lax_friedrichs(UL, UR, n, a.gamma, Fh);
+        if (a.flux == 1) roe_f32(UL, UR, n, a.gamma, Fh);
+        else lax_friedrichs_f32(UL, UR, n, a.gamma, Fh);
         const float jw = sm.sN[fl][3], w = __ldg(a.t.wf32 + g);
         unsigned short* drow = reinterpret_cast<unsigned short*>(a.dev + (int64_t)f * 5 * KF);
         const int hw = 2 * arow_hi_word<KF>(g) + (g & 1), lw = 2 * arow_lo_word<KF>(g) + (g & 1);
@@ -543,7 +543,7 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
             float U[5], F[5][3];
             #pragma unroll
             for (int k = 0; k < 5; ++k) U[k] = sm.sU[el * 5 + k][g];
-            Phys<float>::flux(U, gm1, F);
+            flux_f32(U, gm1, F);
             const float* J = sm.sJ[el];
             #pragma unroll
             for (int k = 0; k < 5; ++k)
@@ -652,7 +652,9 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
         if (a.mode == 0) {
             a.out[idx] = R;
         } else {
-            const double un = a.a0 * a.U0[idx] + a.a1 * (__ldg(a.U + idx) - sm.sDT[el] * T.inv_mass[d.x] * R);
+            // stage 1 has a0 = 0: U^n is not read twice
+            const double u0 = a.a0 != 0.0 ? a.a0 * a.U0[idx] : 0.0;
+            const double un = u0 + a.a1 * (__ldg(a.U + idx) - sm.sDT[el] * T.inv_mass[d.x] * R);
             a.out[idx] = un;
             if (d.x > 0) {
                 unsigned short h, l;
