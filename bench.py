@@ -31,9 +31,9 @@ CONFIGS = {
     "tgv": dict(problem="taylor_green", n=48, L=2 * np.pi, jitter=0.0, P=3, qv=3, qf=3, flux="Roe",
                 desc="Taylor-Green Ma 0.1, [0,2pi]^3 periodic, 48^3x6=663,552 tets, P3, "
                      "Degree6Points23/Degree10Points24, Roe, SSP-RK3 CFL 0.3"),
-    "dwave": dict(problem="density_wave", n=32, L=1.0, jitter=0.1, P=2, qv=1, qf=3, flux="LF",
+    "dwave": dict(problem="density_wave", n=32, L=1.0, jitter=0.1, P=2, qv=1, qf=2, flux="LF",
                   desc="density wave, [0,1]^3 periodic, 32^3x6=196,608 jittered tets, P2, "
-                       "Degree4Points11/Degree10Points24 (the first triangle rule exact to degree 5), LF, "
+                       "Degree4Points11/Degree4Points7 (the 7-point triangle rule is exact to degree 5), LF, "
                        "SSP-RK3 CFL 0.3"),
     "vortex": dict(problem="vortex", n=8, L=10.0, jitter=0.0, P=1, qv=0, qf=1, flux="LF",
                    desc="isentropic vortex, [0,10]^3 periodic, 8^3x6=3,072 tets, P1, "
@@ -50,6 +50,10 @@ CFL = 0.3
 # Algorithmic minimum HBM bytes per DOF-stage of one SSP-RK3 stage: read U^(i) and U^n, write U^(i+1)
 # (24 B per DOF) plus the per-element geometry and the per-face trace data, amortised over the DOFs.
 MIN_BYTES_PER_DOF_STAGE = {1: 32.2, 2: 27.3, 3: 25.6, 4: 24.9}
+# Algorithmic flops per DOF-stage of the same stage at the configs' rules: volume interpolation and
+# projection, the flux at the volume and face points, the face traces and integrals, the update.
+FLOP_PER_DOF_STAGE = {1: 219.0, 2: 262.0, 3: 651.0, 4: 801.0}
+FP64_NOMINAL_TFLOPS = 40.0  # B200 FP64 (vector and tensor), the bound of the FP64 form
 
 
 def problem_fn(name, problems):
@@ -212,16 +216,36 @@ def cpu_baseline(cfg):
     rm = RefMesh.from_mesh(ref, m)
     b = rm.mass(P, qv)
     U = rm.ssprk3(U, b, P, qv, qf, 1e-4, 1)  # warm-up step
-    k, t0 = 0, time.perf_counter()
-    while True:
-        U = rm.ssprk3(U, b, P, qv, qf, 1e-4, 1)
-        k += 1
-        if time.perf_counter() - t0 > 10.0 or k >= 50:
-            break
-    el = time.perf_counter() - t0
-    return {"value": 5 * nb_of(P) * m.ncell * 3 * k / el, "unit": "DOF-stage/s", "cores": threads,
-            "kind": "reference",
-            "sample": f"{cfg['problem']} P{P}, {n_s}^3x6={m.ncell} tets, {k} SSP-RK3 steps (LF flux), {el:.1f} s"}
+
+    def rate(seconds, max_steps):
+        nonlocal U
+        k, t0 = 0, time.perf_counter()
+        while True:
+            U = rm.ssprk3(U, b, P, qv, qf, 1e-4, 1)
+            k += 1
+            if time.perf_counter() - t0 > seconds or k >= max_steps:
+                break
+        el = time.perf_counter() - t0
+        return 5 * nb_of(P) * m.ncell * 3 * k / el, k, el
+
+    val, k, el = rate(10.0, 50)
+    ref.set_threads(1)
+    val1, k1, el1 = rate(4.0, 20)
+    ref.set_threads(threads)
+    return {"value": val, "unit": "DOF-stage/s", "cores": threads, "kind": "reference",
+            "sample": f"{cfg['problem']} P{P}, {n_s}^3x6={m.ncell} tets, {k} SSP-RK3 steps (LF flux), {el:.1f} s",
+            "value_1_thread": val1, "sample_1_thread": f"{k1} steps, {el1:.1f} s", "cpu_model": cpu_model()}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def main():
@@ -412,7 +436,12 @@ def make_roofline(kt, precision, schedule, P, ncell, nface, nqf, nb, config):
             "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": b, "avg_launch_ms": dom_ms,
             "stage": {"ms": stage_ms, "bytes_per_dof_stage_min": MIN_BYTES_PER_DOF_STAGE[P],
                       "achieved_gbs_at_min_bytes": MIN_BYTES_PER_DOF_STAGE[P] * 5 * nb * ncell
-                      / (stage_ms / 1e3) / 1e9},
+                      / (stage_ms / 1e3) / 1e9,
+                      "flop_per_dof_stage": FLOP_PER_DOF_STAGE[P],
+                      "achieved_tflops": FLOP_PER_DOF_STAGE[P] * 5 * nb * ncell / (stage_ms / 1e3) / 1e12,
+                      "fp64_nominal_tflops": FP64_NOMINAL_TFLOPS,
+                      "frac_of_fp64_nominal": FLOP_PER_DOF_STAGE[P] * 5 * nb * ncell / (stage_ms / 1e3) / 1e12
+                      / FP64_NOMINAL_TFLOPS},
             "kernels_ms_per_launch": {names.get(k, str(k)): v[0] / v[1] for k, v in kt.items()}}
 
 
