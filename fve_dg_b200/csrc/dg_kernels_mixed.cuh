@@ -959,8 +959,8 @@ inline int mixed_launch(MixedData& m, int which, const double* U, const double* 
         const int64_t n = m.ncell * 5 * (pad8(NB - 1) / 2);
         mirror_split<NB><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(U, m.mir[mir_in], m.ncell);
     } else if (which == 0) {
-        constexpr int W = 8;
-        const int g = (int)std::min<int64_t>((m.nfgroups + W - 1) / W, (int64_t)m.sms * 32);
+        constexpr int W = 4;  // 4-warp CTAs: finer-grained scheduling than 8 at the same occupancy
+        const int g = (int)std::min<int64_t>((m.nfgroups + W - 1) / W, (int64_t)m.sms * 64);
         face_flux_mixed<NB, NQF, W><<<g, W * 32, 0, s>>>(face_args(m, U, mir_in, face_mask));
     } else {
         constexpr size_t smem = sizeof(ElemMixedSmem<NB, NQV, NQF>) * WE;
