@@ -16,7 +16,7 @@ c_int_p = ctypes.POINTER(ctypes.c_int)
 
 DG_OK = 0
 STATUS = {0: "DG_OK", -1: "DG_E_ARG", -2: "DG_E_MESH", -3: "DG_E_CUDA", -4: "DG_E_NOMEM",
-          -5: "DG_E_NONPHYSICAL", -6: "DG_E_WATCHDOG", -7: "DG_E_STATE"}
+          -5: "DG_E_NONPHYSICAL", -6: "DG_E_WATCHDOG", -7: "DG_E_STATE", -8: "DG_E_IO"}
 
 
 class DGError(RuntimeError):
@@ -39,7 +39,7 @@ class MeshDesc(ctypes.Structure):
 class Config(ctypes.Structure):
     _fields_ = [("order", ctypes.c_int), ("flux", ctypes.c_int), ("quad_vol", ctypes.c_int),
                 ("quad_face", ctypes.c_int), ("gamma", ctypes.c_double), ("precision", ctypes.c_int),
-                ("device", ctypes.c_int), ("schedule", ctypes.c_int)]
+                ("device", ctypes.c_int), ("schedule", ctypes.c_int), ("limiter", ctypes.c_int)]
 
 
 _lib = None
@@ -65,6 +65,10 @@ def lib():
         "dg_ssprk3": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
         "dg_ssprk3_graph": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
         "dg_mass": (ctypes.c_int, [vp, c_double_p, ctypes.c_size_t]),
+        "dg_limit": (ctypes.c_int, [vp, c_double_p, c_double_p, ctypes.c_size_t, ctypes.c_int]),
+        "dg_limit_device": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp]),
+        "dg_save_checkpoint": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_double, ctypes.c_int64]),
+        "dg_load_checkpoint": (ctypes.c_int, [vp, ctypes.c_char_p, c_double_p, c_int64_p]),
         "dg_ssprk3_timed": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int, c_double_p, ctypes.c_int]),
         "dg_stream": (vp, [vp]),
         "dg_create_ensemble": (vp, [ctypes.POINTER(MeshDesc), ctypes.c_int, ctypes.POINTER(Config), c_int_p]),
@@ -103,7 +107,9 @@ def exported_symbols():
     return ["dg_create", "dg_destroy", "dg_residual", "dg_residual_device", "dg_residual_device_static",
             "dg_static_scratch_capacity", "dg_set_state", "dg_get_state",
             "dg_ssprk3", "dg_ssprk3_graph", "dg_ssprk3_timed", "dg_stream", "dg_create_ensemble",
-            "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_mass", "dg_set_dirichlet", "dg_conservation",
+            "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_mass", "dg_limit", "dg_limit_device",
+            "dg_save_checkpoint", "dg_load_checkpoint",
+            "dg_set_dirichlet", "dg_conservation",
             "dg_max_wave_speed", "dg_check_state", "dg_info", "dg_mesh_geometry", "dg_face_perms", "dg_basis",
             "dg_quad_rule", "dg_auto_rules", "dg_status_string", "dg_launch_count", "dg_box_mesh_create",
             "dg_box_mesh_destroy", "dg_box_mesh_view"]

@@ -13,6 +13,7 @@ Beyond the reference interface the object also owns a device-resident state for 
 (set_state / ssprk3 / get_state), the diagonal mass of the drivers, and conservation sums.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -21,11 +22,12 @@ from . import _lib as L
 FLUX = {"LF": 0, "Roe": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
 SCHEDULE = {"two-launch": 0, "persistent": 1}
+LIMITER = {None: 0, "none": 0, "positive": 1, "positive-avg": 2}
 
 
 class ExplicitConvection:
     def __init__(self, mesh, order=3, flux="LF", quad_vol=-1, quad_face=-1, gamma=1.4,
-                 precision="fp64", device=0, schedule="two-launch", _ensemble=None):
+                 precision="fp64", device=0, schedule="two-launch", limiter=None, _ensemble=None):
         self.mesh = mesh
         self.order = int(order)
         self.flux = flux
@@ -35,7 +37,8 @@ class ExplicitConvection:
         cfg = L.Config(order=self.order, flux=FLUX[flux] if isinstance(flux, str) else int(flux),
                        quad_vol=int(quad_vol), quad_face=int(quad_face), gamma=self.gamma,
                        precision=PRECISION[precision] if isinstance(precision, str) else int(precision),
-                       device=int(device), schedule=SCHEDULE[schedule] if isinstance(schedule, str) else int(schedule))
+                       device=int(device), schedule=SCHEDULE[schedule] if isinstance(schedule, str) else int(schedule),
+                       limiter=LIMITER[limiter] if limiter is None or isinstance(limiter, str) else int(limiter))
         err = ctypes.c_int(0)
         if _ensemble is None:
             self._desc = mesh.desc()
@@ -69,6 +72,25 @@ class ExplicitConvection:
     @property
     def shape(self):
         return (self.ncell, 5 * self.num_basis)
+
+    def limit(self, U, Uprev, only_neighbor_avg=False):
+        """PositiveLimiter::constructMinMax(U, Uprev) then apply(U, Uprev) on the GPU: bounds from
+        Uprev, the limited U returned (element means unchanged)."""
+        U = np.array(U, dtype=np.float64, copy=True)
+        Uprev = np.ascontiguousarray(Uprev, dtype=np.float64)
+        L.check(L.lib().dg_limit(self._ctx, L.dptr(U), L.dptr(Uprev), 0, int(bool(only_neighbor_avg))), "dg_limit")
+        return U
+
+    def save_checkpoint(self, path, t=0.0, step=0):
+        """Binary checkpoint of the device state with the time and step (dg_save_checkpoint)."""
+        L.check(L.lib().dg_save_checkpoint(self._ctx, os.fsencode(path), float(t), int(step)), "dg_save_checkpoint")
+
+    def load_checkpoint(self, path):
+        """Restore a checkpoint written for the same mesh, order and volume rule; returns (t, step)."""
+        t, step = ctypes.c_double(0.0), ctypes.c_int64(0)
+        L.check(L.lib().dg_load_checkpoint(self._ctx, os.fsencode(path), ctypes.byref(t), ctypes.byref(step)),
+                "dg_load_checkpoint")
+        return t.value, step.value
 
     def autotune(self, dt):
         """Time the persistent schedule's tile candidates on the current state (which is restored)

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <mutex>
@@ -14,6 +15,7 @@
 #include "dg_kernels_fp64.cuh"
 #include "dg_kernels_mixed.cuh"
 #include "dg_persistent.cuh"
+#include "dg_limiter.cuh"
 #include "dg_reduce.cuh"
 
 using namespace fvedg;
@@ -84,6 +86,10 @@ struct dg_ctx {
     QueueState* d_queue = nullptr;
     PersistentParams pp;
     QueueSchedule qs;
+    // limiter: per-face bounds [nface][10] and a staging buffer for host calls
+    double* d_lim_bnd = nullptr;
+    double* d_lim_prev = nullptr;
+    int sms = 148;
     // ensembles: instance element offsets, per-instance dt on the device, instance of each element
     int ninst = 1;
     std::vector<int64_t> inst_off;
@@ -262,6 +268,17 @@ int timed(dg_ctx* c, int cls, cudaStream_t s, F&& fn) {
 
 // One SSP-RK3 step (Shu-Osher) on the device state, FP64 form:
 //   U1 = U + dt L(U);  U2 = 3/4 U + 1/4 (U1 + dt L(U1));  U = 1/3 U + 2/3 (U2 + dt L(U2)).
+// Limiter after a stage (dg_config.limiter): bounds from the stage input, the output limited in
+// place; mir = the output's split rows in the mixed form (refreshed where the limiter acted).
+int limit_stage(dg_ctx* c, const double* in, double* out, uint32_t* mir, cudaStream_t s) {
+    if (!c->cfg.limiter) return DG_OK;
+    g_launches += 2;
+    return timed(c, 4, s, [&] {
+        return launch_limiter(c->cfg.order, c->qv, out, in, c->d_fi, c->d_ef, c->d_phi_v, c->ncell, c->nface,
+                              c->cfg.gamma, c->cfg.limiter == 2, c->d_lim_bnd, mir, c->sms, s);
+    });
+}
+
 int step_fp64(dg_ctx* c, double dt, cudaStream_t s) {
     const double A0[3] = {0.0, 0.75, 1.0 / 3.0};
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
@@ -274,6 +291,7 @@ int step_fp64(dg_ctx* c, double dt, cudaStream_t s) {
             return dispatch_element(c->cfg.order, c->qv, c->qf, stage_args(c, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 1), s);
         });
         if (rc) return rc;
+        if ((rc = limit_stage(c, in[st], out[st], nullptr, s))) return rc;
     }
     return DG_OK;
 }
@@ -282,17 +300,19 @@ int step(dg_ctx* c, double dt, cudaStream_t s) {
     if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
     auto tm = [&](int cls, auto&& fn) { return timed(c, cls, s, fn); };
     if (c->cfg.precision == DG_PREC_MIXED) {
+        auto post = [&](const double* in, double* out, int mir) { return limit_stage(c, in, out, c->mixed.mir[mir], s); };
         if (c->cfg.schedule == 1)
             return step_persistent(c->mixed, c->d_queue, c->qs, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches,
-                                   tm);
-        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm);
+                                   tm, post);
+        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm, post);
     }
     return step_fp64(c, dt, s);
 }
 
 int launches_per_step(const dg_ctx* c) {
-    if (c->cfg.precision == DG_PREC_MIXED) return c->cfg.schedule == 1 ? 3 : mixed_launches_per_step(c->mixed);
-    return 6;
+    const int lim = c->cfg.limiter ? 6 : 0;
+    if (c->cfg.precision == DG_PREC_MIXED) return (c->cfg.schedule == 1 ? 3 : mixed_launches_per_step(c->mixed)) + lim;
+    return 6 + lim;
 }
 
 // After a synchronize: the watchdog word of the persistent queue (DG_OK or DG_E_WATCHDOG).
@@ -335,6 +355,8 @@ void free_ctx(dg_ctx* c) {
     free_mixed(c->mixed);
     if (c->d_queue) cudaFree(c->d_queue);
     if (c->d_dt_inst) cudaFree(c->d_dt_inst);
+    if (c->d_lim_bnd) cudaFree(c->d_lim_bnd);
+    if (c->d_lim_prev) cudaFree(c->d_lim_prev);
     if (c->d_elem_inst) cudaFree(c->d_elem_inst);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -354,6 +376,7 @@ const char* dg_status_string(int s) {
         case DG_E_NONPHYSICAL: return "non-physical state (NaN/Inf, rho <= 0 or p <= 0)";
         case DG_E_WATCHDOG: return "bounded device wait expired";
         case DG_E_STATE: return "call out of order";
+        case DG_E_IO: return "file error (open, read, write or checksum)";
     }
     return "unknown status";
 }
@@ -377,6 +400,8 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
     const int qv = cfg->quad_vol < 0 ? auto_tet_rule(cfg->order) : cfg->quad_vol;
     const int qf = cfg->quad_face < 0 ? auto_tri_rule(cfg->order) : cfg->quad_face;
     if (tet_rule_npts(qv) <= 0 || tri_rule_npts(qf) <= 0) return fail(nullptr, DG_E_ARG);
+    if (cfg->limiter < 0 || cfg->limiter > 2 || (cfg->limiter && !limiter_supported(cfg->order, qv)))
+        return fail(nullptr, DG_E_ARG);
     if (mesh->ncell <= 0 || mesh->ncell > (int64_t)1 << 30 || mesh->nface <= 0 || mesh->nface > (int64_t)1 << 30)
         return fail(nullptr, DG_E_ARG);
     Geometry geo;
@@ -448,6 +473,13 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
         if (cudaMemset(c->d_queue, 0, sizeof(QueueState)) != cudaSuccess) return fail(c, DG_E_CUDA);
         if ((rc = build_schedule(c->mixed, c->qs, c->pp))) return fail(c, rc);
     }
+    {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+            c->sms = sms;
+    }
+    // the limiter's per-face bounds, allocated here so that no step allocates (graph capture)
+    if (cfg->limiter && (rc = dev_alloc(&c->d_lim_bnd, (size_t)c->nface * 10))) return fail(c, rc);
     if (err) *err = DG_OK;
     return c;
 }
@@ -622,6 +654,31 @@ int dg_residual(dg_ctx* c, const double* U, double* R, size_t stride, double t, 
     return cuda_ok(cudaStreamSynchronize(c->stream));
 }
 
+int dg_limit_device(dg_ctx* c, double* U, const double* Uprev, int only_avg, void* stream) {
+    if (!c || !U || !Uprev) return DG_E_ARG;
+    if (!limiter_supported(c->cfg.order, c->qv)) return DG_E_ARG;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    int rc;
+    if (!c->d_lim_bnd && (rc = dev_alloc(&c->d_lim_bnd, (size_t)c->nface * 10))) return rc;
+    g_launches += 2;
+    return launch_limiter(c->cfg.order, c->qv, U, Uprev, c->d_fi, c->d_ef, c->d_phi_v, c->ncell, c->nface,
+                          c->cfg.gamma, only_avg != 0, c->d_lim_bnd, nullptr, c->sms, (cudaStream_t)stream);
+}
+
+int dg_limit(dg_ctx* c, double* U, const double* Uprev, size_t stride, int only_avg) {
+    if (!c || !U || !Uprev) return DG_E_ARG;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    const size_t nstate = (size_t)c->ncell * 5 * c->tab.nb;
+    int rc;
+    if (!c->d_io && (rc = dev_alloc(&c->d_io, nstate))) return rc;
+    if (!c->d_lim_prev && (rc = dev_alloc(&c->d_lim_prev, nstate))) return rc;
+    if ((rc = copy_in(c, c->d_io, U, stride, c->stream)) || (rc = copy_in(c, c->d_lim_prev, Uprev, stride, c->stream)))
+        return rc;
+    if ((rc = dg_limit_device(c, c->d_io, c->d_lim_prev, only_avg, c->stream))) return rc;
+    if ((rc = copy_out(c, U, c->d_io, stride, c->stream))) return rc;
+    return cuda_ok(cudaStreamSynchronize(c->stream));
+}
+
 int dg_set_state(dg_ctx* c, const double* U, size_t stride) {
     if (!c || !U) return DG_E_ARG;
     DG_CUDA(cudaSetDevice(c->cfg.device));
@@ -785,6 +842,89 @@ int dg_autotune(dg_ctx* c, double dt, char* report, size_t len) {
         report[n] = 0;
     }
     return rc;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Binary checkpoint / restart (new: the reference writes text solution files only). Layout:
+//   96-byte header: "FVEDGCK1", version, order, quad_vol, quad_face, flux, precision, ncell,
+//   nface, num_basis, gamma, t, step, reserved; then the state U^n, [ncell][5*Nb] FP64 packed;
+//   then the FNV-1a 64-bit hash of the state bytes. Little-endian, as the host writes it.
+// ------------------------------------------------------------------------------------------------
+namespace {
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, order, quad_vol, quad_face, flux, precision;
+    int64_t ncell, nface;
+    uint32_t num_basis, reserved0;
+    double gamma, t;
+    int64_t step;
+    uint64_t reserved1[2];
+};
+static_assert(sizeof(CkptHeader) == 96, "checkpoint header layout");
+
+uint64_t fnv1a(const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    uint64_t h = 1469598103934665603ull;
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    return h;
+}
+}  // namespace
+
+int dg_save_checkpoint(dg_ctx* c, const char* path, double t, int64_t step) {
+    if (!c || !path) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    const size_t n = (size_t)c->ncell * 5 * c->tab.nb;
+    std::vector<double> U(n);
+    int rc = dg_get_state(c, U.data(), 0);
+    if (rc) return rc;
+    CkptHeader h{};
+    std::memcpy(h.magic, "FVEDGCK1", 8);
+    h.version = 1;
+    h.order = (uint32_t)c->cfg.order;
+    h.quad_vol = (uint32_t)c->qv;
+    h.quad_face = (uint32_t)c->qf;
+    h.flux = (uint32_t)c->cfg.flux;
+    h.precision = (uint32_t)c->cfg.precision;
+    h.ncell = c->ncell;
+    h.nface = c->nface;
+    h.num_basis = (uint32_t)c->tab.nb;
+    h.gamma = c->cfg.gamma;
+    h.t = t;
+    h.step = step;
+    const uint64_t sum = fnv1a(U.data(), n * sizeof(double));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return DG_E_IO;
+    const bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1 && std::fwrite(U.data(), sizeof(double), n, f) == n &&
+                    std::fwrite(&sum, sizeof(sum), 1, f) == 1;
+    return (std::fclose(f) == 0 && ok) ? DG_OK : DG_E_IO;
+}
+
+int dg_load_checkpoint(dg_ctx* c, const char* path, double* t, int64_t* step) {
+    if (!c || !path) return DG_E_ARG;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return DG_E_IO;
+    CkptHeader h{};
+    const size_t n = (size_t)c->ncell * 5 * c->tab.nb;
+    std::vector<double> U;
+    uint64_t sum = 0;
+    int rc = DG_OK;
+    if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, "FVEDGCK1", 8) != 0 || h.version != 1) {
+        rc = DG_E_IO;
+    } else if (h.order != (uint32_t)c->cfg.order || h.quad_vol != (uint32_t)c->qv || h.ncell != c->ncell ||
+               h.nface != c->nface || h.num_basis != (uint32_t)c->tab.nb) {
+        rc = DG_E_MESH;  // written by a context of another mesh, order or volume rule
+    } else {
+        U.resize(n);
+        if (std::fread(U.data(), sizeof(double), n, f) != n || std::fread(&sum, sizeof(sum), 1, f) != 1 ||
+            sum != fnv1a(U.data(), n * sizeof(double)))
+            rc = DG_E_IO;
+    }
+    std::fclose(f);
+    if (rc) return rc;
+    if ((rc = dg_set_state(c, U.data(), 0))) return rc;
+    if (t) *t = h.t;
+    if (step) *step = h.step;
+    return DG_OK;
 }
 
 int dg_mass(dg_ctx* c, double* mass, size_t stride) {

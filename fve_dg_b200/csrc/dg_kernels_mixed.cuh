@@ -1052,18 +1052,18 @@ inline int mixed_launches_per_step(const MixedData&) { return 6; }
 
 // SSP-RK3 step; `timed(cls, fn)` runs fn (one launch) and may bracket it with timing events. The
 // mirror of Un must be current (the upload writes it, and stage 3 of every step rewrites it).
-template <class Timed>
+// `post(in, out, mir_out)` runs after every stage (the limiter, or nothing).
+template <class Timed, class Post>
 inline int step_mixed(MixedData& m, double* Un, double* Ua, double* Ub, double dt, cudaStream_t s,
-                      std::atomic<int64_t>* launches, Timed&& timed) {
+                      std::atomic<int64_t>* launches, Timed&& timed, Post&& post) {
     const double A0[3] = {0.0, 0.75, 1.0 / 3.0};
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
     const double* in[3] = {Un, Ua, Ub};
     double* out[3] = {Ua, Ub, Un};
     const int mi[3] = {0, 1, 2}, mo[3] = {1, 2, 0};
     for (int st = 0; st < 3; ++st) {
-        const int rc =
-            mixed_stage(m, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches, timed, mi[st], mo[st]);
-        if (rc) return rc;
+        int rc = mixed_stage(m, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches, timed, mi[st], mo[st]);
+        if (rc || (rc = post(in[st], out[st], mo[st]))) return rc;
     }
     return DG_OK;
 }

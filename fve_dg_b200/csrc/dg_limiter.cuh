@@ -1,0 +1,255 @@
+// Positivity-preserving two-step limiter, after include/DG/DG_Schemes/PositiveLimiter.h:12-261, as
+// the reference's drivers call it: constructMinMax(current, previous) then apply(current, previous)
+// (examples/Eular1D/Sod1D/Riemann1D.cpp:194-195). FP64 in both forms.
+//
+//   bounds (constructMinMax, :57-103): per face, both cells' previous states evaluated at the
+//     volume rule's reference points; max over points of max(v1, v2) per variable, and - as the
+//     reference computes it (:86) - the min is min(v1, v2) at the last point. With only_avg the
+//     bounds are the max/min of the two cells' means. A boundary face uses its one cell twice.
+//     Each cell's bounds are the max/min over its faces.
+//   step 1 (apply_1_limitCell, :128-163): per variable, if the quadrature values leave the cell's
+//     bounds, scale the modes l >= 1 by min(theta_min, theta_max, 1) with
+//     theta_min = (avg - min_b) / (avg - v_min + 1e-32), theta_max = (max_b - avg) / (v_max - avg + 1e-32).
+//   step 2 (apply_21_limitCell, :164-188): density kept >= 1e-16 at the points by scaling its modes.
+//   step 3 (apply_22_limitCell, :189-258): for every point with negative pressure, 100 bisection
+//     steps on t in [0, 1] for p((1 - t) avg + t U(x_g)) = 0; all modes l >= 1 scaled by the
+//     smallest t.
+// Means are never changed, so mass, momentum and energy are conserved exactly.
+//
+// One warp per face / element, lanes over the quadrature points; each point value is summed over
+// the modes in order, as the reference does. Warps never wait on one another.
+#pragma once
+#include <cfloat>
+
+#include "dg_kernels_fp64.cuh"
+#include "dg_kernels_mixed.cuh"
+
+namespace fvedg {
+
+__device__ __forceinline__ double ref_max(double a, double b) { return (a < b) ? b : a; }  // std::max
+__device__ __forceinline__ double ref_min(double a, double b) { return (b < a) ? b : a; }  // std::min
+
+__device__ __forceinline__ double warp_max(double v) {
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = ref_max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = ref_min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+template <int NB>
+__device__ __forceinline__ double point_value(const double* phi_g, const double* u, int k) {
+    double v = 0.0;
+    #pragma unroll 5
+    for (int l = 0; l < NB; ++l) v = fma(phi_g[l], u[k + 5 * l], v);
+    return v;
+}
+
+// PositiveLimiter.h:112-123
+__device__ __forceinline__ double limiter_pressure(const double U[5], double gamma) {
+    const double rho = U[0];
+    if (rho <= 1e-16) return -1.0;
+    const double ke = (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / (2.0 * rho);
+    return (gamma - 1.0) * (U[4] - ke);
+}
+
+constexpr int kLimWarps = 4;
+
+template <int NB, int NQV>
+__global__ void __launch_bounds__(kLimWarps * 32)
+    limiter_face_bounds(const double* __restrict__ Up, const FaceInfo* __restrict__ fi,
+                        const double* __restrict__ phi, int64_t nface, int only_avg, double* __restrict__ bnd) {
+    __shared__ double sphi[NQV * NB];
+    for (int i = threadIdx.x; i < NQV * NB; i += blockDim.x) sphi[i] = phi[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (int64_t f = (int64_t)blockIdx.x * kLimWarps + (threadIdx.x >> 5); f < nface;
+         f += (int64_t)gridDim.x * kLimWarps) {
+        const FaceInfo F = fi[f];
+        const double* u1 = Up + (int64_t)F.c0 * (5 * NB);
+        const double* u2 = Up + (int64_t)(F.c1 >= 0 ? F.c1 : F.c0) * (5 * NB);
+        double* out = bnd + f * 10;
+        if (only_avg) {
+            if (lane < 5) {
+                out[lane] = ref_max(u1[lane], u2[lane]);
+                out[5 + lane] = ref_min(u1[lane], u2[lane]);
+            }
+            continue;
+        }
+        double mx[5], lastmin[5];
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) { mx[k] = -DBL_MAX; lastmin[k] = DBL_MAX; }
+        for (int g = lane; g < NQV; g += 32) {
+            #pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                const double v1 = point_value<NB>(sphi + g * NB, u1, k), v2 = point_value<NB>(sphi + g * NB, u2, k);
+                mx[k] = ref_max(mx[k], ref_max(v1, v2));
+                if (g == NQV - 1) lastmin[k] = ref_min(v1, v2);
+            }
+        }
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            mx[k] = warp_max(mx[k]);
+            lastmin[k] = __shfl_sync(0xffffffffu, lastmin[k], (NQV - 1) % 32);
+        }
+        if (lane < 5) {
+            double a = mx[0], b = lastmin[0];
+            #pragma unroll
+            for (int k = 1; k < 5; ++k)
+                if (lane == k) { a = mx[k]; b = lastmin[k]; }
+            out[lane] = a;
+            out[5 + lane] = b;
+        }
+    }
+}
+
+// mir: when non-null, the element's split coefficient rows (A rows, [ncell][5][KB]) are rewritten
+// if the limiter changed the element, so the mixed form's next stage reads the limited state.
+template <int NB, int NQV>
+__global__ void __launch_bounds__(kLimWarps * 32)
+    limiter_apply(double* __restrict__ U, const ElemFace* __restrict__ ef, const double* __restrict__ bnd,
+                  const double* __restrict__ phi, int64_t ncell, double gamma, uint32_t* __restrict__ mir) {
+    constexpr int KB = pad8(NB - 1);
+    __shared__ double sphi[NQV * NB];
+    for (int i = threadIdx.x; i < NQV * NB; i += blockDim.x) sphi[i] = phi[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (int64_t e = (int64_t)blockIdx.x * kLimWarps + (threadIdx.x >> 5); e < ncell;
+         e += (int64_t)gridDim.x * kLimWarps) {
+        double* u = U + e * (5 * NB);
+        // the cell's bounds: max/min over its faces (constructMinMax, :92-102)
+        double gmax = -DBL_MAX, gmin = DBL_MAX;
+        if (lane < 5) {
+            #pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int64_t f = ef[4 * e + q].face;
+                gmax = ref_max(gmax, bnd[f * 10 + lane]);
+                gmin = ref_min(gmin, bnd[f * 10 + 5 + lane]);
+            }
+        }
+        bool changed = false;
+        // step 1: each variable within the cell's bounds
+        for (int k = 0; k < 5; ++k) {
+            const double bmax = __shfl_sync(0xffffffffu, gmax, k), bmin = __shfl_sync(0xffffffffu, gmin, k);
+            const double avg = u[k];
+            double vmin = DBL_MAX, vmax = -DBL_MAX;
+            for (int g = lane; g < NQV; g += 32) {
+                const double v = point_value<NB>(sphi + g * NB, u, k);
+                vmin = ref_min(vmin, v);
+                vmax = ref_max(vmax, v);
+            }
+            vmin = warp_min(vmin);
+            vmax = warp_max(vmax);
+            if (vmin < bmin || vmax > bmax) {
+                const double tmin = (avg != vmin) ? (avg - bmin) / (avg - vmin + 1e-32) : 0.0;
+                const double tmax = (avg != vmax) ? (bmax - avg) / (vmax - avg + 1e-32) : 0.0;
+                const double theta = ref_min(ref_min(tmin, tmax), 1.0);
+                __syncwarp();
+                for (int l = 1 + lane; l < NB; l += 32) u[k + 5 * l] *= theta;
+                __syncwarp();
+                changed = true;
+            }
+        }
+        // step 2: density at the points >= 1e-16
+        {
+            const double eps = 1e-16;
+            double rmin = DBL_MAX;
+            for (int g = lane; g < NQV; g += 32) rmin = ref_min(rmin, point_value<NB>(sphi + g * NB, u, 0));
+            rmin = warp_min(rmin);
+            const double ravg = u[0];
+            if (rmin < eps) {
+                const double eff = ref_max(ravg, eps);
+                const double num = eff - eps, den = eff - rmin;
+                const double theta = (den < 1e-32) ? 0.0 : ref_min(1.0, num / den);
+                __syncwarp();
+                for (int l = 1 + lane; l < NB; l += 32) u[5 * l] *= theta;
+                __syncwarp();
+                changed = true;
+            }
+        }
+        // step 3: pressure at the points >= 0 by bisection toward the mean
+        {
+            double avgU[5];
+            #pragma unroll
+            for (int k = 0; k < 5; ++k) avgU[k] = u[k];
+            double tp = 1.0;
+            for (int g = lane; g < NQV; g += 32) {
+                double pu[5];
+                #pragma unroll
+                for (int k = 0; k < 5; ++k) pu[k] = point_value<NB>(sphi + g * NB, u, k);
+                if (limiter_pressure(pu, gamma) >= 0) continue;
+                double lo = 0.0, hi = 1.0, mid = 0.5 * (lo + hi);
+                for (int it = 0; it < 100; ++it) {
+                    mid = 0.5 * (lo + hi);
+                    double um[5];
+                    #pragma unroll
+                    for (int k = 0; k < 5; ++k) um[k] = (1.0 - mid) * avgU[k] + mid * pu[k];
+                    if (limiter_pressure(um, gamma) < 0) hi = mid;
+                    else lo = mid;
+                }
+                tp = ref_min(tp, mid);
+            }
+            tp = warp_min(tp);
+            if (tp != 1.0) {
+                __syncwarp();
+                for (int i = lane; i < 5 * (NB - 1); i += 32) u[5 + i] *= tp;
+                __syncwarp();
+                changed = true;
+            }
+        }
+        if (mir && changed) {  // refresh the split rows of the changed element
+            for (int i = lane; i < 5 * (KB / 2); i += 32) {
+                const int k = i / (KB / 2), x = 2 * (i - k * (KB / 2));
+                const float v0 = x + 1 < NB ? (float)u[5 * (x + 1) + k] : 0.f;
+                const float v1 = x + 2 < NB ? (float)u[5 * (x + 2) + k] : 0.f;
+                uint32_t h, l;
+                split2(v0, v1, h, l);
+                uint32_t* row = mir + (e * 5 + k) * KB;
+                row[arow_hi_word<KB>(x)] = h;
+                row[arow_lo_word<KB>(x)] = l;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// X(order, qv, NB, NQV)
+#define FVEDG_LIMITER_COMBOS(X) \
+    X(1, 0, 4, 4)               \
+    X(1, 2, 4, 15)              \
+    X(2, 1, 10, 11)             \
+    X(2, 2, 10, 15)             \
+    X(3, 3, 20, 23)             \
+    X(3, 4, 20, 31)             \
+    X(4, 5, 35, 44)             \
+    X(4, 6, 35, 57)
+
+inline bool limiter_supported(int order, int qv) {
+#define X(P, QV, NB, NQV) \
+    if (order == P && qv == QV) return true;
+    FVEDG_LIMITER_COMBOS(X)
+#undef X
+    return false;
+}
+
+// Bounds from Uprev, then the three steps on U (in place). bnd: [nface][10] scratch.
+inline int launch_limiter(int order, int qv, double* U, const double* Uprev, const FaceInfo* fi, const ElemFace* ef,
+                          const double* phi_v, int64_t ncell, int64_t nface, double gamma, int only_avg, double* bnd,
+                          uint32_t* mir, int sms, cudaStream_t s) {
+#define X(P, QV, NB, NQV)                                                                                        \
+    if (order == P && qv == QV) {                                                                                \
+        const unsigned gf = (unsigned)std::min<int64_t>((nface + kLimWarps - 1) / kLimWarps, (int64_t)sms * 16); \
+        limiter_face_bounds<NB, NQV><<<gf, kLimWarps * 32, 0, s>>>(Uprev, fi, phi_v, nface, only_avg, bnd);      \
+        const unsigned ge = (unsigned)std::min<int64_t>((ncell + kLimWarps - 1) / kLimWarps, (int64_t)sms * 16); \
+        limiter_apply<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(U, ef, bnd, phi_v, ncell, gamma, mir);             \
+        return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;                                            \
+    }
+    FVEDG_LIMITER_COMBOS(X)
+#undef X
+    return DG_E_ARG;
+}
+
+}  // namespace fvedg

@@ -253,21 +253,22 @@ inline int persistent_kernel(MixedData& m, QueueState* q, const QueueSchedule& q
     return DG_E_ARG;
 }
 
-template <class Timed>
+template <class Timed, class Post>
 inline int step_persistent(MixedData& m, QueueState* q, const QueueSchedule& qs, const PersistentParams& pp,
                            double* Un, double* Ua, double* Ub, double dt, cudaStream_t s,
-                           std::atomic<int64_t>* launches, Timed&& timed) {
+                           std::atomic<int64_t>* launches, Timed&& timed, Post&& post) {
     const double A0[3] = {0.0, 0.75, 1.0 / 3.0};
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
     const double* in[3] = {Un, Ua, Ub};
     double* out[3] = {Ua, Ub, Un};
     const int mi[3] = {0, 1, 2}, mo[3] = {1, 2, 0};
     for (int st = 0; st < 3; ++st) {
-        const int rc = timed(2, [&] {
+        int rc = timed(2, [&] {
             return persistent_kernel(m, q, qs, pp, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches,
                                      mi[st], mo[st]);
         });
         if (rc) return rc;
+        if ((rc = post(in[st], out[st], mo[st]))) return rc;
     }
     return DG_OK;
 }

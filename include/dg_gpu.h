@@ -39,7 +39,8 @@ enum dg_status {
     DG_E_NOMEM = -4,      /* device or host allocation failed */
     DG_E_NONPHYSICAL = -5,/* the state has NaN/Inf or non-positive density or pressure */
     DG_E_WATCHDOG = -6,   /* a bounded device wait ran out (batched persistent form) */
-    DG_E_STATE = -7       /* call out of order (e.g. stepping before a state was set) */
+    DG_E_STATE = -7,      /* call out of order (e.g. stepping before a state was set) */
+    DG_E_IO = -8          /* file could not be opened, read or written, or failed its checksum */
 };
 
 enum dg_flux_kind { DG_FLUX_LF = 0, DG_FLUX_ROE = 1 };
@@ -101,8 +102,11 @@ typedef struct dg_config {
     int precision;   /* dg_precision */
     int device;      /* CUDA device ordinal */
     int schedule;    /* 0: two launches per RK stage (face fluxes, then elements);
-                        1: one persistent cooperative launch per stage pulling face and element
-                           tiles from work queues (mixed precision only; see dg_autotune) */
+                        1: one persistent launch per stage over a tile list of face and element
+                           tiles interleaved by mesh region (mixed precision only; see dg_autotune) */
+    int limiter;     /* 0: none; 1: positivity-preserving limiter after every RK stage, bounds from
+                        the stage input's values at the volume points; 2: the same with bounds from
+                        the neighbours' means (PositiveLimiter<.., OnlyNeigbAvg = true>); see dg_limit */
 } dg_config;
 
 typedef struct dg_ctx dg_ctx;
@@ -158,8 +162,8 @@ int dg_ensemble_offsets(const dg_ctx* ctx, int64_t* elem_offsets);
  * graph per step (the dt values are read from device memory, so one graph serves any dt). */
 int dg_ssprk3_ensemble(dg_ctx* ctx, const double* dt, int nsteps, int use_graph);
 
-/* Autotuner of the persistent schedule: times each candidate tile shape (face and element groups
- * per queue ticket, CTAs per SM) on the current state (restored afterwards), keeps the fastest and
+/* Autotuner of the persistent schedule: times each candidate (face and element groups per tile,
+ * CTAs per SM, mesh regions, lag) on the current state (restored afterwards), keeps the fastest and
  * writes a JSON record of every candidate and the choice into report[len]. */
 int dg_autotune(dg_ctx* ctx, double dt, char* report, size_t len);
 
@@ -169,6 +173,23 @@ int dg_autotune(dg_ctx* ctx, double dt, char* report, size_t len);
 int dg_ssprk3_timed(dg_ctx* ctx, double dt, int nsteps, double* out, int nclass);
 /* The context's CUDA stream (a cudaStream_t) on which every kernel of the context runs. */
 void* dg_stream(dg_ctx* ctx);
+
+/* Positivity-preserving limiter, replaces PositiveLimiter<P, QuadC, OnlyNeigbAvg>::constructMinMax
+ * (current, previous) followed by apply(current, previous) (include/DG/DG_Schemes/PositiveLimiter.h:
+ * 12-261, called so in examples/Eular1D/Sod1D/Riemann1D.cpp:194-195), with QuadC the context's volume
+ * rule: bounds from Uprev, the three limiting steps on U in place. Element means are unchanged.
+ * Host buffers with the element stride of dg_residual. only_neighbor_avg selects OnlyNeigbAvg. */
+int dg_limit(dg_ctx* ctx, double* U, const double* Uprev, size_t elem_stride_bytes, int only_neighbor_avg);
+/* Same on device buffers (packed [ncell][5*Nb]), enqueued on `stream` (a cudaStream_t, 0 = default). */
+int dg_limit_device(dg_ctx* ctx, double* U_dev, const double* Uprev_dev, int only_neighbor_avg, void* stream);
+
+/* Binary checkpoint / restart of the device state (new: the reference writes text solution files,
+ * examples/Eular1D/Sod1D/Riemann1D.cpp:249-286, which fve_dg_b200/io.py reads and writes). The file
+ * holds a header (order, rules, flux, precision, mesh sizes, gamma, time t, step), U^n in FP64 and a
+ * checksum. Loading checks that the context has the same order, volume rule and mesh sizes
+ * (DG_E_MESH otherwise) and the checksum (DG_E_IO), then sets the state; t and step may be NULL. */
+int dg_save_checkpoint(dg_ctx* ctx, const char* path, double t, int64_t step);
+int dg_load_checkpoint(dg_ctx* ctx, const char* path, double* t, int64_t* step);
 
 /* Diagonal mass b[e][5i+k] = detJ * sum_g w_g phi_i(x_g)^2 (Riemann1D.cpp:108-121). */
 int dg_mass(dg_ctx* ctx, double* mass, size_t elem_stride_bytes);

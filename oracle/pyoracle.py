@@ -143,6 +143,7 @@ class RefLib:
         L.fveref_ssprk3.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp,
                                     ctypes.c_double, ctypes.c_int, ctypes.c_double]
         L.fveref_mass.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp]
+        L.fveref_limit.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int]
         L.fveref_quad_tet.argtypes = [ctypes.c_int, dp, dp]
         L.fveref_quad_tri.argtypes = [ctypes.c_int, dp, dp]
         L.fveref_basis.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp]
@@ -249,6 +250,16 @@ class RefMesh:
         if rc != 0:
             raise RuntimeError(f"fveref_mass rc={rc}")
         return b
+
+    def limit(self, U, Uprev, order, qv, gamma=1.4, only_avg=False):
+        """PositiveLimiter<P, QC, only_avg>: constructMinMax(U, Uprev) then apply(U, Uprev)."""
+        U = np.array(U, dtype=np.float64, copy=True)
+        Uprev = np.ascontiguousarray(Uprev, dtype=np.float64)
+        rc = self.ref.L.fveref_limit(self.h, order, qv, U.ctypes.data_as(dp), Uprev.ctypes.data_as(dp), gamma,
+                                     int(only_avg))
+        if rc != 0:
+            raise RuntimeError(f"fveref_limit rc={rc}")
+        return U
 
     def ssprk3(self, U, mass, order, qv, qf, dt, nsteps, gamma_id=0, t0=0.0):
         U = np.array(U, dtype=np.float64, copy=True)

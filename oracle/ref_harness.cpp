@@ -17,7 +17,11 @@
 //     written with LongVector operators in the style of examples/Vortex/123/VortexRK.cpp:264-271.
 //   * The reference's quadrature tables and DGBasisEvaluator<P>::eval_all/grad_all, so that the
 //     product's own tables can be pinned against them.
+//   * PositiveLimiter<P, QuadC, OnlyNeigbAvg> (include/DG/DG_Schemes/PositiveLimiter.h:12-261) as the
+//     drivers call it: constructMinMax(current, previous) then apply(current, previous)
+//     (examples/Eular1D/Sod1D/Riemann1D.cpp:194-195).
 #include "DG/DG_Schemes/ExplicitConvection.h"
+#include "DG/DG_Schemes/PositiveLimiter.h"
 #include "src/DG/DG_Schemes/ExplicitConvection.cpp"
 
 #include <cstdint>
@@ -163,6 +167,20 @@ int run_mass(const ComputingMesh& m, double* mass) {
         }
     }
     from_lv<P>(b, nc, mass);
+    return 0;
+}
+
+template <uInt P, class QC, bool OnlyAvg>
+int run_limit(const ComputingMesh& m, double* Ucur, const double* Uprev, double gamma) {
+    using LV = LongVector<5 * DGBasisEvaluator<P>::NumBasis>;
+    const size_t nc = m.m_cells.size();
+    LV cur(nc), prev(nc);
+    to_lv<P>(Ucur, nc, cur);
+    to_lv<P>(Uprev, nc, prev);
+    PositiveLimiter<P, QC, OnlyAvg> lim(m, gamma);
+    lim.constructMinMax(cur, prev);
+    lim.apply(cur, prev);
+    from_lv<P>(cur, nc, Ucur);
     return 0;
 }
 
@@ -347,6 +365,25 @@ int fveref_ssprk3(void* p, int order, int gamma_id, int qv, int qf, double* U, c
                              : run_ssprk3<P, MonatomicFluxC, QC_, QF_>(m, U, mass, dt, nsteps, t0);
     FVEREF_COMBOS(X)
 #undef X
+    return -1;
+}
+
+// The limiter over the volume rule qv; only_avg selects the neighbour-mean bounds.
+int fveref_limit(void* p, int order, int qv, double* Ucur, const double* Uprev, double gamma, int only_avg) {
+    const ComputingMesh& m = *static_cast<RefMesh*>(p)->cm;
+#define L(P, QC_)                                                                                  \
+    return only_avg ? run_limit<P, QC_, true>(m, Ucur, Uprev, gamma) : run_limit<P, QC_, false>(m, Ucur, Uprev, gamma);
+    switch (order * 16 + qv) {
+        case 1 * 16 + 0: L(1, T::Degree2Points4)
+        case 1 * 16 + 2: L(1, T::Degree5Points15)
+        case 2 * 16 + 1: L(2, T::Degree4Points11)
+        case 2 * 16 + 2: L(2, T::Degree5Points15)
+        case 3 * 16 + 3: L(3, T::Degree6Points23)
+        case 3 * 16 + 4: L(3, T::Degree7Points31)
+        case 4 * 16 + 5: L(4, T::Degree8Points44)
+        case 4 * 16 + 6: L(4, T::Degree9Points57)
+    }
+#undef L
     return -1;
 }
 

@@ -42,7 +42,7 @@ def test_oracle_libraries_export_their_api():
 
 def test_status_strings_and_capacity():
     lib = L.lib()
-    for code in range(0, -8, -1):
+    for code in range(0, -9, -1):
         assert lib.dg_status_string(code)
     assert lib.dg_static_scratch_capacity() == 4 << 20
 
