@@ -140,6 +140,8 @@ def kernel_bytes(name, P, ncell, nface, nqf):
         return state + nface * face_rec + nface * nqf * 5 * 8
     if name == "element_fp64":           # stage state + U^n read, new stage written, face fluxes read
         return 3 * state + ncell * elem_rec + nface * nqf * 5 * 8
+    if name == "limiter":                # bounds from the stage input, the output read and written
+        return 3 * state + nface * (48 + 80) + ncell * 32
     kf = (nqf + 7) // 8 * 8
     kb = (nb - 1 + 7) // 8 * 8
     fj = nface * (5 * kf * 4 + 2 * 5 * 8)  # split flux deviations (A rows) + FP64 reference and mode-0 sums
@@ -259,6 +261,8 @@ def main():
     ap.add_argument("--schedule", default=None, choices=["two-launch", "persistent"])
     ap.add_argument("--no-compare", action="store_true", help="skip timing the FP64 form beside the mixed one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--limiter", default=None, choices=["positive", "positive-avg"],
+                    help="positivity-preserving limiter after every RK stage (timed as its own kernel class)")
     ap.add_argument("--n", type=int, default=0, help="override the mesh size (cubes per side), for profiling")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -296,7 +300,7 @@ def main():
     # persistent tile queue serves ensembles of uneven meshes (--config ensemble)
     schedule = args.schedule or "two-launch"
     conv = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf,
-                              precision=args.precision, device=local, schedule=schedule)
+                              precision=args.precision, device=local, schedule=schedule, limiter=args.limiter)
     conv.set_state(U0)
     dt = problems.cfl_dt(CFL, cfg["L"] / cfg["n"], P, conv.max_wave_speed())
     nb = conv.num_basis
@@ -318,7 +322,7 @@ def main():
     forms = {args.precision: {"value": value, "ms_per_step": ms / args.steps, "schedule": schedule}}
     if args.precision == "mixed" and not args.no_compare:
         f64 = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf, precision="fp64",
-                                 device=local)
+                                 device=local, limiter=args.limiter)
         f64.set_state(U0)
         ms64, _ = time_steps(f64, dt, args.warmup, args.steps, dist, torch, launch_count)
         U64 = f64.get_state()  # before the per-kernel timing pass below advances it
@@ -352,7 +356,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "bf16x3 contractions, f32 flux, f64 state",
                 "data": "synthetic",
-                "config": {"workload": args.config, "desc": cfg["desc"], "precision": args.precision,
+                "config": {"workload": args.config, "desc": cfg["desc"], "precision": args.precision, "limiter": args.limiter,
                            "schedule": schedule, "tets": m.ncell, "order": P, "dof_per_stage": 5 * nb * m.ncell,
                            "dt": dt, "l2": "state larger than L2 (no flush needed)",
                            "parallelism": f"independent instance per GPU x{world}"},
@@ -365,9 +369,9 @@ def main():
         dist.destroy_process_group()
 
 
-KNAMES = {("fp64", "two-launch"): {0: "face_flux_fp64", 1: "element_fp64"},
-          ("mixed", "two-launch"): {0: "face_flux_mixed", 1: "element_mixed"},
-          ("mixed", "persistent"): {2: "stage_persistent_mixed"}}
+KNAMES = {("fp64", "two-launch"): {0: "face_flux_fp64", 1: "element_fp64", 4: "limiter"},
+          ("mixed", "two-launch"): {0: "face_flux_mixed", 1: "element_mixed", 4: "limiter"},
+          ("mixed", "persistent"): {2: "stage_persistent_mixed", 4: "limiter"}}
 
 
 def time_steps(conv, dt, warmup, steps, dist, torch, launch_count):
