@@ -66,6 +66,9 @@ def lib():
         "dg_ssprk3_graph": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
         "dg_mass": (ctypes.c_int, [vp, c_double_p, ctypes.c_size_t]),
         "dg_limit": (ctypes.c_int, [vp, c_double_p, c_double_p, ctypes.c_size_t, ctypes.c_int]),
+        "dg_viscous_residual": (ctypes.c_int, [vp, c_double_p, c_double_p, ctypes.c_size_t, ctypes.c_double,
+                                               ctypes.c_double]),
+        "dg_viscous_residual_device": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, ctypes.c_double, vp]),
         "dg_limit_device": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp]),
         "dg_save_checkpoint": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_double, ctypes.c_int64]),
         "dg_load_checkpoint": (ctypes.c_int, [vp, ctypes.c_char_p, c_double_p, c_int64_p]),
@@ -107,7 +110,7 @@ def exported_symbols():
     return ["dg_create", "dg_destroy", "dg_residual", "dg_residual_device", "dg_residual_device_static",
             "dg_static_scratch_capacity", "dg_set_state", "dg_get_state",
             "dg_ssprk3", "dg_ssprk3_graph", "dg_ssprk3_timed", "dg_stream", "dg_create_ensemble",
-            "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_mass", "dg_limit", "dg_limit_device",
+            "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_mass", "dg_limit", "dg_limit_device", "dg_viscous_residual", "dg_viscous_residual_device",
             "dg_save_checkpoint", "dg_load_checkpoint",
             "dg_set_dirichlet", "dg_conservation",
             "dg_max_wave_speed", "dg_check_state", "dg_info", "dg_mesh_geometry", "dg_face_perms", "dg_basis",

@@ -81,6 +81,15 @@ class ExplicitConvection:
         L.check(L.lib().dg_limit(self._ctx, L.dptr(U), L.dptr(Uprev), 0, int(bool(only_neighbor_avg))), "dg_limit")
         return U
 
+    def viscous_eval(self, U, mu=1.0, prandtl=1.0):
+        """ExplicitDiffusion::eval on the GPU (FP64): the viscous residual of U with viscosity mu and
+        Prandtl number prandtl (the reference fixes both to 1)."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        R = np.empty_like(U)
+        L.check(L.lib().dg_viscous_residual(self._ctx, L.dptr(U), L.dptr(R), 0, float(mu), float(prandtl)),
+                "dg_viscous_residual")
+        return R
+
     def save_checkpoint(self, path, t=0.0, step=0):
         """Binary checkpoint of the device state with the time and step (dg_save_checkpoint)."""
         L.check(L.lib().dg_save_checkpoint(self._ctx, os.fsencode(path), float(t), int(step)), "dg_save_checkpoint")

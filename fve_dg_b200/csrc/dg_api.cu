@@ -16,6 +16,7 @@
 #include "dg_kernels_mixed.cuh"
 #include "dg_persistent.cuh"
 #include "dg_limiter.cuh"
+#include "dg_viscous.cuh"
 #include "dg_reduce.cuh"
 
 using namespace fvedg;
@@ -89,6 +90,10 @@ struct dg_ctx {
     // limiter: per-face bounds [nface][10] and a staging buffer for host calls
     double* d_lim_bnd = nullptr;
     double* d_lim_prev = nullptr;
+    // viscous operator: reference gradients at the volume and face points, cell size h
+    double* d_dphi_v = nullptr;
+    double* d_dphi_f = nullptr;
+    double* d_h = nullptr;
     int sms = 148;
     // ensembles: instance element offsets, per-instance dt on the device, instance of each element
     int ninst = 1;
@@ -356,6 +361,9 @@ void free_ctx(dg_ctx* c) {
     if (c->d_queue) cudaFree(c->d_queue);
     if (c->d_dt_inst) cudaFree(c->d_dt_inst);
     if (c->d_lim_bnd) cudaFree(c->d_lim_bnd);
+    if (c->d_dphi_v) cudaFree(c->d_dphi_v);
+    if (c->d_dphi_f) cudaFree(c->d_dphi_f);
+    if (c->d_h) cudaFree(c->d_h);
     if (c->d_lim_prev) cudaFree(c->d_lim_prev);
     if (c->d_elem_inst) cudaFree(c->d_elem_inst);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -444,7 +452,17 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
         hef[4 * fi.c0 + fill[fi.c0]++] = ElemFace{(int)f, p0};
         if (fi.c1 >= 0) hef[4 * fi.c1 + fill[fi.c1]++] = ElemFace{(int)f, p1 | (1 << 8)};
     }
+    // h = volume / sum of the face areas (ComputingMesh.cpp:289-297), for the viscous penalty
+    std::vector<double> hh(c->ncell);
+    for (int64_t e = 0; e < c->ncell; ++e) {
+        double area = 0.0;
+        for (int q = 0; q < 4; ++q) area += geo.area[hef[4 * e + q].face];
+        hh[e] = geo.detj[e] / 6.0 / area;
+    }
     const size_t nstate = (size_t)c->ncell * 5 * nb;
+    if ((rc = upload(&c->d_h, hh)) || (rc = upload(&c->d_dphi_v, c->tab.dphi_v)) ||
+        (rc = upload(&c->d_dphi_f, c->tab.dphi_f)))
+        return fail(c, rc);
     if ((rc = upload(&c->d_geo, hgeo)) || (rc = upload(&c->d_fi, hfi)) || (rc = upload(&c->d_ef, hef)) ||
         (rc = upload(&c->d_phi_v, c->tab.phi_v)) || (rc = upload(&c->d_dphi_vw, c->tab.dphi_vw)) ||
         (rc = upload(&c->d_w_v, c->tab.w_v)) || (rc = upload(&c->d_phi_f, c->tab.phi_f)) ||
@@ -650,6 +668,33 @@ int dg_residual(dg_ctx* c, const double* U, double* R, size_t stride, double t, 
     if (!c->d_R && (rc = dev_alloc(&c->d_R, nstate))) return rc;
     if ((rc = copy_in(c, c->d_io, U, stride, c->stream))) return rc;
     if ((rc = dg_residual_device(c, c->d_io, c->d_R, t, part, c->stream))) return rc;
+    if ((rc = copy_out(c, R, c->d_R, stride, c->stream))) return rc;
+    return cuda_ok(cudaStreamSynchronize(c->stream));
+}
+
+int dg_viscous_residual_device(dg_ctx* c, const double* U, double* R, double mu, double prandtl, void* stream) {
+    if (!c || !U || !R || !(mu >= 0.0) || !(prandtl > 0.0)) return DG_E_ARG;
+    if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    ViscArgs a;
+    a.U = U; a.R = R; a.geo = c->d_geo; a.h = c->d_h; a.fi = c->d_fi; a.ef = c->d_ef;
+    a.phi_v = c->d_phi_v; a.dphi_v = c->d_dphi_v; a.w_v = c->d_w_v;
+    a.phi_f = c->d_phi_f; a.dphi_f = c->d_dphi_f; a.w_f = c->d_w_f; a.UD = c->d_UD;
+    a.ncell = c->ncell; a.nqv = c->tab.nqv; a.nqf = c->tab.nqf; a.order = c->cfg.order;
+    a.mu = mu; a.cq = c->cfg.gamma / prandtl;
+    ++g_launches;
+    return launch_viscous(c->cfg.order, a, (cudaStream_t)stream);
+}
+
+int dg_viscous_residual(dg_ctx* c, const double* U, double* R, size_t stride, double mu, double prandtl) {
+    if (!c || !U || !R) return DG_E_ARG;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    const size_t nstate = (size_t)c->ncell * 5 * c->tab.nb;
+    int rc;
+    if (!c->d_io && (rc = dev_alloc(&c->d_io, nstate))) return rc;
+    if (!c->d_R && (rc = dev_alloc(&c->d_R, nstate))) return rc;
+    if ((rc = copy_in(c, c->d_io, U, stride, c->stream))) return rc;
+    if ((rc = dg_viscous_residual_device(c, c->d_io, c->d_R, mu, prandtl, c->stream))) return rc;
     if ((rc = copy_out(c, R, c->d_R, stride, c->stream))) return rc;
     return cuda_ok(cudaStreamSynchronize(c->stream));
 }

@@ -46,6 +46,8 @@ struct Tables {
     std::vector<double> phi_v;      // [nqv][nb]
     std::vector<double> phi_vT;     // [nb][nqv]
     std::vector<double> dphi_vw;    // [nqv][nb][3] reference gradients times w_g
+    std::vector<double> dphi_v;     // [nqv][nb][3] reference gradients
+    std::vector<double> dphi_f;     // [24][nqf][nb][3] reference gradients at the face points
     std::vector<double> w_v;        // [nqv]
     std::vector<double> phi_f;      // [24][nqf][nb] face point basis values per face map
     std::vector<double> phi_fT;     // [24][nb][nqf]

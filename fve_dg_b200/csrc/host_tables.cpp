@@ -82,6 +82,7 @@ void build_tables(int order, int qv, int qf, Tables* t) {
     t->nqf = nqf;
     t->phi_v.assign(nqv * nb, 0.0);
     t->dphi_vw.assign(nqv * nb * 3, 0.0);
+    t->dphi_v.assign(nqv * nb * 3, 0.0);
     t->w_v.assign(nqv, 0.0);
     t->mass_ref.assign(nb, 0.0);
     double phi[64], grad[192];
@@ -91,13 +92,17 @@ void build_tables(int order, int qv, int qf, Tables* t) {
         t->w_v[g] = w;
         for (int b = 0; b < nb; ++b) {
             t->phi_v[g * nb + b] = phi[b];
-            for (int c = 0; c < 3; ++c) t->dphi_vw[(g * nb + b) * 3 + c] = grad[3 * b + c] * w;
+            for (int c = 0; c < 3; ++c) {
+                t->dphi_vw[(g * nb + b) * 3 + c] = grad[3 * b + c] * w;
+                t->dphi_v[(g * nb + b) * 3 + c] = grad[3 * b + c];
+            }
             t->mass_ref[b] += phi[b] * phi[b] * w;
         }
     }
     // Face point of face map p at face parameters (u, v): xi = V[s0](1-u-v) + V[s1] u + V[s2] v
     // with V[0] = 0 and V[i] = e_{i-1}; the same point as ExplicitConvection.cpp:129-134.
     t->phi_f.assign((size_t)kNumPerms * nqf * nb, 0.0);
+    t->dphi_f.assign((size_t)kNumPerms * nqf * nb * 3, 0.0);
     t->w_f.assign(nqf, 0.0);
     for (int g = 0; g < nqf; ++g) t->w_f[g] = rf[3 * g + 2];
     for (int p = 0; p < kNumPerms; ++p)
@@ -109,8 +114,11 @@ void build_tables(int order, int qv, int qf, Tables* t) {
                 const int s = kPermSlots[p][k];
                 if (s > 0) xi[s - 1] = coef[k];
             }
-            basis_eval(order, xi[0], xi[1], xi[2], phi, nullptr);
-            for (int b = 0; b < nb; ++b) t->phi_f[((size_t)p * nqf + g) * nb + b] = phi[b];
+            basis_eval(order, xi[0], xi[1], xi[2], phi, grad);
+            for (int b = 0; b < nb; ++b) {
+                t->phi_f[((size_t)p * nqf + g) * nb + b] = phi[b];
+                for (int c = 0; c < 3; ++c) t->dphi_f[(((size_t)p * nqf + g) * nb + b) * 3 + c] = grad[3 * b + c];
+            }
         }
     t->phi_vT.assign(nb * nqv, 0.0);
     for (int g = 0; g < nqv; ++g)

@@ -174,6 +174,17 @@ int dg_ssprk3_timed(dg_ctx* ctx, double dt, int nsteps, double* out, int nclass)
 /* The context's CUDA stream (a cudaStream_t) on which every kernel of the context runs. */
 void* dg_stream(dg_ctx* ctx);
 
+/* Explicit viscous operator, replaces ExplicitDiffusion<Order, QuadC, QuadF>::eval(mesh, U, t)
+ * (include/DG/DG_Schemes/ExplicitDiffusion.h:133-626) with the context's order and rules: the
+ * interior-penalty Navier-Stokes viscous residual R of U, same sign and scaling as the reference
+ * (volume term subtracted, face terms added on cells[0] and subtracted on cells[1]). The reference
+ * fixes mu = 1 and Pr = 1; here they are arguments (gamma is the context's). Dirichlet faces use the
+ * data of dg_set_dirichlet. Host buffers with the element stride of dg_residual. */
+int dg_viscous_residual(dg_ctx* ctx, const double* U, double* R, size_t elem_stride_bytes, double mu, double prandtl);
+/* Same on device buffers, enqueued on `stream` (a cudaStream_t, 0 = default). */
+int dg_viscous_residual_device(dg_ctx* ctx, const double* U_dev, double* R_dev, double mu, double prandtl,
+                               void* stream);
+
 /* Positivity-preserving limiter, replaces PositiveLimiter<P, QuadC, OnlyNeigbAvg>::constructMinMax
  * (current, previous) followed by apply(current, previous) (include/DG/DG_Schemes/PositiveLimiter.h:
  * 12-261, called so in examples/Eular1D/Sod1D/Riemann1D.cpp:194-195), with QuadC the context's volume

@@ -143,6 +143,7 @@ class RefLib:
         L.fveref_ssprk3.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp,
                                     ctypes.c_double, ctypes.c_int, ctypes.c_double]
         L.fveref_mass.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp]
+        L.fveref_diffusion.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_double]
         L.fveref_limit.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_int]
         L.fveref_quad_tet.argtypes = [ctypes.c_int, dp, dp]
         L.fveref_quad_tri.argtypes = [ctypes.c_int, dp, dp]
@@ -250,6 +251,15 @@ class RefMesh:
         if rc != 0:
             raise RuntimeError(f"fveref_mass rc={rc}")
         return b
+
+    def diffusion(self, U, order, qv, qf, t=0.0):
+        """ExplicitDiffusion<P, QC, QF>::eval(mesh, U, t)."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        R = np.zeros_like(U)
+        rc = self.ref.L.fveref_diffusion(self.h, order, qv, qf, U.ctypes.data_as(dp), R.ctypes.data_as(dp), t)
+        if rc != 0:
+            raise RuntimeError(f"fveref_diffusion rc={rc}")
+        return R
 
     def limit(self, U, Uprev, order, qv, gamma=1.4, only_avg=False):
         """PositiveLimiter<P, QC, only_avg>: constructMinMax(U, Uprev) then apply(U, Uprev)."""

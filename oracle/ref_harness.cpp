@@ -20,7 +20,10 @@
 //   * PositiveLimiter<P, QuadC, OnlyNeigbAvg> (include/DG/DG_Schemes/PositiveLimiter.h:12-261) as the
 //     drivers call it: constructMinMax(current, previous) then apply(current, previous)
 //     (examples/Eular1D/Sod1D/Riemann1D.cpp:194-195).
+//   * ExplicitDiffusion<P, QuadC, QuadF>::eval (include/DG/DG_Schemes/ExplicitDiffusion.h:133-626),
+//     the explicit viscous operator (mu = 1, Pr = 1, gamma = 1.4 fixed there).
 #include "DG/DG_Schemes/ExplicitConvection.h"
+#include "DG/DG_Schemes/ExplicitDiffusion.h"
 #include "DG/DG_Schemes/PositiveLimiter.h"
 #include "src/DG/DG_Schemes/ExplicitConvection.cpp"
 
@@ -167,6 +170,16 @@ int run_mass(const ComputingMesh& m, double* mass) {
         }
     }
     from_lv<P>(b, nc, mass);
+    return 0;
+}
+
+template <uInt P, class QC, class QF>
+int run_diffusion(const ComputingMesh& m, const double* U, double* R, double t) {
+    const size_t nc = m.m_cells.size();
+    LongVector<5 * DGBasisEvaluator<P>::NumBasis> x(nc);
+    to_lv<P>(U, nc, x);
+    ExplicitDiffusion<P, QC, QF> d;
+    from_lv<P>(d.eval(m, x, t), nc, R);
     return 0;
 }
 
@@ -363,6 +376,15 @@ int fveref_ssprk3(void* p, int order, int gamma_id, int qv, int qf, double* U, c
     if (order == P && qv == QV && qf == QF)                                                       \
         return gamma_id == 0 ? run_ssprk3<P, AirFluxC, QC_, QF_>(m, U, mass, dt, nsteps, t0)      \
                              : run_ssprk3<P, MonatomicFluxC, QC_, QF_>(m, U, mass, dt, nsteps, t0);
+    FVEREF_COMBOS(X)
+#undef X
+    return -1;
+}
+
+int fveref_diffusion(void* p, int order, int qv, int qf, const double* U, double* R, double t) {
+    const ComputingMesh& m = *static_cast<RefMesh*>(p)->cm;
+#define X(P, QV, QF, QC_, QF_) \
+    if (order == P && qv == QV && qf == QF) return run_diffusion<P, QC_, QF_>(m, U, R, t);
     FVEREF_COMBOS(X)
 #undef X
     return -1;
