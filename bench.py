@@ -261,6 +261,8 @@ def main():
     ap.add_argument("--schedule", default=None, choices=["two-launch", "persistent"])
     ap.add_argument("--no-compare", action="store_true", help="skip timing the FP64 form beside the mixed one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--viscous", action="store_true",
+                    help="time the explicit viscous operator (ExplicitDiffusion::eval) on the workload's mesh instead")
     ap.add_argument("--limiter", default=None, choices=["positive", "positive-avg"],
                     help="positivity-preserving limiter after every RK stage (timed as its own kernel class)")
     ap.add_argument("--n", type=int, default=0, help="override the mesh size (cubes per side), for profiling")
@@ -289,6 +291,11 @@ def main():
 
     if args.config == "ensemble":
         run_ensemble(args, rank, world, local, dist)
+        if dist:
+            dist.destroy_process_group()
+        return
+    if args.viscous:
+        run_viscous(args, cfg, rank, world, local, dist)
         if dist:
             dist.destroy_process_group()
         return
@@ -448,6 +455,96 @@ def make_roofline(kt, precision, schedule, P, ncell, nface, nqf, nb, config):
                       "frac_of_fp64_nominal": FLOP_PER_DOF_STAGE[P] * 5 * nb * ncell / (stage_ms / 1e3) / 1e12
                       / FP64_NOMINAL_TFLOPS},
             "kernels_ms_per_launch": {names.get(k, str(k)): v[0] / v[1] for k, v in kt.items()}}
+
+
+def run_viscous(args, cfg, rank, world, local, dist):
+    """The explicit viscous operator (FP64, ExplicitDiffusion::eval) on the workload's mesh and state:
+    residual evaluations per second on device buffers (CUDA events, max over ranks), end to end with
+    host buffers through the C ABI, and the reference's own CPU operator on a bounded sample."""
+    import torch
+    from fve_dg_b200 import ExplicitConvection, box_mesh, launch_count, problems
+    from fve_dg_b200 import _lib as L
+    P, qv, qf = cfg["P"], cfg["qv"], cfg["qf"]
+    m = box_mesh(cfg["n"], hi=(cfg["L"],) * 3, jitter=cfg["jitter"])
+    U0 = problems.project(m, P, problem_fn(cfg["problem"], problems))
+    conv = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf, device=local)
+    nb = conv.num_basis
+    dof = 5 * nb * m.ncell
+    Ud = torch.from_numpy(U0).to(f"cuda:{local}")
+    Rd = torch.empty_like(Ud)
+    lib, s = L.lib(), conv.stream
+    stream = torch.cuda.ExternalStream(s)
+
+    def ev():
+        L.check(lib.dg_viscous_residual_device(conv._ctx, Ud.data_ptr(), Rd.data_ptr(), 1.0, 1.0, s), "viscous")
+
+    for _ in range(args.warmup):
+        ev()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = launch_count()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ev()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = launch_count() - l0
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = dof * args.steps * world / (ms / 1e3)
+    R = np.empty_like(U0)
+    k = max(3, min(args.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        L.check(lib.dg_viscous_residual(conv._ctx, L.dptr(U0), L.dptr(R), 0, 1.0, 1.0), "viscous")
+    e2e = dof * k * world / (time.perf_counter() - t0)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle.pyoracle import RefLib, RefMesh, ref_available
+        if ref_available():
+            ref = RefLib()
+            threads = os.cpu_count() or 1
+            ref.set_threads(threads)
+            n_s = max(4, min(cfg["n"], 12))
+            ms_ = box_mesh(n_s, hi=(cfg["L"],) * 3, jitter=cfg["jitter"])
+            Us = problems.project(ms_, P, problem_fn(cfg["problem"], problems))
+            rm = RefMesh.from_mesh(ref, ms_)
+            rm.diffusion(Us, P, qv, qf)
+            kk, t0 = 0, time.perf_counter()
+            while time.perf_counter() - t0 < 5.0 and kk < 50:
+                rm.diffusion(Us, P, qv, qf)
+                kk += 1
+            el = time.perf_counter() - t0
+            cpu = {"value": 5 * nb * ms_.ncell * kk / el, "unit": "DOF-residual/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": f"ExplicitDiffusion::eval, {cfg['problem']} P{P} on {n_s}^3x6={ms_.ncell} tets, "
+                             f"{kk} evaluations, {el:.1f} s", "cpu_model": cpu_model()}
+    if rank == 0:
+        ms_each = ms / args.steps
+        bytes_each = 2 * dof * 8 + m.ncell * (80 + 8 + 32) + m.nface * 48 * 2
+        peak, peak_kind = read_peaks()
+        line = {"metric": "viscous residual DOF evaluations/s", "value": value, "unit": "DOF-residual/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_each,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": args.config + "-viscous", "desc": cfg["desc"] + "; ExplicitDiffusion, mu = Pr = 1",
+                           "tets": m.ncell, "order": P, "parallelism": f"independent instance per GPU x{world}"},
+                "gpu_launches": launches,
+                "roofline": {"bound": "hbm", "kernel": "viscous_residual", "achieved": bytes_each / (ms_each / 1e3) / 1e9,
+                             "peak": peak, "unit": "GB/s", "frac": bytes_each / (ms_each / 1e3) / 1e9 / peak,
+                             "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": bytes_each,
+                             "note": "one thread per element recomputes its faces' neighbour traces in FP64: "
+                                     "FP64-arithmetic bound, not HBM bound"},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e, "unit": "DOF-residual/s", "h2d_bytes_per_step": dof * 8, "d2h_bytes_per_step": dof * 8,
+                        "steps": k}}
+        print(json.dumps(line), flush=True)
+    conv.close()
 
 
 def run_ensemble(args, rank, world, local, dist):

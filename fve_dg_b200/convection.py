@@ -160,7 +160,7 @@ class ExplicitConvection:
         f = L.lib().dg_ssprk3_graph if graph else L.lib().dg_ssprk3
         L.check(f(self._ctx, float(dt), int(nsteps)), "dg_ssprk3")
 
-    def ssprk3_timed(self, dt, nsteps, nclass=4):
+    def ssprk3_timed(self, dt, nsteps, nclass=5):
         """Step with CUDA events around every launch; returns {class: (total_ms, launches)}."""
         out = np.zeros(2 * nclass)
         L.check(L.lib().dg_ssprk3_timed(self._ctx, float(dt), int(nsteps), L.dptr(out), nclass), "dg_ssprk3_timed")

@@ -87,7 +87,7 @@ struct dg_ctx {
     QueueState* d_queue = nullptr;
     PersistentParams pp;
     QueueSchedule qs;
-    // limiter: per-face bounds [nface][10] and a staging buffer for host calls
+    // limiter: per-cell statistics [ncell][10] and a staging buffer for host calls
     double* d_lim_bnd = nullptr;
     double* d_lim_prev = nullptr;
     // viscous operator: reference gradients at the volume and face points, cell size h
@@ -496,8 +496,8 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
         if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
             c->sms = sms;
     }
-    // the limiter's per-face bounds, allocated here so that no step allocates (graph capture)
-    if (cfg->limiter && (rc = dev_alloc(&c->d_lim_bnd, (size_t)c->nface * 10))) return fail(c, rc);
+    // the limiter's per-cell statistics, allocated here so that no step allocates (graph capture)
+    if (cfg->limiter && (rc = dev_alloc(&c->d_lim_bnd, (size_t)c->ncell * 10))) return fail(c, rc);
     if (err) *err = DG_OK;
     return c;
 }
@@ -704,7 +704,7 @@ int dg_limit_device(dg_ctx* c, double* U, const double* Uprev, int only_avg, voi
     if (!limiter_supported(c->cfg.order, c->qv)) return DG_E_ARG;
     DG_CUDA(cudaSetDevice(c->cfg.device));
     int rc;
-    if (!c->d_lim_bnd && (rc = dev_alloc(&c->d_lim_bnd, (size_t)c->nface * 10))) return rc;
+    if (!c->d_lim_bnd && (rc = dev_alloc(&c->d_lim_bnd, (size_t)c->ncell * 10))) return rc;
     g_launches += 2;
     return launch_limiter(c->cfg.order, c->qv, U, Uprev, c->d_fi, c->d_ef, c->d_phi_v, c->ncell, c->nface,
                           c->cfg.gamma, only_avg != 0, c->d_lim_bnd, nullptr, c->sms, (cudaStream_t)stream);

@@ -16,8 +16,9 @@
 //     smallest t.
 // Means are never changed, so mass, momentum and energy are conserved exactly.
 //
-// One warp per face / element, lanes over the quadrature points; each point value is summed over
-// the modes in order, as the reference does. Warps never wait on one another.
+// Two passes, one warp per cell, lanes over the quadrature points (each point value summed over the
+// modes in order, as the reference does): per-cell statistics of the previous state, then the bounds
+// and the three steps. Warps never wait on one another.
 #pragma once
 #include <cfloat>
 
@@ -57,99 +58,139 @@ __device__ __forceinline__ double limiter_pressure(const double U[5], double gam
 }
 
 constexpr int kLimWarps = 4;
+constexpr int kLimMaxPts = 64;  // volume points a warp holds, two per lane (the largest rule has 57)
 
+// The 5 conserved values at volume point g.
+template <int NB>
+__device__ __forceinline__ void point_values(const double* phi_g, const double* u, double v[5]) {
+    #pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] = 0.0;
+    for (int l = 0; l < NB; ++l) {
+        const double p = phi_g[l];
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) v[k] = fma(p, u[k + 5 * l], v[k]);
+    }
+}
+
+// Per-cell statistics of the previous state for the bounds: the max over the volume points of
+// each variable and the values at the last point. A face's bounds are max(v1, v2) over the points
+// and min(v1, v2) at the last point (PositiveLimiter.h:77-88), i.e. the max of its two cells' maxima
+// and the min of their last-point values; with only_avg both are the cell mean (:70-75).
 template <int NB, int NQV>
 __global__ void __launch_bounds__(kLimWarps * 32)
-    limiter_face_bounds(const double* __restrict__ Up, const FaceInfo* __restrict__ fi,
-                        const double* __restrict__ phi, int64_t nface, int only_avg, double* __restrict__ bnd) {
+    limiter_cell_stats(const double* __restrict__ Up, const double* __restrict__ phi, int64_t ncell, int only_avg,
+                       double* __restrict__ stats) {
     __shared__ double sphi[NQV * NB];
+    __shared__ double scoef[kLimWarps][5 * NB];
     for (int i = threadIdx.x; i < NQV * NB; i += blockDim.x) sphi[i] = phi[i];
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    for (int64_t f = (int64_t)blockIdx.x * kLimWarps + (threadIdx.x >> 5); f < nface;
-         f += (int64_t)gridDim.x * kLimWarps) {
-        const FaceInfo F = fi[f];
-        const double* u1 = Up + (int64_t)F.c0 * (5 * NB);
-        const double* u2 = Up + (int64_t)(F.c1 >= 0 ? F.c1 : F.c0) * (5 * NB);
-        double* out = bnd + f * 10;
+    double* su = scoef[threadIdx.x >> 5];
+    for (int64_t c = (int64_t)blockIdx.x * kLimWarps + (threadIdx.x >> 5); c < ncell;
+         c += (int64_t)gridDim.x * kLimWarps) {
+        const double* ug = Up + c * (5 * NB);
+        for (int i = lane; i < 5 * NB; i += 32) su[i] = ug[i];  // coalesced, then broadcast reads
+        __syncwarp();
+        const double* u = su;
+        double* out = stats + c * 10;
         if (only_avg) {
-            if (lane < 5) {
-                out[lane] = ref_max(u1[lane], u2[lane]);
-                out[5 + lane] = ref_min(u1[lane], u2[lane]);
-            }
+            if (lane < 5) { out[lane] = u[lane]; out[5 + lane] = u[lane]; }
+            __syncwarp();
             continue;
         }
-        double mx[5], lastmin[5];
+        double mx[5], last[5];
         #pragma unroll
-        for (int k = 0; k < 5; ++k) { mx[k] = -DBL_MAX; lastmin[k] = DBL_MAX; }
+        for (int k = 0; k < 5; ++k) { mx[k] = -DBL_MAX; last[k] = 0.0; }
         for (int g = lane; g < NQV; g += 32) {
+            double v[5];
+            point_values<NB>(sphi + g * NB, u, v);
             #pragma unroll
             for (int k = 0; k < 5; ++k) {
-                const double v1 = point_value<NB>(sphi + g * NB, u1, k), v2 = point_value<NB>(sphi + g * NB, u2, k);
-                mx[k] = ref_max(mx[k], ref_max(v1, v2));
-                if (g == NQV - 1) lastmin[k] = ref_min(v1, v2);
+                mx[k] = ref_max(mx[k], v[k]);
+                if (g == NQV - 1) last[k] = v[k];
             }
         }
         #pragma unroll
         for (int k = 0; k < 5; ++k) {
             mx[k] = warp_max(mx[k]);
-            lastmin[k] = __shfl_sync(0xffffffffu, lastmin[k], (NQV - 1) % 32);
+            last[k] = __shfl_sync(0xffffffffu, last[k], (NQV - 1) % 32);
         }
         if (lane < 5) {
-            double a = mx[0], b = lastmin[0];
+            double a = mx[0], b = last[0];
             #pragma unroll
             for (int k = 1; k < 5; ++k)
-                if (lane == k) { a = mx[k]; b = lastmin[k]; }
+                if (lane == k) { a = mx[k]; b = last[k]; }
             out[lane] = a;
             out[5 + lane] = b;
         }
+        __syncwarp();
     }
 }
 
-// mir: when non-null, the element's split coefficient rows (A rows, [ncell][5][KB]) are rewritten
-// if the limiter changed the element, so the mixed form's next stage reads the limited state.
+// The three steps per element (PositiveLimiter.h:128-258). Point values are evaluated once; after a
+// step scales the modes l >= 1 of a variable by theta, its point values become avg + theta (v - avg)
+// (phi_0 = 1), which is what the reference re-evaluates. mir: when non-null, the element's split
+// coefficient rows (A rows, [ncell][5][KB]) are rewritten if the limiter changed the element.
 template <int NB, int NQV>
 __global__ void __launch_bounds__(kLimWarps * 32)
-    limiter_apply(double* __restrict__ U, const ElemFace* __restrict__ ef, const double* __restrict__ bnd,
-                  const double* __restrict__ phi, int64_t ncell, double gamma, uint32_t* __restrict__ mir) {
+    limiter_apply(double* __restrict__ U, const ElemFace* __restrict__ ef, const FaceInfo* __restrict__ fi,
+                  const double* __restrict__ stats, const double* __restrict__ phi, int64_t ncell, double gamma,
+                  uint32_t* __restrict__ mir) {
     constexpr int KB = pad8(NB - 1);
+    constexpr int PPL = (NQV + 31) / 32;  // points per lane
+    static_assert(NQV <= kLimMaxPts, "volume rule too large");
     __shared__ double sphi[NQV * NB];
+    __shared__ double scoef[kLimWarps][5 * NB];
     for (int i = threadIdx.x; i < NQV * NB; i += blockDim.x) sphi[i] = phi[i];
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    double* u = scoef[threadIdx.x >> 5];
     for (int64_t e = (int64_t)blockIdx.x * kLimWarps + (threadIdx.x >> 5); e < ncell;
          e += (int64_t)gridDim.x * kLimWarps) {
-        double* u = U + e * (5 * NB);
-        // the cell's bounds: max/min over its faces (constructMinMax, :92-102)
+        double* ug = U + e * (5 * NB);
+        for (int i = lane; i < 5 * NB; i += 32) u[i] = ug[i];  // coalesced, then broadcast reads
+        __syncwarp();
+        // the cell's bounds over its faces (constructMinMax, :92-102); a boundary face has one cell
         double gmax = -DBL_MAX, gmin = DBL_MAX;
         if (lane < 5) {
             #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int64_t f = ef[4 * e + q].face;
-                gmax = ref_max(gmax, bnd[f * 10 + lane]);
-                gmin = ref_min(gmin, bnd[f * 10 + 5 + lane]);
+                const FaceInfo& F = fi[ef[4 * e + q].face];
+                const int64_t c0 = F.c0, c1 = F.c1 >= 0 ? F.c1 : F.c0;
+                gmax = ref_max(gmax, ref_max(stats[c0 * 10 + lane], stats[c1 * 10 + lane]));
+                gmin = ref_min(gmin, ref_min(stats[c0 * 10 + 5 + lane], stats[c1 * 10 + 5 + lane]));
             }
         }
+        double avg[5], v[PPL][5];
+        #pragma unroll
+        for (int k = 0; k < 5; ++k) avg[k] = u[k];
+        #pragma unroll
+        for (int r = 0; r < PPL; ++r) {
+            const int g = lane + 32 * r;
+            if (g < NQV) point_values<NB>(sphi + g * NB, u, v[r]);
+            else
+                #pragma unroll
+                for (int k = 0; k < 5; ++k) v[r][k] = avg[k];  // neutral for min/max and pressure
+        }
+        double scale[5] = {1.0, 1.0, 1.0, 1.0, 1.0};
         bool changed = false;
         // step 1: each variable within the cell's bounds
+        #pragma unroll
         for (int k = 0; k < 5; ++k) {
             const double bmax = __shfl_sync(0xffffffffu, gmax, k), bmin = __shfl_sync(0xffffffffu, gmin, k);
-            const double avg = u[k];
             double vmin = DBL_MAX, vmax = -DBL_MAX;
-            for (int g = lane; g < NQV; g += 32) {
-                const double v = point_value<NB>(sphi + g * NB, u, k);
-                vmin = ref_min(vmin, v);
-                vmax = ref_max(vmax, v);
-            }
+            #pragma unroll
+            for (int r = 0; r < PPL; ++r)
+                if (lane + 32 * r < NQV) { vmin = ref_min(vmin, v[r][k]); vmax = ref_max(vmax, v[r][k]); }
             vmin = warp_min(vmin);
             vmax = warp_max(vmax);
             if (vmin < bmin || vmax > bmax) {
-                const double tmin = (avg != vmin) ? (avg - bmin) / (avg - vmin + 1e-32) : 0.0;
-                const double tmax = (avg != vmax) ? (bmax - avg) / (vmax - avg + 1e-32) : 0.0;
+                const double tmin = (avg[k] != vmin) ? (avg[k] - bmin) / (avg[k] - vmin + 1e-32) : 0.0;
+                const double tmax = (avg[k] != vmax) ? (bmax - avg[k]) / (vmax - avg[k] + 1e-32) : 0.0;
                 const double theta = ref_min(ref_min(tmin, tmax), 1.0);
-                __syncwarp();
-                for (int l = 1 + lane; l < NB; l += 32) u[k + 5 * l] *= theta;
-                __syncwarp();
+                scale[k] *= theta;
+                #pragma unroll
+                for (int r = 0; r < PPL; ++r) v[r][k] = avg[k] + theta * (v[r][k] - avg[k]);
                 changed = true;
             }
         }
@@ -157,59 +198,59 @@ __global__ void __launch_bounds__(kLimWarps * 32)
         {
             const double eps = 1e-16;
             double rmin = DBL_MAX;
-            for (int g = lane; g < NQV; g += 32) rmin = ref_min(rmin, point_value<NB>(sphi + g * NB, u, 0));
+            #pragma unroll
+            for (int r = 0; r < PPL; ++r)
+                if (lane + 32 * r < NQV) rmin = ref_min(rmin, v[r][0]);
             rmin = warp_min(rmin);
-            const double ravg = u[0];
             if (rmin < eps) {
-                const double eff = ref_max(ravg, eps);
+                const double eff = ref_max(avg[0], eps);
                 const double num = eff - eps, den = eff - rmin;
                 const double theta = (den < 1e-32) ? 0.0 : ref_min(1.0, num / den);
-                __syncwarp();
-                for (int l = 1 + lane; l < NB; l += 32) u[5 * l] *= theta;
-                __syncwarp();
+                scale[0] *= theta;
+                #pragma unroll
+                for (int r = 0; r < PPL; ++r) v[r][0] = avg[0] + theta * (v[r][0] - avg[0]);
                 changed = true;
             }
         }
         // step 3: pressure at the points >= 0 by bisection toward the mean
-        {
-            double avgU[5];
-            #pragma unroll
-            for (int k = 0; k < 5; ++k) avgU[k] = u[k];
-            double tp = 1.0;
-            for (int g = lane; g < NQV; g += 32) {
-                double pu[5];
+        double tp = 1.0;
+        #pragma unroll
+        for (int r = 0; r < PPL; ++r) {
+            if (lane + 32 * r >= NQV || limiter_pressure(v[r], gamma) >= 0) continue;
+            double lo = 0.0, hi = 1.0, mid = 0.5 * (lo + hi);
+            for (int it = 0; it < 100; ++it) {
+                mid = 0.5 * (lo + hi);
+                double um[5];
                 #pragma unroll
-                for (int k = 0; k < 5; ++k) pu[k] = point_value<NB>(sphi + g * NB, u, k);
-                if (limiter_pressure(pu, gamma) >= 0) continue;
-                double lo = 0.0, hi = 1.0, mid = 0.5 * (lo + hi);
-                for (int it = 0; it < 100; ++it) {
-                    mid = 0.5 * (lo + hi);
-                    double um[5];
-                    #pragma unroll
-                    for (int k = 0; k < 5; ++k) um[k] = (1.0 - mid) * avgU[k] + mid * pu[k];
-                    if (limiter_pressure(um, gamma) < 0) hi = mid;
-                    else lo = mid;
-                }
-                tp = ref_min(tp, mid);
+                for (int k = 0; k < 5; ++k) um[k] = (1.0 - mid) * avg[k] + mid * v[r][k];
+                if (limiter_pressure(um, gamma) < 0) hi = mid;
+                else lo = mid;
             }
-            tp = warp_min(tp);
-            if (tp != 1.0) {
-                __syncwarp();
-                for (int i = lane; i < 5 * (NB - 1); i += 32) u[5 + i] *= tp;
-                __syncwarp();
-                changed = true;
-            }
+            tp = ref_min(tp, mid);
         }
-        if (mir && changed) {  // refresh the split rows of the changed element
-            for (int i = lane; i < 5 * (KB / 2); i += 32) {
-                const int k = i / (KB / 2), x = 2 * (i - k * (KB / 2));
-                const float v0 = x + 1 < NB ? (float)u[5 * (x + 1) + k] : 0.f;
-                const float v1 = x + 2 < NB ? (float)u[5 * (x + 2) + k] : 0.f;
-                uint32_t h, l;
-                split2(v0, v1, h, l);
-                uint32_t* row = mir + (e * 5 + k) * KB;
-                row[arow_hi_word<KB>(x)] = h;
-                row[arow_lo_word<KB>(x)] = l;
+        tp = warp_min(tp);
+        if (tp != 1.0) changed = true;
+        if (changed) {  // modes l >= 1: c *= theta_1 [*= theta_rho] *= theta_p, in the reference's order
+            for (int i = lane; i < 5 * (NB - 1); i += 32) {
+                const int k = i % 5;
+                double c = u[5 + i];
+                if (scale[k] != 1.0 || (k == 0 && scale[0] != 1.0)) c *= scale[k];
+                if (tp != 1.0) c *= tp;
+                u[5 + i] = c;
+                ug[5 + i] = c;
+            }
+            __syncwarp();
+            if (mir) {  // refresh the split rows of the changed element
+                for (int i = lane; i < 5 * (KB / 2); i += 32) {
+                    const int k = i / (KB / 2), x = 2 * (i - k * (KB / 2));
+                    const float v0 = x + 1 < NB ? (float)u[5 * (x + 1) + k] : 0.f;
+                    const float v1 = x + 2 < NB ? (float)u[5 * (x + 2) + k] : 0.f;
+                    uint32_t h, l;
+                    split2(v0, v1, h, l);
+                    uint32_t* row = mir + (e * 5 + k) * KB;
+                    row[arow_hi_word<KB>(x)] = h;
+                    row[arow_lo_word<KB>(x)] = l;
+                }
             }
         }
         __syncwarp();
@@ -235,16 +276,15 @@ inline bool limiter_supported(int order, int qv) {
     return false;
 }
 
-// Bounds from Uprev, then the three steps on U (in place). bnd: [nface][10] scratch.
+// Bounds from Uprev, then the three steps on U (in place). stats: [ncell][10] scratch.
 inline int launch_limiter(int order, int qv, double* U, const double* Uprev, const FaceInfo* fi, const ElemFace* ef,
-                          const double* phi_v, int64_t ncell, int64_t nface, double gamma, int only_avg, double* bnd,
-                          uint32_t* mir, int sms, cudaStream_t s) {
+                          const double* phi_v, int64_t ncell, int64_t /*nface*/, double gamma, int only_avg,
+                          double* stats, uint32_t* mir, int sms, cudaStream_t s) {
 #define X(P, QV, NB, NQV)                                                                                        \
     if (order == P && qv == QV) {                                                                                \
-        const unsigned gf = (unsigned)std::min<int64_t>((nface + kLimWarps - 1) / kLimWarps, (int64_t)sms * 16); \
-        limiter_face_bounds<NB, NQV><<<gf, kLimWarps * 32, 0, s>>>(Uprev, fi, phi_v, nface, only_avg, bnd);      \
         const unsigned ge = (unsigned)std::min<int64_t>((ncell + kLimWarps - 1) / kLimWarps, (int64_t)sms * 16); \
-        limiter_apply<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(U, ef, bnd, phi_v, ncell, gamma, mir);             \
+        limiter_cell_stats<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(Uprev, phi_v, ncell, only_avg, stats);         \
+        limiter_apply<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(U, ef, fi, stats, phi_v, ncell, gamma, mir);       \
         return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;                                            \
     }
     FVEDG_LIMITER_COMBOS(X)
