@@ -284,12 +284,12 @@ int limit_stage(dg_ctx* c, const double* in, double* out, uint32_t* mir, cudaStr
     });
 }
 
-int step_fp64(dg_ctx* c, double dt, cudaStream_t s) {
+int step_fp64(dg_ctx* c, double dt, cudaStream_t s, int st0, int st1) {
     const double A0[3] = {0.0, 0.75, 1.0 / 3.0};
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
     const double* in[3] = {c->d_Un, c->d_Ua, c->d_Ub};
     double* out[3] = {c->d_Ua, c->d_Ub, c->d_Un};
-    for (int st = 0; st < 3; ++st) {
+    for (int st = st0; st < st1; ++st) {
         int rc = timed(c, 0, s, [&] { return dispatch_face(c->cfg.order, c->qv, c->qf, face_args(c, in[st], 3), s); });
         if (rc) return rc;
         rc = timed(c, 1, s, [&] {
@@ -301,17 +301,18 @@ int step_fp64(dg_ctx* c, double dt, cudaStream_t s) {
     return DG_OK;
 }
 
-int step(dg_ctx* c, double dt, cudaStream_t s) {
+// Stages st0..st1-1 of one step (all three by default).
+int step(dg_ctx* c, double dt, cudaStream_t s, int st0 = 0, int st1 = 3) {
     if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
     auto tm = [&](int cls, auto&& fn) { return timed(c, cls, s, fn); };
     if (c->cfg.precision == DG_PREC_MIXED) {
         auto post = [&](const double* in, double* out, int mir) { return limit_stage(c, in, out, c->mixed.mir[mir], s); };
         if (c->cfg.schedule == 1)
             return step_persistent(c->mixed, c->d_queue, c->qs, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches,
-                                   tm, post);
-        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm, post);
+                                   tm, post, st0, st1);
+        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm, post, st0, st1);
     }
-    return step_fp64(c, dt, s);
+    return step_fp64(c, dt, s, st0, st1);
 }
 
 int launches_per_step(const dg_ctx* c) {
@@ -796,6 +797,26 @@ int dg_ssprk3_ensemble(dg_ctx* c, const double* dt, int nsteps, int use_graph) {
 }
 
 void* dg_stream(dg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+double* dg_state_device(dg_ctx* c, int which) {
+    if (!c || which < 0 || which > 2) return nullptr;
+    return which == 0 ? c->d_Un : which == 1 ? c->d_Ua : c->d_Ub;
+}
+
+int dg_refresh_split(dg_ctx* c, int which, const int64_t* elems, int64_t n, void* stream) {
+    if (!c || which < 0 || which > 2 || n < 0 || (n > 0 && !elems)) return DG_E_ARG;
+    if (c->cfg.precision != DG_PREC_MIXED || n == 0) return DG_OK;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    const cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    return mixed_mirror_list(c->mixed, dg_state_device(c, which), which, elems, n, s, &g_launches);
+}
+
+int dg_ssprk3_stage(dg_ctx* c, double dt, int stage) {
+    if (!c || stage < 0 || stage > 2 || !(dt >= 0)) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    return step(c, dt, c->stream, stage, stage + 1);
+}
 
 int dg_ssprk3_timed(dg_ctx* c, double dt, int nsteps, double* out, int nclass) {
     if (!c || nsteps < 0 || !(dt >= 0) || !out || nclass <= 0) return DG_E_ARG;

@@ -235,14 +235,17 @@ __device__ __forceinline__ void mma_bt(float acc[4], const AFrag<K>& A, const ui
 // Writes the split deviation coefficients of a state as A rows (after an upload, or for a residual
 // of an arbitrary state): one thread per (element, var, column pair).
 template <int NB>
-__global__ void mirror_split(const double* __restrict__ U, uint32_t* __restrict__ mir, int64_t ncell) {
+__global__ void mirror_split(const double* __restrict__ U, uint32_t* __restrict__ mir, int64_t ncell,
+                             const int64_t* __restrict__ list) {
     constexpr int KB = pad8(NB - 1), NP = KB / 2;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ncell * 5 * NP) return;
-    const int64_t row = i / NP;
-    const int x = 2 * (int)(i - row * NP);
-    const int64_t e = row / 5;
-    const int k = (int)(row - e * 5);
+    const int64_t r = i / NP;
+    const int x = 2 * (int)(i - r * NP);
+    const int64_t j = r / 5;
+    const int k = (int)(r - j * 5);
+    const int64_t e = list ? list[j] : j;  // the listed elements only (ghost rows after an exchange)
+    const int64_t row = e * 5 + k;
     const double* u = U + e * (5 * NB) + k;
     const float v0 = x + 1 < NB ? (float)u[5 * (x + 1)] : 0.f;
     const float v1 = x + 2 < NB ? (float)u[5 * (x + 2)] : 0.f;
@@ -988,7 +991,7 @@ inline int mixed_launch(MixedData& m, int which, const double* U, const double* 
                         int mir_in, int mir_out) {
     if (which == 4) {
         const int64_t n = m.ncell * 5 * (pad8(NB - 1) / 2);
-        mirror_split<NB><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(U, m.mir[mir_in], m.ncell);
+        mirror_split<NB><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(U, m.mir[mir_in], m.ncell, nullptr);
     } else if (which == 0) {
         constexpr int W = 4;  // 4-warp CTAs: finer-grained scheduling than 8 at the same occupancy
         const int g = (int)std::min<int64_t>((m.nfgroups + W - 1) / W, (int64_t)m.sms * 64);
@@ -1039,6 +1042,23 @@ inline int mixed_mirror(MixedData& m, const double* U, int mir, cudaStream_t s, 
     return mixed_kernel(m, 4, U, U, nullptr, 0, 0.0, 0.0, 0.0, 0, 0, s, launches, mir, -1);
 }
 
+// Rewrites the mirror rows of the listed elements only (device list of n element indices).
+inline int mixed_mirror_list(MixedData& m, const double* U, int mir, const int64_t* list, int64_t n, cudaStream_t s,
+                             std::atomic<int64_t>* launches) {
+    if (!m.ready) return DG_E_ARG;
+    if (n == 0) return DG_OK;
+#define X(P, QV, QF, NB, NQV, NQF, W)                                                                   \
+    if (m.order == P && m.qv == QV && m.qf == QF) {                                                     \
+        const int64_t nt = n * 5 * (pad8(NB - 1) / 2);                                                  \
+        ++*launches;                                                                                    \
+        mirror_split<NB><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(U, m.mir[mir], n, list);          \
+        return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;                                   \
+    }
+    FVEDG_MIXED_COMBOS(X)
+#undef X
+    return DG_E_ARG;
+}
+
 inline int residual_mixed(MixedData& m, const double* U, double* R, int part, cudaStream_t s,
                           std::atomic<int64_t>* launches) {
     const int mask = part == 0 ? 3 : part == 1 ? 0 : part == 2 ? 1 : 2;
@@ -1052,16 +1072,17 @@ inline int mixed_launches_per_step(const MixedData&) { return 6; }
 
 // SSP-RK3 step; `timed(cls, fn)` runs fn (one launch) and may bracket it with timing events. The
 // mirror of Un must be current (the upload writes it, and stage 3 of every step rewrites it).
-// `post(in, out, mir_out)` runs after every stage (the limiter, or nothing).
+// `post(in, out, mir_out)` runs after every stage (the limiter, or nothing). Stages st0..st1-1 only
+// (one stage at a time when a halo exchange runs between stages).
 template <class Timed, class Post>
 inline int step_mixed(MixedData& m, double* Un, double* Ua, double* Ub, double dt, cudaStream_t s,
-                      std::atomic<int64_t>* launches, Timed&& timed, Post&& post) {
+                      std::atomic<int64_t>* launches, Timed&& timed, Post&& post, int st0 = 0, int st1 = 3) {
     const double A0[3] = {0.0, 0.75, 1.0 / 3.0};
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
     const double* in[3] = {Un, Ua, Ub};
     double* out[3] = {Ua, Ub, Un};
     const int mi[3] = {0, 1, 2}, mo[3] = {1, 2, 0};
-    for (int st = 0; st < 3; ++st) {
+    for (int st = st0; st < st1; ++st) {
         int rc = mixed_stage(m, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches, timed, mi[st], mo[st]);
         if (rc || (rc = post(in[st], out[st], mo[st]))) return rc;
     }

@@ -256,13 +256,14 @@ inline int persistent_kernel(MixedData& m, QueueState* q, const QueueSchedule& q
 template <class Timed, class Post>
 inline int step_persistent(MixedData& m, QueueState* q, const QueueSchedule& qs, const PersistentParams& pp,
                            double* Un, double* Ua, double* Ub, double dt, cudaStream_t s,
-                           std::atomic<int64_t>* launches, Timed&& timed, Post&& post) {
+                           std::atomic<int64_t>* launches, Timed&& timed, Post&& post, int st0 = 0,
+                           int st1 = 3) {
     const double A0[3] = {0.0, 0.75, 1.0 / 3.0};
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
     const double* in[3] = {Un, Ua, Ub};
     double* out[3] = {Ua, Ub, Un};
     const int mi[3] = {0, 1, 2}, mo[3] = {1, 2, 0};
-    for (int st = 0; st < 3; ++st) {
+    for (int st = st0; st < st1; ++st) {
         int rc = timed(2, [&] {
             return persistent_kernel(m, q, qs, pp, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches,
                                      mi[st], mo[st]);

@@ -1,0 +1,249 @@
+"""One mesh across several GPUs: element partition, local meshes with ghost cells, and the per-stage
+halo exchange of coefficient blocks.
+
+Each rank owns a contiguous range of the mesh's elements (on the box meshes, slabs). Its local mesh
+holds the owned elements first, then the ghost elements: the face neighbours of owned elements
+that another rank owns. The local faces are every face that touches an owned element, with its
+cells renumbered and its orientation unchanged, so an owned element sees exactly the faces,
+normals and face maps it has in the whole mesh. A ghost's other faces become boundary faces of a
+type that contributes nothing. Its own residual is therefore wrong, but a ghost's state is
+overwritten by its owner's before every stage, and only ghost values are ever read.
+
+Before each RK stage the stage input's ghost entries are refreshed: every rank sends, to each
+neighbouring rank, the coefficient blocks of its owned elements that are ghosts there, and
+unpacks what it receives into its ghost slots (one send and one receive per neighbour,
+`torch.distributed.batch_isend_irecv`, NCCL between GPUs). Owned results then equal the
+whole-mesh results: the same faces, in the same order, see the same inputs.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from .mesh import BC, Mesh
+
+INACTIVE_BC = BC["Neumann"]  # a boundary type the operator treats as contributing nothing
+
+
+def partition_elements(mesh, nparts):
+    """Owner of every element: nparts contiguous, balanced ranges of the element numbering."""
+    return (np.arange(mesh.ncell, dtype=np.int64) * nparts) // mesh.ncell
+
+
+class LocalMesh:
+    """Rank `rank`'s part of `mesh` under the ownership `part` (see the module docstring)."""
+
+    def __init__(self, mesh, part, rank):
+        part = np.asarray(part, dtype=np.int64)
+        nparts = int(part.max()) + 1
+        self.rank, self.nparts = rank, nparts
+        fc = mesh.face_cells
+        c0, c1 = fc[:, 0], fc[:, 1]
+        own = part == rank
+        c1s = np.where(c1 >= 0, c1, c0)
+        touch = own[c0] | ((c1 >= 0) & own[c1s])
+        other = np.where(own[c0], c1, c0)[touch]
+        owned = np.flatnonzero(own)
+        ghosts = np.unique(other[(other >= 0) & ~own[np.maximum(other, 0)]])
+        self.owned, self.ghosts = owned, ghosts
+        self.n_owned = len(owned)
+        self.l2g = np.concatenate([owned, ghosts])
+        g2l = np.full(mesh.ncell, -1, dtype=np.int64)
+        g2l[self.l2g] = np.arange(len(self.l2g))
+        # faces touching owned elements keep their orientation and order
+        tf = np.flatnonzero(touch)
+        faces = [mesh.faces[tf]]
+        fcs = [np.stack([g2l[c0[tf]], np.where(c1[tf] >= 0, g2l[c1s[tf]], -1)], axis=1)]
+        fn1 = [mesh.face_nodes1[tf] if mesh.face_nodes1 is not None else mesh.faces[tf]]
+        per = [mesh.periodic[tf] if mesh.periodic is not None else np.zeros(len(tf), np.uint8)]
+        bcs = [mesh.bc[tf] if mesh.bc is not None else np.full(len(tf), BC["Pseudo3DZ"], np.uint8)]
+        # the ghosts' remaining faces, as inactive boundary faces of the ghost
+        is_ghost = np.zeros(mesh.ncell, dtype=bool)
+        is_ghost[ghosts] = True
+        rest = np.flatnonzero(~touch)
+        for side, cells in ((0, c0), (1, c1)):
+            sel = rest[(cells[rest] >= 0) & is_ghost[np.maximum(cells[rest], 0)]]
+            if not len(sel):
+                continue
+            nodes = mesh.faces[sel] if (side == 0 or mesh.face_nodes1 is None) else mesh.face_nodes1[sel]
+            faces.append(nodes)
+            fcs.append(np.stack([g2l[cells[sel]], np.full(len(sel), -1)], axis=1))
+            fn1.append(nodes)
+            per.append(np.zeros(len(sel), np.uint8))
+            bcs.append(np.full(len(sel), INACTIVE_BC, np.uint8))
+        self.mesh = Mesh(mesh.points, mesh.cells[self.l2g], np.concatenate(faces), np.concatenate(fcs),
+                         np.concatenate(fn1), np.concatenate(per), np.concatenate(bcs))
+        self.global_face = tf  # local face i < len(tf) is global face tf[i]
+        # exchange plan: what this rank sends to / receives from every other rank, by global id
+        ghost_owner = part[ghosts]
+        self.recv = {int(q): g2l[ghosts[ghost_owner == q]] for q in np.unique(ghost_owner)}
+        self.send = {}
+        for q in range(nparts):
+            if q == rank:
+                continue
+            theirs = LocalMesh.ghost_set(mesh, part, q)
+            mine = theirs[part[theirs] == rank]
+            if len(mine):
+                self.send[q] = g2l[mine]
+
+    @staticmethod
+    def ghost_set(mesh, part, rank):
+        """Global ids of rank `rank`'s ghost elements, sorted."""
+        fc = mesh.face_cells
+        c0, c1 = fc[:, 0], fc[:, 1]
+        own = np.asarray(part) == rank
+        c1s = np.where(c1 >= 0, c1, c0)
+        touch = own[c0] | ((c1 >= 0) & own[c1s])
+        other = np.where(own[c0], c1, c0)[touch]
+        return np.unique(other[(other >= 0) & ~own[np.maximum(other, 0)]])
+
+    @property
+    def ncell(self):
+        return len(self.l2g)
+
+
+def halo_exchange(state, lm, dist):
+    """Fill the ghost rows of `state` (a torch tensor [local cells][...]) from their owners: one
+    send and one receive per neighbouring rank. Every rank calls it with the same sequence."""
+    import torch
+    cache = lm.__dict__.setdefault("_index_cache", {})
+    key = str(state.device)
+    if key not in cache:
+        cache[key] = ({q: torch.as_tensor(i, device=state.device) for q, i in lm.send.items()},
+                      {q: torch.as_tensor(i, device=state.device) for q, i in lm.recv.items()})
+    send_idx, recv_idx = cache[key]
+    ops, bufs = [], []
+    for q in sorted(send_idx):
+        buf = state.index_select(0, send_idx[q])
+        bufs.append(buf)
+        ops.append(dist.P2POp(dist.isend, buf, q))
+    recvs = []
+    for q in sorted(recv_idx):
+        buf = torch.empty((len(recv_idx[q]),) + tuple(state.shape[1:]), dtype=state.dtype, device=state.device)
+        recvs.append((recv_idx[q], buf))
+        ops.append(dist.P2POp(dist.irecv, buf, q))
+    if ops:
+        for r in dist.batch_isend_irecv(ops):
+            r.wait()
+    for idx, buf in recvs:
+        state.index_copy_(0, idx, buf)
+
+
+class _DeviceArray:
+    """A device buffer of the library, viewed by torch through __cuda_array_interface__."""
+
+    def __init__(self, ptr, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+class PartitionedConvection:
+    """ExplicitConvection on rank `rank`'s part of one mesh: SSP-RK3 with a halo exchange before
+    every stage, all of it ordered on the context's CUDA stream (the exchange's gathers, the NCCL
+    sends and receives and the scatters run on that stream; the host never waits between stages).
+    `dist` is torch.distributed with a process group over the parts; single-process users pass
+    `exchange` instead, a callable (which) that fills the ghost rows of state buffer `which` on
+    the context's stream."""
+
+    def __init__(self, mesh, part, rank, dist=None, exchange=None, device=0, **kw):
+        from .convection import ExplicitConvection
+        if (dist is None) == (exchange is None):
+            raise ValueError("give exactly one of dist and exchange")
+        self.lm = LocalMesh(mesh, part, rank)
+        self.conv = ExplicitConvection(self.lm.mesh, device=device, **kw)
+        self.dist, self._exchange, self.device = dist, exchange, device
+        self.mixed = self.conv.precision == "mixed"
+        self._ghost_dev = None
+        self._idx = None
+
+    def torch_stream(self):
+        import torch
+        return torch.cuda.ExternalStream(self.conv.stream, device=torch.device("cuda", self.device))
+
+    def state_view(self, which):
+        """Torch view of device state buffer `which` (0 = U^n, 1 = U^(1), 2 = U^(2))."""
+        import torch
+        ptr = L.lib().dg_state_device(self.conv._ctx, int(which))
+        if not ptr:
+            raise ValueError(f"no state buffer {which}")
+        with torch.cuda.device(self.device):
+            return torch.as_tensor(_DeviceArray(ptr, self.conv.shape), device=torch.device("cuda", self.device))
+
+    def set_state(self, U_global):
+        self.conv.set_state(np.asarray(U_global)[self.lm.l2g])
+
+    def get_owned(self):
+        return self.conv.get_state()[: self.lm.n_owned]
+
+    def _refresh(self, which):
+        """After ghost rows of buffer `which` changed: the mixed form re-splits their coefficients."""
+        if not self.mixed or not len(self.lm.ghosts):
+            return
+        import torch
+        if self._ghost_dev is None:
+            self._ghost_dev = torch.arange(self.lm.n_owned, self.lm.ncell, dtype=torch.int64,
+                                           device=torch.device("cuda", self.device))
+        L.check(L.lib().dg_refresh_split(self.conv._ctx, int(which), ctypes.c_void_p(self._ghost_dev.data_ptr()),
+                                         int(self._ghost_dev.numel()), None), "dg_refresh_split")
+
+    def exchange(self, which):
+        """Fill the ghost rows of state buffer `which` from their owners (stream-ordered)."""
+        import torch
+        with torch.cuda.stream(self.torch_stream()):
+            if self._exchange is not None:
+                self._exchange(which)
+            else:
+                halo_exchange(self.state_view(which), self.lm, self.dist)
+        self._refresh(which)
+
+    def stage(self, dt, st):
+        L.check(L.lib().dg_ssprk3_stage(self.conv._ctx, float(dt), int(st)), "dg_ssprk3_stage")
+
+    def wait(self):
+        """Wait for the context's stream; reports a watchdog error of the persistent schedule."""
+        L.check(L.lib().dg_ssprk3(self.conv._ctx, 0.0, 0), "dg_ssprk3")
+
+    def ssprk3(self, dt, nsteps=1):
+        for _ in range(nsteps):
+            for st in range(3):
+                self.exchange(st)
+                self.stage(dt, st)
+        self.wait()
+
+
+def emulated_ranks(mesh, nparts, **kw):
+    """nparts PartitionedConvection objects in one process on one GPU, exchanging ghost rows by
+    device copies; step them together with `step_emulated` (the decomposition on one GPU)."""
+    import torch
+    part = partition_elements(mesh, nparts)
+    ranks = []
+
+    def make_exchange(r):
+        def ex(which):
+            dst = ranks[r]
+            view = dst.state_view(which)
+            for q, idx in sorted(dst.lm.recv.items()):
+                src = ranks[q]
+                sidx = np.searchsorted(src.lm.owned, dst.lm.l2g[idx])
+                view.index_copy_(0, torch.as_tensor(idx, device=view.device),
+                                 src.state_view(which).index_select(0, torch.as_tensor(sidx, device=view.device)))
+        return ex
+
+    for r in range(nparts):
+        ranks.append(PartitionedConvection(mesh, part, r, exchange=make_exchange(r), **kw))
+    return ranks
+
+
+def step_emulated(ranks, dt, nsteps=1):
+    """SSP-RK3 on emulated ranks: all parts finish a stage before any exchange reads it."""
+    import torch
+    for _ in range(nsteps):
+        for st in range(3):
+            torch.cuda.synchronize()
+            for r in ranks:
+                r.exchange(st)
+            torch.cuda.synchronize()
+            for r in ranks:
+                r.stage(dt, st)
+    for r in ranks:
+        r.wait()

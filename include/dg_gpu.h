@@ -174,6 +174,21 @@ int dg_ssprk3_timed(dg_ctx* ctx, double dt, int nsteps, double* out, int nclass)
 /* The context's CUDA stream (a cudaStream_t) on which every kernel of the context runs. */
 void* dg_stream(dg_ctx* ctx);
 
+/* One mesh across several GPUs (new; the reference runs one mesh in one process). Each process
+ * creates a context on its part of the mesh, owned elements first and then ghost copies of the
+ * neighbours that other processes own, and runs SSP-RK3 one stage at a time, filling the ghost rows
+ * of the stage input from their owners in between (fve_dg_b200/partition.py).
+ * State buffer `which` on the device, packed [ncell][5*Nb]: 0 = U^n, 1 = U^(1), 2 = U^(2); stage s
+ * reads buffer s and writes buffer (s + 1) mod 3. NULL for a bad argument. */
+double* dg_state_device(dg_ctx* ctx, int which);
+/* After rows of state buffer `which` were written from outside the library (a halo exchange): the
+ * mixed form re-splits the coefficients of the n listed elements (device array of element indices)
+ * on `stream` (a cudaStream_t, 0 = the context's stream). Nothing to do in the FP64 form. */
+int dg_refresh_split(dg_ctx* ctx, int which, const int64_t* elems_dev, int64_t n, void* stream);
+/* Enqueues stage `stage` (0, 1, 2) of one SSP-RK3 step, with the limiter when configured, on the
+ * context's stream and returns; dg_ssprk3(ctx, dt, 0) waits for it and reports a watchdog error. */
+int dg_ssprk3_stage(dg_ctx* ctx, double dt, int stage);
+
 /* Explicit viscous operator, replaces ExplicitDiffusion<Order, QuadC, QuadF>::eval(mesh, U, t)
  * (include/DG/DG_Schemes/ExplicitDiffusion.h:133-626) with the context's order and rules: the
  * interior-penalty Navier-Stokes viscous residual R of U, same sign and scaling as the reference

@@ -1,0 +1,86 @@
+"""GPU: one mesh split into parts with ghost elements (fve_dg_b200/partition.py), each part its own
+context, stepped one SSP-RK3 stage at a time (dg_ssprk3_stage) with the ghost rows of every stage
+input filled from their owners by device copies in between. The owned states must equal the
+whole-mesh context's. (Parts run as separate contexts on one GPU, one after another; the NCCL
+exchange between processes is the same plan, checked on CPU over gloo.)"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from fve_dg_b200 import ExplicitConvection, box_mesh, problems
+from fve_dg_b200 import _lib as L
+from fve_dg_b200.partition import emulated_ranks, step_emulated
+
+pytestmark = pytest.mark.gpu
+
+
+def run_parts(m, U0, nparts, dt, nsteps, **kw):
+    ranks = emulated_ranks(m, nparts, **kw)
+    for r in ranks:
+        r.set_state(U0)
+    step_emulated(ranks, dt, nsteps)
+    got = np.empty_like(U0)
+    for r in ranks:
+        got[r.lm.owned] = r.get_owned()
+    return got
+
+
+def run_whole(m, U0, dt, nsteps, **kw):
+    conv = ExplicitConvection(m, **kw)
+    conv.set_state(U0)
+    conv.ssprk3(dt, nsteps)
+    return conv.get_state()
+
+
+CASES = [
+    # (mesh kwargs, nparts, convection kwargs, tolerance)
+    (dict(periodic=(1, 1, 1)), 2, dict(order=3), 0.0),
+    (dict(periodic=(1, 1, 1)), 3, dict(order=2, flux="Roe"), 0.0),
+    (dict(periodic=(1, 1, 0), bc="Pseudo3DZ"), 4, dict(order=3), 0.0),
+    (dict(periodic=(1, 1, 1)), 2, dict(order=3, precision="mixed"), 1e-13),
+    (dict(periodic=(1, 1, 1)), 3, dict(order=3, precision="mixed", schedule="persistent"), 1e-13),
+    (dict(periodic=(1, 1, 0), bc="Pseudo3DZ"), 2, dict(order=4, precision="mixed"), 1e-13),
+]
+
+
+@pytest.mark.parametrize("mk,nparts,kw,tol", CASES)
+def test_parts_equal_whole_mesh(mk, nparts, kw, tol):
+    m = box_mesh(6, jitter=0.1, seed=21, **mk)
+    U0 = problems.project(m, kw["order"], problems.density_wave(A=0.3, vel=(1.0, 0.5, 0.25)))
+    dt, nsteps = 2e-3, 4
+    want = run_whole(m, U0, dt, nsteps, **kw)
+    got = run_parts(m, U0, nparts, dt, nsteps, **kw)
+    assert np.abs(want - U0).max() > 1e-4  # the state moved
+    assert rel_l2(got, want) <= tol, rel_l2(got, want)
+
+
+def test_parts_with_limiter_equal_whole_mesh():
+    m = box_mesh(6, jitter=0.1, seed=11)
+    P = 2
+    U0 = problems.project(m, P, problems.density_wave(A=0.8, vel=(2.0, 1.0, 0.5), p=0.01))
+    kw = dict(order=P, quad_vol=1, quad_face=2, limiter="positive")
+    dt = 1e-3
+    want = run_whole(m, U0, dt, 3, **kw)
+    plain = run_whole(m, U0, dt, 3, order=P, quad_vol=1, quad_face=2)
+    assert np.abs(want - plain).max() > 1e-8  # the limiter acted
+    got = run_parts(m, U0, 3, dt, 3, **kw)
+    assert rel_l2(got, want) == 0.0, rel_l2(got, want)
+
+
+def test_stage_entry_points_validate():
+    m = box_mesh(3)
+    conv = ExplicitConvection(m, order=2)
+    lib = L.lib()
+    assert lib.dg_state_device(conv._ctx, 3) is None
+    assert lib.dg_ssprk3_stage(conv._ctx, 1e-3, 0) == -7  # no state yet
+    conv.set_state(np.zeros(conv.shape) + np.tile([1.0, 0, 0, 0, 2.5] + [0.0] * (conv.shape[1] - 5), 1))
+    assert lib.dg_ssprk3_stage(conv._ctx, 1e-3, 3) == -1
+    assert lib.dg_ssprk3_stage(conv._ctx, -1.0, 0) == -1
+    assert lib.dg_refresh_split(conv._ctx, 0, None, 5, None) == -1
+    assert lib.dg_refresh_split(conv._ctx, 0, None, 0, None) == 0
+    for which in range(3):
+        assert lib.dg_state_device(conv._ctx, which)
+    assert lib.dg_ssprk3_stage(conv._ctx, 1e-3, 0) == 0
+    assert lib.dg_ssprk3(conv._ctx, 0.0, 0) == 0

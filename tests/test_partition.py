@@ -1,0 +1,141 @@
+"""CPU: one mesh split across ranks (fve_dg_b200/partition.py): the element partition, the local meshes
+with ghost elements, the exchange plan, and SSP-RK3 on 2 gloo ranks with a halo exchange before
+every stage, checked bit for bit against the whole mesh with the oracle's residual."""
+import datetime
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from fve_dg_b200 import box_mesh, problems
+from fve_dg_b200.partition import LocalMesh, halo_exchange, partition_elements
+from oracle.pyoracle import Oracle
+
+P, QV, QF = 2, 1, 2
+
+
+def meshes():
+    return [box_mesh(4, jitter=0.1, seed=3),
+            box_mesh(4, jitter=0.1, seed=4, periodic=(1, 1, 0), bc="Pseudo3DZ")]
+
+
+def initial(m):
+    return problems.project(m, P, problems.density_wave(A=0.3, vel=(1.0, 0.5, 0.25)))
+
+
+@pytest.mark.parametrize("mi", [0, 1])
+@pytest.mark.parametrize("nparts", [2, 3, 4])
+def test_local_meshes_cover_and_agree(mi, nparts):
+    m = meshes()[mi]
+    g = m.compute_geometry()
+    part = partition_elements(m, nparts)
+    assert np.bincount(part).min() >= m.ncell // nparts
+    lms = [LocalMesh(m, part, r) for r in range(nparts)]
+    owned = np.concatenate([lm.owned for lm in lms])
+    assert np.array_equal(np.sort(owned), np.arange(m.ncell))
+    nbr = m.face_cells
+    for lm in lms:
+        assert np.all(part[lm.owned] == lm.rank) and np.all(part[lm.ghosts] != lm.rank)
+        # every ghost is a face neighbour of an owned element, and every neighbour is present
+        c0, c1 = nbr[:, 0], nbr[:, 1]
+        mine = (part[c0] == lm.rank) | ((c1 >= 0) & (part[np.maximum(c1, 0)] == lm.rank))
+        need = np.unique(np.concatenate([c0[mine], c1[mine][c1[mine] >= 0]]))
+        assert np.array_equal(np.sort(lm.l2g), need)
+        # owned elements see the whole mesh's faces and geometry (the local mesh's geometry is
+        # recomputed from its topology, so it is built the same way for the faces kept)
+        lg = lm.mesh.compute_geometry()
+        tf = lm.global_face
+        for k in ("normal", "area", "natural"):
+            assert np.array_equal(lg[k][: len(tf)], g[k][tf]), k
+        for k in ("invjac", "detj"):
+            assert np.array_equal(lg[k], g[k][lm.l2g]), k
+        # the plan: what p sends to q is exactly what q receives from p, in the same order
+        for q, idx in lm.send.items():
+            assert np.array_equal(lm.l2g[idx], lms[q].l2g[lms[q].recv[lm.rank]])
+            assert np.all(idx < lm.n_owned)
+        assert sum(len(v) for v in lm.recv.values()) == len(lm.ghosts)
+
+
+@pytest.mark.parametrize("mi", [0, 1])
+def test_owned_residual_equals_whole_mesh(mi):
+    m = meshes()[mi]
+    U = initial(m)
+    R = Oracle.from_mesh(m).residual(U, P, QV, QF)
+    part = partition_elements(m, 3)
+    for r in range(3):
+        lm = LocalMesh(m, part, r)
+        Rl = Oracle.from_mesh(lm.mesh).residual(U[lm.l2g], P, QV, QF)
+        assert np.array_equal(Rl[: lm.n_owned], R[lm.owned])
+
+
+def ssprk3(o, U, b, dt, nsteps, exchange=lambda U: None):
+    """Shu-Osher SSP-RK3 with L(U) = -R(U) / mass; `exchange` fills ghost rows of each stage input."""
+    def L(V):
+        return -o.residual(V, P, QV, QF) / b
+    for _ in range(nsteps):
+        exchange(U)
+        U1 = U + dt * L(U)
+        exchange(U1)
+        U2 = 0.75 * U + 0.25 * (U1 + dt * L(U1))
+        exchange(U2)
+        U = U / 3.0 + 2.0 / 3.0 * (U2 + dt * L(U2))
+    return U
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, mi, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        m = meshes()[mi]
+        part = partition_elements(m, world)
+        lm = LocalMesh(m, part, rank)
+        o = Oracle.from_mesh(lm.mesh)
+        b = o.mass(P, QV)
+        U0 = initial(m)
+        U = U0[lm.l2g].copy()
+        U[lm.n_owned:] = np.nan  # ghosts hold nothing until the first exchange
+
+        def exchange(V):
+            halo_exchange(torch.from_numpy(V), lm, dist)
+
+        U = ssprk3(o, U, b, 2e-3, 2, exchange)
+        q.put((rank, lm.owned, U[: lm.n_owned]))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+@pytest.mark.parametrize("mi", [0, 1])
+def test_two_rank_ssprk3_over_gloo_equals_whole_mesh(mi):
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, mi, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=150) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=30)
+        assert p.exitcode == 0
+    m = meshes()[mi]
+    o = Oracle.from_mesh(m)
+    want = ssprk3(o, initial(m), o.mass(P, QV), 2e-3, 2)
+    got = np.empty_like(want)
+    for _, owned, Uo in res:
+        got[owned] = Uo
+    assert np.array_equal(got, want)
