@@ -266,6 +266,12 @@ def main():
     ap.add_argument("--limiter", default=None, choices=["positive", "positive-avg"],
                     help="positivity-preserving limiter after every RK stage (timed as its own kernel class)")
     ap.add_argument("--n", type=int, default=0, help="override the mesh size (cubes per side), for profiling")
+    ap.add_argument("--split", action="store_true",
+                    help="one mesh split across the N ranks (element slabs with ghost elements), SSP-RK3 one "
+                         "stage at a time with the NCCL halo exchange before every stage (strong scaling)")
+    ap.add_argument("--part-of", type=int, default=0,
+                    help="(one GPU) time part 1 of a K-way split alone, ghost rows held fixed, against the "
+                         "whole mesh: the decomposition's compute overhead without the exchange")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = dict(CONFIGS[args.config])
@@ -296,6 +302,11 @@ def main():
         return
     if args.viscous:
         run_viscous(args, cfg, rank, world, local, dist)
+        if dist:
+            dist.destroy_process_group()
+        return
+    if args.split or args.part_of:
+        run_split(args, cfg, rank, world, local, dist)
         if dist:
             dist.destroy_process_group()
         return
@@ -545,6 +556,104 @@ def run_viscous(args, cfg, rank, world, local, dist):
                         "steps": k}}
         print(json.dumps(line), flush=True)
     conv.close()
+
+
+def run_split(args, cfg, rank, world, local, dist):
+    """One mesh across the ranks: rank r steps element slab r and its ghost elements, one SSP-RK3
+    stage at a time, the ghost rows of every stage input filled by the NCCL halo exchange; all of
+    it ordered on the context's stream (CUDA events there, max over ranks). With --part-of K on
+    one GPU: part 1 of K alone (its ghost rows held fixed, no exchange) and the whole mesh, to
+    measure the compute overhead of the decomposition."""
+    import torch
+    from fve_dg_b200 import ExplicitConvection, box_mesh, launch_count, problems
+    from fve_dg_b200.partition import PartitionedConvection, partition_elements
+    P, qv, qf = cfg["P"], cfg["qv"], cfg["qf"]
+    m = box_mesh(cfg["n"], hi=(cfg["L"],) * 3, jitter=cfg["jitter"])
+    U0 = problems.project(m, P, problem_fn(cfg["problem"], problems))
+    schedule = args.schedule or "two-launch"
+    kw = dict(order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf, precision=args.precision, schedule=schedule,
+              limiter=args.limiter, device=local)
+    nparts, me = (world, rank) if not args.part_of else (args.part_of, min(1, args.part_of - 1))
+    if args.part_of and world > 1:
+        raise SystemExit("--part-of runs on one GPU")
+    part = partition_elements(m, nparts)
+    if dist:
+        pc = PartitionedConvection(m, part, me, dist=dist, **kw)
+    else:
+        pc = PartitionedConvection(m, part, me, exchange=lambda which: None, **kw)
+    pc.set_state(U0)
+    lam = torch.tensor([pc.conv.max_wave_speed()], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(lam, op=dist.ReduceOp.MAX)
+    dt = problems.cfl_dt(CFL, cfg["L"] / cfg["n"], P, float(lam.item()))
+    nb = pc.conv.num_basis
+    stream = torch.cuda.ExternalStream(pc.conv.stream)
+
+    def timed(run, k):
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = launch_count()
+        e0.record(stream)
+        run(k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_, n_ = e0.elapsed_time(e1), launch_count() - l0
+        if dist:
+            t = torch.tensor([ms_], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_ = float(t.item())
+        return ms_, n_
+
+    def steps(k):
+        for _ in range(k):
+            for st in range(3):
+                pc.exchange(st)
+                pc.stage(dt, st)
+
+    steps(args.warmup)
+    ms, launches = timed(steps, args.steps)
+    pc.wait()
+    owned_dof = 5 * nb * pc.lm.n_owned * 3
+    halo = {"parts": nparts, "owned": pc.lm.n_owned, "ghosts": int(len(pc.lm.ghosts)),
+            "faces": pc.lm.mesh.nface, "recv_bytes_per_stage": int(len(pc.lm.ghosts)) * 5 * nb * 8,
+            "neighbours": sorted(int(q) for q in pc.lm.recv)}
+    if args.part_of:
+        whole = ExplicitConvection(m, **kw)
+        whole.set_state(U0)
+        whole.ssprk3(dt, args.warmup, graph=True)
+        wstream = torch.cuda.ExternalStream(whole.stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(wstream)
+        whole.ssprk3(dt, args.steps, graph=True)
+        e1.record(wstream)
+        torch.cuda.synchronize()
+        ms_whole = e0.elapsed_time(e1)
+        whole.close()
+        value = owned_dof * args.steps / (ms / 1e3)
+        whole_value = 5 * nb * m.ncell * 3 * args.steps / (ms_whole / 1e3)
+        halo.update({"whole_mesh_value": whole_value, "whole_ms_per_step": ms_whole / args.steps,
+                     "part_times_parts_over_whole": value * nparts / whole_value,
+                     "note": "part 1 alone on one GPU, ghost rows held fixed (no exchange), eager stages; the "
+                             "whole mesh with one CUDA graph per step"})
+        scaling, parallelism = "strong", f"part 1 of a {nparts}-way element split, alone on one GPU"
+    else:
+        value = 5 * nb * m.ncell * 3 * args.steps / (ms / 1e3)
+        scaling, parallelism = "strong", f"one mesh split into {world} element slabs, NCCL halo exchange per stage"
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "DOF-stage/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": scaling, "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "bf16x3 contractions, f32 flux, f64 state",
+                "data": "synthetic",
+                "config": {"workload": args.config + "-split", "desc": cfg["desc"], "precision": args.precision,
+                           "schedule": schedule, "limiter": args.limiter, "tets": m.ncell, "order": P, "dt": dt,
+                           "l2": "state larger than L2 (no flush needed)", "parallelism": parallelism},
+                "gpu_launches": launches, "halo": halo, "e2e": None}
+        print(json.dumps(line), flush=True)
+    pc.conv.close()
 
 
 def run_ensemble(args, rank, world, local, dist):

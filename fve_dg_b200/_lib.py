@@ -33,6 +33,7 @@ class MeshDesc(ctypes.Structure):
         ("cell_invjac", c_double_p), ("cell_detj", c_double_p),
         ("npts", ctypes.c_int64), ("points", c_double_p), ("cell_nodes", c_int64_p),
         ("face_nodes", c_int64_p), ("face_nodes1", c_int64_p), ("face_periodic", c_uint8_p),
+        ("nghost", ctypes.c_int64),
     ]
 
 

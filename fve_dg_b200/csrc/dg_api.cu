@@ -97,6 +97,7 @@ struct dg_ctx {
     int sms = 148;
     // ensembles: instance element offsets, per-instance dt on the device, instance of each element
     int ninst = 1;
+    int64_t nowned = 0;  // cells [nowned, ncell) are ghosts (dg_mesh_desc.nghost)
     std::vector<int64_t> inst_off;
     double* d_dt_inst = nullptr;
     int* d_elem_inst = nullptr;
@@ -226,7 +227,7 @@ StageArgs stage_args(dg_ctx* c, const double* U, const double* U0, double* out, 
     a.dphi_vw = c->d_dphi_vw;
     a.phi_f = c->d_phi_f;
     a.mass_ref = c->d_mass_ref;
-    a.ncell = (int)c->ncell;
+    a.ncell = (int)c->nowned;  // ghosts get no residual
     a.nqv = c->tab.nqv;
     a.nqf = c->tab.nqf;
     a.gamma = c->cfg.gamma;
@@ -279,7 +280,7 @@ int limit_stage(dg_ctx* c, const double* in, double* out, uint32_t* mir, cudaStr
     if (!c->cfg.limiter) return DG_OK;
     g_launches += 2;
     return timed(c, 4, s, [&] {
-        return launch_limiter(c->cfg.order, c->qv, out, in, c->d_fi, c->d_ef, c->d_phi_v, c->ncell, c->nface,
+        return launch_limiter(c->cfg.order, c->qv, out, in, c->d_fi, c->d_ef, c->d_phi_v, c->ncell, c->nowned,
                               c->cfg.gamma, c->cfg.limiter == 2, c->d_lim_bnd, mir, c->sms, s);
     });
 }
@@ -424,6 +425,7 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
     c->cfg.quad_vol = qv;
     c->cfg.quad_face = qf;
     c->ncell = mesh->ncell;
+    c->nowned = mesh->ncell - mesh->nghost;
     c->nface = mesh->nface;
     if (cudaSetDevice(cfg->device) != cudaSuccess) return fail(c, DG_E_CUDA);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(c, DG_E_CUDA);
@@ -457,7 +459,7 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
     std::vector<double> hh(c->ncell);
     for (int64_t e = 0; e < c->ncell; ++e) {
         double area = 0.0;
-        for (int q = 0; q < 4; ++q) area += geo.area[hef[4 * e + q].face];
+        for (int q = 0; q < fill[e]; ++q) area += geo.area[hef[4 * e + q].face];
         hh[e] = geo.detj[e] / 6.0 / area;
     }
     const size_t nstate = (size_t)c->ncell * 5 * nb;
@@ -483,7 +485,7 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
         if ((rc = upload(&c->d_elem_inst, inst)) || (rc = upload(&c->d_dt_inst, dts))) return fail(c, rc);
     }
     if (cfg->precision == DG_PREC_MIXED) {
-        rc = init_mixed(c->mixed, c->tab, hgeo, hfi, hef, c->ncell, c->nface, cfg->gamma, cfg->flux, qv, qf,
+        rc = init_mixed(c->mixed, c->tab, hgeo, hfi, hef, c->ncell, c->nowned, c->nface, cfg->gamma, cfg->flux, qv, qf,
                         c->d_geo, c->d_fi, c->d_ef, c->d_mass_ref);
         if (rc) return fail(c, rc);
         c->mixed.dt_inst = c->d_dt_inst;
@@ -521,7 +523,7 @@ dg_ctx* dg_create_ensemble(const dg_mesh_desc* meshes, int ninst, const dg_confi
     for (int i = 0; i < ninst; ++i) {
         const dg_mesh_desc& d = meshes[i];
         const bool gi = d.face_natural != nullptr;
-        if (gi != given || !d.face_cells || (!gi && (!d.points || !d.cell_nodes || !d.face_nodes))) {
+        if (gi != given || !d.face_cells || (!gi && (!d.points || !d.cell_nodes || !d.face_nodes)) || d.nghost != 0) {
             if (err) *err = DG_E_ARG;
             return nullptr;
         }
@@ -681,7 +683,7 @@ int dg_viscous_residual_device(dg_ctx* c, const double* U, double* R, double mu,
     a.U = U; a.R = R; a.geo = c->d_geo; a.h = c->d_h; a.fi = c->d_fi; a.ef = c->d_ef;
     a.phi_v = c->d_phi_v; a.dphi_v = c->d_dphi_v; a.w_v = c->d_w_v;
     a.phi_f = c->d_phi_f; a.dphi_f = c->d_dphi_f; a.w_f = c->d_w_f; a.UD = c->d_UD;
-    a.ncell = c->ncell; a.nqv = c->tab.nqv; a.nqf = c->tab.nqf; a.order = c->cfg.order;
+    a.ncell = c->nowned; a.nqv = c->tab.nqv; a.nqf = c->tab.nqf; a.order = c->cfg.order;
     a.mu = mu; a.cq = c->cfg.gamma / prandtl;
     ++g_launches;
     return launch_viscous(c->cfg.order, a, (cudaStream_t)stream);
@@ -707,7 +709,7 @@ int dg_limit_device(dg_ctx* c, double* U, const double* Uprev, int only_avg, voi
     int rc;
     if (!c->d_lim_bnd && (rc = dev_alloc(&c->d_lim_bnd, (size_t)c->ncell * 10))) return rc;
     g_launches += 2;
-    return launch_limiter(c->cfg.order, c->qv, U, Uprev, c->d_fi, c->d_ef, c->d_phi_v, c->ncell, c->nface,
+    return launch_limiter(c->cfg.order, c->qv, U, Uprev, c->d_fi, c->d_ef, c->d_phi_v, c->ncell, c->nowned,
                           c->cfg.gamma, only_avg != 0, c->d_lim_bnd, nullptr, c->sms, (cudaStream_t)stream);
 }
 
@@ -1028,7 +1030,7 @@ int dg_conservation(dg_ctx* c, double out[6]) {
     if (!c || !out) return DG_E_ARG;
     if (!c->have_state) return DG_E_STATE;
     DG_CUDA(cudaSetDevice(c->cfg.device));
-    return reduce_conservation(c->d_Un, c->d_geo, c->d_phi_v, c->d_w_v, (int)c->ncell, c->tab.nb, c->tab.nqv,
+    return reduce_conservation(c->d_Un, c->d_geo, c->d_phi_v, c->d_w_v, (int)c->nowned, c->tab.nb, c->tab.nqv,
                                c->d_red, out, c->stream, &g_launches);
 }
 
@@ -1036,7 +1038,7 @@ int dg_max_wave_speed(dg_ctx* c, double* lam) {
     if (!c || !lam) return DG_E_ARG;
     if (!c->have_state) return DG_E_STATE;
     DG_CUDA(cudaSetDevice(c->cfg.device));
-    return reduce_wave_speed(c->d_Un, c->d_phi_v, (int)c->ncell, c->tab.nb, c->tab.nqv, c->cfg.gamma, c->d_red,
+    return reduce_wave_speed(c->d_Un, c->d_phi_v, (int)c->nowned, c->tab.nb, c->tab.nqv, c->cfg.gamma, c->d_red,
                              lam, c->stream, &g_launches);
 }
 
@@ -1045,7 +1047,7 @@ int dg_check_state(dg_ctx* c, int64_t* bad) {
     if (!c->have_state) return DG_E_STATE;
     DG_CUDA(cudaSetDevice(c->cfg.device));
     double nbad = 0;
-    int rc = reduce_bad_points(c->d_Un, c->d_phi_v, (int)c->ncell, c->tab.nb, c->tab.nqv, c->cfg.gamma, c->d_red,
+    int rc = reduce_bad_points(c->d_Un, c->d_phi_v, (int)c->nowned, c->tab.nb, c->tab.nqv, c->cfg.gamma, c->d_red,
                                &nbad, c->stream, &g_launches);
     if (rc) return rc;
     if (bad) *bad = (int64_t)nbad;

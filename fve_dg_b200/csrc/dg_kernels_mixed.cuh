@@ -869,7 +869,7 @@ inline void build_groups(const std::vector<FaceInfo>& hfi, const std::vector<Ele
 
 inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>& hgeo,
                       const std::vector<FaceInfo>& hfi, const std::vector<ElemFace>& hef, int64_t ncell,
-                      int64_t nface, double gamma, int flux, int qv, int qf, const double* d_geo,
+                      int64_t nowned, int64_t nface, double gamma, int flux, int qv, int qf, const double* d_geo,
                       const FaceInfo* d_fi, const ElemFace*, const double*) {
     if (!mixed_supported(tab.order, qv, qf)) return DG_E_ARG;
     const int NB = tab.nb, NQV = tab.nqv, NQF = tab.nqf;
@@ -919,7 +919,7 @@ inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>
         return rc;
     std::vector<FaceGroup> fg;
     std::vector<ElemGroup> eg;
-    build_groups(hfi, hef, ncell, fg, eg);
+    build_groups(hfi, hef, nowned, fg, eg);  // element groups over owned cells only (no ghosts)
     m.nfgroups = (int)fg.size();
     m.negroups = (int)eg.size();
     if ((rc = mixed_upload(m, &m.fgroups, fg)) || (rc = mixed_upload(m, &m.egroups, eg))) return rc;

@@ -276,15 +276,16 @@ inline bool limiter_supported(int order, int qv) {
     return false;
 }
 
-// Bounds from Uprev, then the three steps on U (in place). stats: [ncell][10] scratch.
+// Bounds from Uprev, then the three steps on U (in place) for cells [0, napply) (the owned cells;
+// the statistics cover ghost cells too). stats: [ncell][10] scratch.
 inline int launch_limiter(int order, int qv, double* U, const double* Uprev, const FaceInfo* fi, const ElemFace* ef,
-                          const double* phi_v, int64_t ncell, int64_t /*nface*/, double gamma, int only_avg,
+                          const double* phi_v, int64_t ncell, int64_t napply, double gamma, int only_avg,
                           double* stats, uint32_t* mir, int sms, cudaStream_t s) {
 #define X(P, QV, NB, NQV)                                                                                        \
     if (order == P && qv == QV) {                                                                                \
         const unsigned ge = (unsigned)std::min<int64_t>((ncell + kLimWarps - 1) / kLimWarps, (int64_t)sms * 16); \
         limiter_cell_stats<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(Uprev, phi_v, ncell, only_avg, stats);         \
-        limiter_apply<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(U, ef, fi, stats, phi_v, ncell, gamma, mir);       \
+        limiter_apply<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(U, ef, fi, stats, phi_v, napply, gamma, mir);      \
         return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;                                            \
     }
     FVEDG_LIMITER_COMBOS(X)

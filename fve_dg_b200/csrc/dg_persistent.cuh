@@ -126,7 +126,7 @@ inline int build_schedule(MixedData& m, QueueSchedule& qs, const PersistentParam
     if (ne < 1 || nf < 1) return DG_E_ARG;
     const int R = std::max(1, std::min({pp.regions, kMaxRegions, ne}));
     const int tf = std::max(1, pp.tile_f), te = std::max(1, pp.tile_e), lag = std::max(0, pp.lag);
-    std::vector<int> ereg(m.ncell, 0), greg(ne);
+    std::vector<int> ereg(m.ncell, R), greg(ne);  // ghost cells (in no element group) stay at R
     for (int g = 0; g < ne; ++g) {
         greg[g] = (int)((int64_t)g * R / ne);
         for (int i = 0; i < m.heg[g].n; ++i) ereg[m.heg[g].e[i]] = greg[g];
@@ -140,7 +140,7 @@ inline int build_schedule(MixedData& m, QueueSchedule& qs, const PersistentParam
             r = std::min(r, ereg[m.hface_cells[2 * f]]);
             if (m.hface_cells[2 * f + 1] >= 0) r = std::min(r, ereg[m.hface_cells[2 * f + 1]]);
         }
-        freg[g] = r;
+        freg[g] = std::min(r, R - 1);
     }
     std::vector<int> order(nf);
     for (int g = 0; g < nf; ++g) order[g] = g;

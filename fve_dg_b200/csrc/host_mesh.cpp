@@ -121,7 +121,10 @@ int build_geometry(const dg_mesh_desc* d, Geometry* g) {
     g->perm.assign(2 * nf, -1);
     g->invjac.assign(9 * nc, 0.0);
     g->detj.assign(nc, 0.0);
-    // face -> cell incidence must be consistent: every cell has exactly four face slots
+    // face -> cell incidence must be consistent: every cell has exactly four face slots (a ghost
+    // cell, one of the last nghost, only those it shares with owned cells: one to four)
+    if (d->nghost < 0 || d->nghost >= nc) return DG_E_ARG;
+    const int64_t nowned = nc - d->nghost;
     std::vector<int> deg(nc, 0);
     for (int64_t f = 0; f < nf; ++f) {
         const int64_t c0 = d->face_cells[2 * f], c1 = d->face_cells[2 * f + 1];
@@ -131,7 +134,7 @@ int build_geometry(const dg_mesh_desc* d, Geometry* g) {
         if (c1 != DG_NO_CELL) ++deg[c1];
     }
     for (int64_t c = 0; c < nc; ++c)
-        if (deg[c] != 4) return DG_E_MESH;
+        if (c < nowned ? deg[c] != 4 : (deg[c] < 1 || deg[c] > 4)) return DG_E_MESH;
 
     if (given) {
         std::memcpy(g->normal.data(), d->face_normal, sizeof(double) * 3 * nf);

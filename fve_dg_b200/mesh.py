@@ -15,7 +15,7 @@ class Mesh:
     """Raw topology (form (b) of dg_mesh_desc), optionally with reference-held geometry (form (a))."""
 
     def __init__(self, points, cells, faces, face_cells, face_nodes1=None, periodic=None, bc=None,
-                 cell_faces=None, cell_cells=None, geometry=None):
+                 cell_faces=None, cell_cells=None, geometry=None, nghost=0):
         self.points = L.as_f64(points).reshape(-1, 3)
         self.cells = L.as_i64(cells).reshape(-1, 4)
         self.faces = L.as_i64(faces).reshape(-1, 3)
@@ -26,6 +26,7 @@ class Mesh:
         self.cell_faces = None if cell_faces is None else L.as_i64(cell_faces).reshape(-1, 4)
         self.cell_cells = None if cell_cells is None else L.as_i64(cell_cells).reshape(-1, 4)
         self.geometry = geometry  # dict(natural, normal, area, invjac, detj) or None
+        self.nghost = int(nghost)  # the last nghost cells are ghost copies (dg_mesh_desc.nghost)
 
     @property
     def ncell(self):
@@ -51,6 +52,7 @@ class Mesh:
         d.face_nodes = L.iptr(self.faces)
         d.face_nodes1 = L.iptr(self.face_nodes1)
         d.face_periodic = L.u8ptr(self.periodic)
+        d.nghost = self.nghost
         return d
 
     def compute_geometry(self):

@@ -3,11 +3,11 @@ halo exchange of coefficient blocks.
 
 Each rank owns a contiguous range of the mesh's elements (on the box meshes, slabs). Its local mesh
 holds the owned elements first, then the ghost elements: the face neighbours of owned elements
-that another rank owns. The local faces are every face that touches an owned element, with its
-cells renumbered and its orientation unchanged, so an owned element sees exactly the faces,
-normals and face maps it has in the whole mesh. A ghost's other faces become boundary faces of a
-type that contributes nothing. Its own residual is therefore wrong, but a ghost's state is
-overwritten by its owner's before every stage, and only ghost values are ever read.
+that another rank owns. The local faces are the faces that touch an owned element, with their
+cells renumbered and their orientation unchanged, so an owned element sees exactly the faces,
+normals and face maps it has in the whole mesh. A ghost keeps only the faces it shares with owned
+elements (the mesh's `nghost` marks the ghosts: the library computes no residual, limiting or
+reduction for them), and its state is overwritten by its owner's before every stage.
 
 Before each RK stage the stage input's ghost entries are refreshed: every rank sends, to each
 neighbouring rank, the coefficient blocks of its owned elements that are ghosts there, and
@@ -20,9 +20,7 @@ import ctypes
 import numpy as np
 
 from . import _lib as L
-from .mesh import BC, Mesh
-
-INACTIVE_BC = BC["Neumann"]  # a boundary type the operator treats as contributing nothing
+from .mesh import Mesh
 
 
 def partition_elements(mesh, nparts):
@@ -50,30 +48,16 @@ class LocalMesh:
         self.l2g = np.concatenate([owned, ghosts])
         g2l = np.full(mesh.ncell, -1, dtype=np.int64)
         g2l[self.l2g] = np.arange(len(self.l2g))
-        # faces touching owned elements keep their orientation and order
+        # the faces touching owned elements, with their orientation and order; a ghost keeps only
+        # these (the mesh's last nghost cells need not be closed)
         tf = np.flatnonzero(touch)
-        faces = [mesh.faces[tf]]
-        fcs = [np.stack([g2l[c0[tf]], np.where(c1[tf] >= 0, g2l[c1s[tf]], -1)], axis=1)]
-        fn1 = [mesh.face_nodes1[tf] if mesh.face_nodes1 is not None else mesh.faces[tf]]
-        per = [mesh.periodic[tf] if mesh.periodic is not None else np.zeros(len(tf), np.uint8)]
-        bcs = [mesh.bc[tf] if mesh.bc is not None else np.full(len(tf), BC["Pseudo3DZ"], np.uint8)]
-        # the ghosts' remaining faces, as inactive boundary faces of the ghost
-        is_ghost = np.zeros(mesh.ncell, dtype=bool)
-        is_ghost[ghosts] = True
-        rest = np.flatnonzero(~touch)
-        for side, cells in ((0, c0), (1, c1)):
-            sel = rest[(cells[rest] >= 0) & is_ghost[np.maximum(cells[rest], 0)]]
-            if not len(sel):
-                continue
-            nodes = mesh.faces[sel] if (side == 0 or mesh.face_nodes1 is None) else mesh.face_nodes1[sel]
-            faces.append(nodes)
-            fcs.append(np.stack([g2l[cells[sel]], np.full(len(sel), -1)], axis=1))
-            fn1.append(nodes)
-            per.append(np.zeros(len(sel), np.uint8))
-            bcs.append(np.full(len(sel), INACTIVE_BC, np.uint8))
-        self.mesh = Mesh(mesh.points, mesh.cells[self.l2g], np.concatenate(faces), np.concatenate(fcs),
-                         np.concatenate(fn1), np.concatenate(per), np.concatenate(bcs))
-        self.global_face = tf  # local face i < len(tf) is global face tf[i]
+        fn1 = mesh.face_nodes1[tf] if mesh.face_nodes1 is not None else None
+        per = mesh.periodic[tf] if mesh.periodic is not None else None
+        bcs = mesh.bc[tf] if mesh.bc is not None else None
+        fcs = np.stack([g2l[c0[tf]], np.where(c1[tf] >= 0, g2l[c1s[tf]], -1)], axis=1)
+        self.mesh = Mesh(mesh.points, mesh.cells[self.l2g], mesh.faces[tf], fcs, fn1, per, bcs,
+                         nghost=len(ghosts))
+        self.global_face = tf  # local face i is global face tf[i]
         # exchange plan: what this rank sends to / receives from every other rank, by global id
         ghost_owner = part[ghosts]
         self.recv = {int(q): g2l[ghosts[ghost_owner == q]] for q in np.unique(ghost_owner)}

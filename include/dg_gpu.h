@@ -91,6 +91,13 @@ typedef struct dg_mesh_desc {
     const int64_t* face_nodes;   /* [nface][3] (face node order defines the face parameters)   */
     const int64_t* face_nodes1;  /* [nface][3] the face's nodes as numbered in cells[1]; NULL = face_nodes */
     const uint8_t* face_periodic;/* [nface] 1 = periodic pair (normal by the boundary rule); NULL = none */
+    /* Ghost elements (one mesh split across processes, fve_dg_b200/partition.py): the last nghost
+     * cells are copies of elements that another process owns. A ghost needs only the faces it
+     * shares with owned cells (1 to 4); the context holds its state and computes the fluxes of those
+     * faces but no residual, limiting, viscous term or reduction for it: residual rows of ghosts are
+     * left unwritten and dg_conservation / dg_max_wave_speed / dg_check_state cover owned cells.
+     * 0 for an ordinary mesh (zero-initialise the struct). */
+    int64_t nghost;
 } dg_mesh_desc;
 
 typedef struct dg_config {

@@ -56,6 +56,19 @@ def test_parts_equal_whole_mesh(mk, nparts, kw, tol):
     assert rel_l2(got, want) <= tol, rel_l2(got, want)
 
 
+@pytest.mark.parametrize("precision,tol", [("fp64", 0.0), ("mixed", 1e-13)])
+def test_owned_residual_equals_whole_mesh(precision, tol):
+    from fve_dg_b200.partition import LocalMesh, partition_elements
+    m = box_mesh(6, jitter=0.1, seed=22)
+    U = problems.project(m, 3, problems.density_wave(A=0.3, vel=(1.0, 0.5, 0.25)))
+    want = ExplicitConvection(m, order=3, precision=precision).eval(U)
+    part = partition_elements(m, 3)
+    for r in range(3):
+        lm = LocalMesh(m, part, r)
+        got = ExplicitConvection(lm.mesh, order=3, precision=precision).eval(U[lm.l2g])[: lm.n_owned]
+        assert rel_l2(got, want[lm.owned]) <= tol
+
+
 def test_parts_with_limiter_equal_whole_mesh():
     m = box_mesh(6, jitter=0.1, seed=11)
     P = 2

@@ -60,6 +60,19 @@ def test_local_meshes_cover_and_agree(mi, nparts):
         assert sum(len(v) for v in lm.recv.values()) == len(lm.ghosts)
 
 
+def test_ghost_count_is_validated():
+    m = meshes()[0]
+    lm = LocalMesh(m, partition_elements(m, 2), 0)
+    lm.mesh.compute_geometry()  # ghosts with fewer than four faces are accepted
+    assert lm.mesh.nghost == len(lm.ghosts) and np.bincount(lm.mesh.face_cells[lm.mesh.face_cells >= 0],
+                                                            minlength=lm.ncell)[lm.n_owned:].min() < 4
+    for bad, code in ((len(lm.ghosts) - 1, "DG_E_MESH"), (-1, "DG_E_ARG"), (lm.ncell, "DG_E_ARG")):
+        lm.mesh.nghost = bad  # an owned cell without four faces, or a count out of range
+        with pytest.raises(Exception, match=code):
+            lm.mesh.compute_geometry()
+    lm.mesh.nghost = len(lm.ghosts)
+
+
 @pytest.mark.parametrize("mi", [0, 1])
 def test_owned_residual_equals_whole_mesh(mi):
     m = meshes()[mi]
