@@ -90,10 +90,19 @@ struct dg_ctx {
     // limiter: per-cell statistics [ncell][10] and a staging buffer for host calls
     double* d_lim_bnd = nullptr;
     double* d_lim_prev = nullptr;
+    double* d_lim_stats[3] = {nullptr, nullptr, nullptr};  // limiter statistics of state buffer 0, 1, 2
+    int* d_lim_nbr = nullptr;                              // [ncell][4] face neighbours (self across a boundary)
+    bool lim_valid = false;                                // d_lim_stats[0] describes U^n's owned cells
     // viscous operator: reference gradients at the volume and face points, cell size h
     double* d_dphi_v = nullptr;
     double* d_dphi_f = nullptr;
     double* d_h = nullptr;
+    // viscous operator, allocated by its first call: transposed basis tables, per-face-point fluxes
+    double* d_visc_phiT_v = nullptr;
+    double* d_visc_dphiT_v = nullptr;
+    double* d_visc_phiT_f = nullptr;
+    double* d_visc_dphiT_f = nullptr;
+    double* d_visc_vf = nullptr;
     int sms = 148;
     // ensembles: instance element offsets, per-instance dt on the device, instance of each element
     int ninst = 1;
@@ -274,15 +283,31 @@ int timed(dg_ctx* c, int cls, cudaStream_t s, F&& fn) {
 
 // One SSP-RK3 step (Shu-Osher) on the device state, FP64 form:
 //   U1 = U + dt L(U);  U2 = 3/4 U + 1/4 (U1 + dt L(U1));  U = 1/3 U + 2/3 (U2 + dt L(U2)).
-// Limiter after a stage (dg_config.limiter): bounds from the stage input, the output limited in
-// place; mir = the output's split rows in the mixed form (refreshed where the limiter acted).
-int limit_stage(dg_ctx* c, const double* in, double* out, uint32_t* mir, cudaStream_t s) {
+// Limiter after stage st (dg_config.limiter): bounds from the stage input's statistics, the output
+// limited in place and its statistics written for the next stage; mir = the output's split rows in
+// the mixed form (refreshed where the limiter acted). The input's statistics come from the previous
+// stage's launch, except after the state was set from outside (computed here at stage 0) and for
+// ghost cells (computed here every stage: a halo exchange rewrote their rows).
+int limit_stage(dg_ctx* c, int st, const double* in, double* out, uint32_t* mir, cudaStream_t s) {
     if (!c->cfg.limiter) return DG_OK;
-    g_launches += 2;
-    return timed(c, 4, s, [&] {
-        return launch_limiter(c->cfg.order, c->qv, out, in, c->d_fi, c->d_ef, c->d_phi_v, c->ncell, c->nowned,
-                              c->cfg.gamma, c->cfg.limiter == 2, c->d_lim_bnd, mir, c->sms, s);
+    const int64_t stats_begin = (st == 0 && !c->lim_valid) ? 0 : c->nowned;
+    const int rc = timed(c, 4, s, [&] {
+        return launch_limiter_stage(c->cfg.order, c->qv, out, in, c->d_lim_nbr, c->d_phi_v, c->ncell, c->nowned,
+                                    stats_begin, c->cfg.gamma, c->cfg.limiter == 2, c->d_lim_stats[st],
+                                    c->d_lim_stats[(st + 1) % 3], mir, c->sms, s, &g_launches);
     });
+    if (rc == DG_OK && st != 1) c->lim_valid = true;  // stage 0 made them valid, stage 2 rewrote them
+    return rc;
+}
+
+// Before a CUDA graph of whole steps is captured or replayed: the statistics of U^n, so that the
+// graph never needs the full statistics pass.
+int ensure_limiter_stats(dg_ctx* c, cudaStream_t s) {
+    if (!c->cfg.limiter || c->lim_valid) return DG_OK;
+    const int rc = launch_limiter_stats(c->cfg.order, c->qv, c->d_Un, c->d_phi_v, 0, c->ncell, c->cfg.limiter == 2,
+                                        c->d_lim_stats[0], c->sms, s, &g_launches);
+    if (rc == DG_OK) c->lim_valid = true;
+    return rc;
 }
 
 int step_fp64(dg_ctx* c, double dt, cudaStream_t s, int st0, int st1) {
@@ -297,7 +322,7 @@ int step_fp64(dg_ctx* c, double dt, cudaStream_t s, int st0, int st1) {
             return dispatch_element(c->cfg.order, c->qv, c->qf, stage_args(c, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 1), s);
         });
         if (rc) return rc;
-        if ((rc = limit_stage(c, in[st], out[st], nullptr, s))) return rc;
+        if ((rc = limit_stage(c, st, in[st], out[st], nullptr, s))) return rc;
     }
     return DG_OK;
 }
@@ -307,7 +332,10 @@ int step(dg_ctx* c, double dt, cudaStream_t s, int st0 = 0, int st1 = 3) {
     if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
     auto tm = [&](int cls, auto&& fn) { return timed(c, cls, s, fn); };
     if (c->cfg.precision == DG_PREC_MIXED) {
-        auto post = [&](const double* in, double* out, int mir) { return limit_stage(c, in, out, c->mixed.mir[mir], s); };
+        // post(in, out, mir_out) after stage st, whose output mirror is mir_out = (st + 1) % 3
+        auto post = [&](const double* in, double* out, int mir) {
+            return limit_stage(c, (mir + 2) % 3, in, out, c->mixed.mir[mir], s);
+        };
         if (c->cfg.schedule == 1)
             return step_persistent(c->mixed, c->d_queue, c->qs, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches,
                                    tm, post, st0, st1);
@@ -317,7 +345,7 @@ int step(dg_ctx* c, double dt, cudaStream_t s, int st0 = 0, int st1 = 3) {
 }
 
 int launches_per_step(const dg_ctx* c) {
-    const int lim = c->cfg.limiter ? 6 : 0;
+    const int lim = c->cfg.limiter ? (c->nowned < c->ncell ? 6 : 3) : 0;
     if (c->cfg.precision == DG_PREC_MIXED) return (c->cfg.schedule == 1 ? 3 : mixed_launches_per_step(c->mixed)) + lim;
     return 6 + lim;
 }
@@ -363,9 +391,14 @@ void free_ctx(dg_ctx* c) {
     if (c->d_queue) cudaFree(c->d_queue);
     if (c->d_dt_inst) cudaFree(c->d_dt_inst);
     if (c->d_lim_bnd) cudaFree(c->d_lim_bnd);
+    for (double* p : c->d_lim_stats)
+        if (p) cudaFree(p);
+    if (c->d_lim_nbr) cudaFree(c->d_lim_nbr);
     if (c->d_dphi_v) cudaFree(c->d_dphi_v);
     if (c->d_dphi_f) cudaFree(c->d_dphi_f);
     if (c->d_h) cudaFree(c->d_h);
+    for (double* p : {c->d_visc_phiT_v, c->d_visc_dphiT_v, c->d_visc_phiT_f, c->d_visc_dphiT_f, c->d_visc_vf})
+        if (p) cudaFree(p);
     if (c->d_lim_prev) cudaFree(c->d_lim_prev);
     if (c->d_elem_inst) cudaFree(c->d_elem_inst);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -500,7 +533,24 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
             c->sms = sms;
     }
     // the limiter's per-cell statistics, allocated here so that no step allocates (graph capture)
-    if (cfg->limiter && (rc = dev_alloc(&c->d_lim_bnd, (size_t)c->ncell * 10))) return fail(c, rc);
+    if (cfg->limiter) {
+        for (double*& p : c->d_lim_stats)
+            if ((rc = dev_alloc(&p, (size_t)c->ncell * 10))) return fail(c, rc);
+    }
+    {  // the limiter's neighbour table: the cell across each face, the cell itself on a boundary
+        std::vector<int> nbr(4 * c->ncell);
+        for (int64_t e = 0; e < c->ncell; ++e)
+            for (int q = 0; q < 4; ++q) {
+                int o = (int)e;
+                if (q < fill[e]) {
+                    const FaceInfo& F = hfi[hef[4 * e + q].face];
+                    o = F.c0 == (int)e ? F.c1 : F.c0;
+                    if (o < 0) o = (int)e;
+                }
+                nbr[4 * e + q] = o;
+            }
+        if ((rc = upload(&c->d_lim_nbr, nbr))) return fail(c, rc);
+    }
     if (err) *err = DG_OK;
     return c;
 }
@@ -675,18 +725,50 @@ int dg_residual(dg_ctx* c, const double* U, double* R, size_t stride, double t, 
     return cuda_ok(cudaStreamSynchronize(c->stream));
 }
 
+// The viscous operator's tables transposed so that lanes over points read rows, and its
+// per-face-point buffer; made by the first call on the context.
+int viscous_buffers(dg_ctx* c) {
+    if (c->d_visc_vf) return DG_OK;
+    const Tables& t = c->tab;
+    const int nb = t.nb, nqv = t.nqv, nqf = t.nqf;
+    std::vector<double> pv((size_t)nb * nqv), dpv((size_t)nb * 3 * nqv), pf((size_t)24 * nb * nqf),
+        dpf((size_t)24 * nb * 3 * nqf);
+    for (int g = 0; g < nqv; ++g)
+        for (int b = 0; b < nb; ++b) {
+            pv[(size_t)b * nqv + g] = t.phi_v[(size_t)g * nb + b];
+            for (int d = 0; d < 3; ++d) dpv[((size_t)b * 3 + d) * nqv + g] = t.dphi_v[((size_t)g * nb + b) * 3 + d];
+        }
+    for (int p = 0; p < 24; ++p)
+        for (int g = 0; g < nqf; ++g)
+            for (int b = 0; b < nb; ++b) {
+                pf[((size_t)p * nb + b) * nqf + g] = t.phi_f[((size_t)p * nqf + g) * nb + b];
+                for (int d = 0; d < 3; ++d)
+                    dpf[(((size_t)p * nb + b) * 3 + d) * nqf + g] = t.dphi_f[(((size_t)p * nqf + g) * nb + b) * 3 + d];
+            }
+    int rc;
+    if ((rc = upload(&c->d_visc_phiT_v, pv)) || (rc = upload(&c->d_visc_dphiT_v, dpv)) ||
+        (rc = upload(&c->d_visc_phiT_f, pf)) || (rc = upload(&c->d_visc_dphiT_f, dpf)) ||
+        (rc = dev_alloc(&c->d_visc_vf, (size_t)c->nface * 6 * nqf)))
+        return rc;
+    return DG_OK;
+}
+
 int dg_viscous_residual_device(dg_ctx* c, const double* U, double* R, double mu, double prandtl, void* stream) {
     if (!c || !U || !R || !(mu >= 0.0) || !(prandtl > 0.0)) return DG_E_ARG;
     if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
     DG_CUDA(cudaSetDevice(c->cfg.device));
+    int rc = viscous_buffers(c);
+    if (rc) return rc;
     ViscArgs a;
     a.U = U; a.R = R; a.geo = c->d_geo; a.h = c->d_h; a.fi = c->d_fi; a.ef = c->d_ef;
     a.phi_v = c->d_phi_v; a.dphi_v = c->d_dphi_v; a.w_v = c->d_w_v;
     a.phi_f = c->d_phi_f; a.dphi_f = c->d_dphi_f; a.w_f = c->d_w_f; a.UD = c->d_UD;
-    a.ncell = c->nowned; a.nqv = c->tab.nqv; a.nqf = c->tab.nqf; a.order = c->cfg.order;
+    a.phiT_v = c->d_visc_phiT_v; a.dphiT_v = c->d_visc_dphiT_v;
+    a.phiT_f = c->d_visc_phiT_f; a.dphiT_f = c->d_visc_dphiT_f; a.vf = c->d_visc_vf;
+    a.ncell = c->nowned; a.nface = c->nface; a.nqv = c->tab.nqv; a.nqf = c->tab.nqf; a.order = c->cfg.order;
     a.mu = mu; a.cq = c->cfg.gamma / prandtl;
-    ++g_launches;
-    return launch_viscous(c->cfg.order, a, (cudaStream_t)stream);
+    g_launches += 2;
+    return launch_viscous(c->cfg.order, a, c->sms, (cudaStream_t)stream);
 }
 
 int dg_viscous_residual(dg_ctx* c, const double* U, double* R, size_t stride, double mu, double prandtl) {
@@ -709,7 +791,7 @@ int dg_limit_device(dg_ctx* c, double* U, const double* Uprev, int only_avg, voi
     int rc;
     if (!c->d_lim_bnd && (rc = dev_alloc(&c->d_lim_bnd, (size_t)c->ncell * 10))) return rc;
     g_launches += 2;
-    return launch_limiter(c->cfg.order, c->qv, U, Uprev, c->d_fi, c->d_ef, c->d_phi_v, c->ncell, c->nowned,
+    return launch_limiter(c->cfg.order, c->qv, U, Uprev, c->d_lim_nbr, c->d_phi_v, c->ncell, c->nowned,
                           c->cfg.gamma, only_avg != 0, c->d_lim_bnd, nullptr, c->sms, (cudaStream_t)stream);
 }
 
@@ -730,6 +812,7 @@ int dg_limit(dg_ctx* c, double* U, const double* Uprev, size_t stride, int only_
 int dg_set_state(dg_ctx* c, const double* U, size_t stride) {
     if (!c || !U) return DG_E_ARG;
     DG_CUDA(cudaSetDevice(c->cfg.device));
+    c->lim_valid = false;
     int rc = copy_in(c, c->d_Un, U, stride, c->stream);
     if (rc) return rc;
     // the mixed form reads U^n's split deviation coefficients from a mirror the steps keep current
@@ -764,6 +847,7 @@ int dg_ssprk3_graph(dg_ctx* c, double dt, int nsteps) {
     if (!c || nsteps < 0 || !(dt >= 0)) return DG_E_ARG;
     if (!c->have_state) return DG_E_STATE;
     DG_CUDA(cudaSetDevice(c->cfg.device));
+    if (const int lrc = ensure_limiter_stats(c, c->stream)) return lrc;
     if (!c->graph || c->graph_dt != dt) {
         if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
         cudaGraph_t g = nullptr;
@@ -899,6 +983,7 @@ int dg_autotune(dg_ctx* c, double dt, char* report, size_t len) {
           ", \"ms_per_step\": " + std::to_string(best) + "}}";
     cudaMemcpyAsync(c->d_Un, save, nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
     mixed_mirror(c->mixed, c->d_Un, 0, c->stream, &g_launches);
+    c->lim_valid = false;
     cudaStreamSynchronize(c->stream);
     cudaFree(save);
     cudaEventDestroy(e0);

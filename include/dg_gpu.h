@@ -193,7 +193,8 @@ double* dg_state_device(dg_ctx* ctx, int which);
  * on `stream` (a cudaStream_t, 0 = the context's stream). Nothing to do in the FP64 form. */
 int dg_refresh_split(dg_ctx* ctx, int which, const int64_t* elems_dev, int64_t n, void* stream);
 /* Enqueues stage `stage` (0, 1, 2) of one SSP-RK3 step, with the limiter when configured, on the
- * context's stream and returns; dg_ssprk3(ctx, dt, 0) waits for it and reports a watchdog error. */
+ * context's stream and returns; dg_ssprk3(ctx, dt, 0) waits for it and reports a watchdog error.
+ * Run the stages of a step in order 0, 1, 2; between them, write only ghost rows from outside. */
 int dg_ssprk3_stage(dg_ctx* ctx, double dt, int stage);
 
 /* Explicit viscous operator, replaces ExplicitDiffusion<Order, QuadC, QuadF>::eval(mesh, U, t)
@@ -203,7 +204,9 @@ int dg_ssprk3_stage(dg_ctx* ctx, double dt, int stage);
  * fixes mu = 1 and Pr = 1; here they are arguments (gamma is the context's). Dirichlet faces use the
  * data of dg_set_dirichlet. Host buffers with the element stride of dg_residual. */
 int dg_viscous_residual(dg_ctx* ctx, const double* U, double* R, size_t elem_stride_bytes, double mu, double prandtl);
-/* Same on device buffers, enqueued on `stream` (a cudaStream_t, 0 = default). */
+/* Same on device buffers, enqueued on `stream` (a cudaStream_t, 0 = default). The first call on a
+ * context allocates the operator's per-face buffer (nface * 6 * nqf doubles) and its tables; calls
+ * on one context share that buffer, so calls whose kernels could overlap must be serialised. */
 int dg_viscous_residual_device(dg_ctx* ctx, const double* U_dev, double* R_dev, double mu, double prandtl,
                                void* stream);
 
