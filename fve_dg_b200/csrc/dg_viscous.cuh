@@ -25,8 +25,16 @@
 //   H_n[4]   = sum_a u_a H_n[1+a] + mu gamma/Pr (Ye_n - sum_k u_k Y_k,n),   H_n[0] = 0
 // with u = U_1..3 / U_0, e = U_4 / U_0 and rho = max(U_0, 1e-8), as ExplicitDiffusion.h:28-31,69-73.
 //
-// One thread per element owns that element's residual: the volume term and its share of each of
-// its four faces (the neighbour's trace is recomputed), so no atomics and a deterministic result.
+// Two launches, FP64:
+//   viscous_face     one warp per face, lanes over the face points: both traces (values and physical
+//                    gradients) once per face, the averaged flux with its penalty and the symmetric
+//                    term's scalar; stored per point as Fl w 2A (5 values) and sfac w 2A.
+//   viscous_element  one warp per element: the volume term (lanes over the volume points: J^T H w detJ
+//                    per point; then lanes over the outputs (mode j, variable i) contract it with the
+//                    reference gradients), then the element's four faces gathered with its side's basis
+//                    values, plus the energy-only symmetric term n . (grad phi_j^L + grad phi_j^R),
+//                    written as (J_L^T n) . dphi^L + (J_R^T n) . dphi^R. Each element writes its own
+//                    residual: no atomics, a deterministic result.
 #pragma once
 #include "dg_kernels_fp64.cuh"
 
@@ -46,10 +54,19 @@ struct ViscArgs {
     const double* dphi_f;   // [24][nqf][nb][3]
     const double* w_f;      // [nqf]
     const double* UD;       // [nface][nqf][5] Dirichlet data, or null
-    int64_t ncell;
+    const double* phiT_v;   // [nb][nqv] the volume tables transposed (lanes over points read rows)
+    const double* dphiT_v;  // [nb][3][nqv]
+    const double* phiT_f;   // [24][nb][nqf]
+    const double* dphiT_f;  // [24][nb][3][nqf]
+    double* vf;             // [nface][6][nqf] per face point: Fl w 2A (5), sfac w 2A
+    int64_t ncell, nface;
     int nqv, nqf, order;
     double mu, cq;          // viscosity and gamma / Pr
 };
+
+constexpr int kViscWarps = 4;
+constexpr int kViscMaxQv = 64;  // volume points an element warp stages (the largest rule has 57)
+constexpr int kViscMaxQf = 32;  // face points, one per lane (the largest rule has 24)
 
 struct ViscState {  // what K needs of the state it is taken at
     double u[3], e, irho;
@@ -93,147 +110,248 @@ __device__ __forceinline__ void visc_contract(const ViscState& s, double mu, dou
     out[4] = o4;
 }
 
-// Value and physical gradient of the state at a point: Uv[k], G[k][m].
+// Value and physical gradient of the state at point g from transposed tables (phiT [nb][nq],
+// dphiT [nb][3][nq]): Uv[k], G[k][m] = sum_d J[m][d] (sum_b c_bk dphi_bd).
 template <int NB>
-__device__ __forceinline__ void visc_trace(const double* c, const double* phi, const double* dphi, const double J[9],
-                                           double Uv[5], double G[5][3]) {
+__device__ __forceinline__ void visc_trace_t(const double* c, const double* __restrict__ phiT,
+                                             const double* __restrict__ dphiT, int nq, int g, const double J[9],
+                                             double Uv[5], double G[5][3]) {
+    double R[5][3];
     #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        Uv[k] = 0.0;
-        G[k][0] = G[k][1] = G[k][2] = 0.0;
-    }
+    for (int k = 0; k < 5; ++k) { Uv[k] = 0.0; R[k][0] = R[k][1] = R[k][2] = 0.0; }
+    #pragma unroll 2
     for (int b = 0; b < NB; ++b) {
-        const double gr[3] = {J[0] * dphi[3 * b] + J[1] * dphi[3 * b + 1] + J[2] * dphi[3 * b + 2],
-                              J[3] * dphi[3 * b] + J[4] * dphi[3 * b + 1] + J[5] * dphi[3 * b + 2],
-                              J[6] * dphi[3 * b] + J[7] * dphi[3 * b + 1] + J[8] * dphi[3 * b + 2]};
+        const double p = phiT[b * nq + g];
+        const double d0 = dphiT[(3 * b) * nq + g], d1 = dphiT[(3 * b + 1) * nq + g], d2 = dphiT[(3 * b + 2) * nq + g];
         #pragma unroll
         for (int k = 0; k < 5; ++k) {
             const double cb = c[5 * b + k];
-            Uv[k] += phi[b] * cb;
-            G[k][0] += gr[0] * cb;
-            G[k][1] += gr[1] * cb;
-            G[k][2] += gr[2] * cb;
+            Uv[k] = fma(p, cb, Uv[k]);
+            R[k][0] = fma(d0, cb, R[k][0]);
+            R[k][1] = fma(d1, cb, R[k][1]);
+            R[k][2] = fma(d2, cb, R[k][2]);
         }
     }
+    #pragma unroll
+    for (int k = 0; k < 5; ++k)
+        #pragma unroll
+        for (int m = 0; m < 3; ++m) G[k][m] = J[3 * m] * R[k][0] + J[3 * m + 1] * R[k][1] + J[3 * m + 2] * R[k][2];
 }
 
-__device__ __forceinline__ double grad_phi_dot(const double J[9], const double* dphi_b, const double d[3]) {
-    const double g0 = J[0] * dphi_b[0] + J[1] * dphi_b[1] + J[2] * dphi_b[2];
-    const double g1 = J[3] * dphi_b[0] + J[4] * dphi_b[1] + J[5] * dphi_b[2];
-    const double g2 = J[6] * dphi_b[0] + J[7] * dphi_b[1] + J[8] * dphi_b[2];
-    return g0 * d[0] + g1 * d[1] + g2 * d[2];
+// Faces whose viscous terms act: interior, Dirichlet with data, Pseudo3DZ (ExplicitDiffusion.h:380-612).
+__device__ __forceinline__ bool visc_face_active(const FaceInfo& F, const double* UD) {
+    const int bc = (F.meta >> 16) & 0xff;
+    return F.c1 >= 0 || bc == 5 || (bc == 0 && UD != nullptr);
 }
 
 template <int NB>
-__global__ void __launch_bounds__(128) viscous_residual(ViscArgs a) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= a.ncell) return;
-    double acc[5 * NB];
-    for (int i = 0; i < 5 * NB; ++i) acc[i] = 0.0;
-    double J[9];
-    for (int i = 0; i < 9; ++i) J[i] = a.geo[e * 10 + i];
-    const double detj = a.geo[e * 10 + 9];
-    const double* c = a.U + e * (5 * NB);
-    // volume term
-    for (int g = 0; g < a.nqv; ++g) {
-        double Uv[5], G[5][3];
-        visc_trace<NB>(c, a.phi_v + g * NB, a.dphi_v + g * NB * 3, J, Uv, G);
-        const ViscState st = visc_state(Uv);
-        double H[3][5];  // H_n for unit directions n
-        #pragma unroll
-        for (int n = 0; n < 3; ++n) {
-            const double d[3] = {n == 0 ? 1.0 : 0.0, n == 1 ? 1.0 : 0.0, n == 2 ? 1.0 : 0.0};
-            visc_contract(st, a.mu, a.cq, G, d, H[n]);
-        }
-        const double wj = a.w_v[g] * detj;
-        for (int j = 0; j < NB; ++j) {
-            const double* dp = a.dphi_v + (g * NB + j) * 3;
-            const double gj[3] = {J[0] * dp[0] + J[1] * dp[1] + J[2] * dp[2], J[3] * dp[0] + J[4] * dp[1] + J[5] * dp[2],
-                                  J[6] * dp[0] + J[7] * dp[1] + J[8] * dp[2]};
-            #pragma unroll
-            for (int i = 0; i < 5; ++i) acc[5 * j + i] -= (gj[0] * H[0][i] + gj[1] * H[1][i] + gj[2] * H[2][i]) * wj;
-        }
-    }
-    // faces
+__global__ void __launch_bounds__(kViscWarps * 32) viscous_face(ViscArgs a) {
+    __shared__ double sc[kViscWarps][2][5 * NB];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double* cL = sc[w][0];
+    double* cR = sc[w][1];
+    const int nqf = a.nqf;
     const double beta_base = (double)((a.order + 1) * (a.order + 1));
-    for (int q = 0; q < 4; ++q) {
-        const ElemFace E = a.ef[4 * e + q];
-        const FaceInfo F = a.fi[E.face];
-        const int side = E.meta >> 8;
-        const int bc = (F.meta >> 16) & 0xff;
+    for (int64_t f = (int64_t)blockIdx.x * kViscWarps + w; f < a.nface; f += (int64_t)gridDim.x * kViscWarps) {
+        const FaceInfo F = a.fi[f];
+        if (!visc_face_active(F, a.UD)) continue;  // warp-uniform
         const bool interior = F.c1 >= 0;
-        if (!interior && bc != 0 && bc != 5) continue;
-        if (!interior && bc == 0 && !a.UD) continue;
-        const double n[3] = {F.n[0], F.n[1], F.n[2]};
-        const double beta = beta_base / a.h[F.c0];
-        const int pL = F.meta & 0xff, pR = (F.meta >> 8) & 0xff;
-        double JL[9], JR[9];
-        for (int i = 0; i < 9; ++i) JL[i] = a.geo[(int64_t)F.c0 * 10 + i];
-        if (interior)
-            for (int i = 0; i < 9; ++i) JR[i] = a.geo[(int64_t)F.c1 * 10 + i];
-        const double* cL = a.U + (int64_t)F.c0 * (5 * NB);
-        const double* cR = interior ? a.U + (int64_t)F.c1 * (5 * NB) : cL;
-        for (int g = 0; g < a.nqf; ++g) {
-            const double jw = a.w_f[g] * F.jw;
-            const double* phL = a.phi_f + ((int64_t)pL * a.nqf + g) * NB;
-            const double* dpL = a.dphi_f + ((int64_t)pL * a.nqf + g) * NB * 3;
-            double UL[5], GL[5][3], UR[5], GR[5][3];
-            visc_trace<NB>(cL, phL, dpL, JL, UL, GL);
-            const double* phR = nullptr;
-            const double* dpR = nullptr;
+        const int bc = (F.meta >> 16) & 0xff;
+        const double* gL = a.U + (int64_t)F.c0 * (5 * NB);
+        for (int i = lane; i < 5 * NB; i += 32) cL[i] = gL[i];
+        if (interior) {
+            const double* gR = a.U + (int64_t)F.c1 * (5 * NB);
+            for (int i = lane; i < 5 * NB; i += 32) cR[i] = gR[i];
+        }
+        __syncwarp();
+        if (lane < nqf) {
+            const int g = lane;
+            const int pL = F.meta & 0xff, pR = (F.meta >> 8) & 0xff;
+            const double n[3] = {F.n[0], F.n[1], F.n[2]};
+            double J[9];
+            #pragma unroll
+            for (int i = 0; i < 9; ++i) J[i] = a.geo[(int64_t)F.c0 * 10 + i];
+            double UL[5], UR[5], X[5][3];
+            visc_trace_t<NB>(cL, a.phiT_f + (int64_t)pL * NB * nqf, a.dphiT_f + (int64_t)pL * NB * 3 * nqf, nqf, g, J,
+                             UL, X);
             if (interior) {
-                phR = a.phi_f + ((int64_t)pR * a.nqf + g) * NB;
-                dpR = a.dphi_f + ((int64_t)pR * a.nqf + g) * NB * 3;
-                visc_trace<NB>(cR, phR, dpR, JR, UR, GR);
+                #pragma unroll
+                for (int i = 0; i < 9; ++i) J[i] = a.geo[(int64_t)F.c1 * 10 + i];
+                double GR[5][3];
+                visc_trace_t<NB>(cR, a.phiT_f + (int64_t)pR * NB * nqf, a.dphiT_f + (int64_t)pR * NB * 3 * nqf, nqf,
+                                 g, J, UR, GR);
+                #pragma unroll
+                for (int k = 0; k < 5; ++k)
+                    #pragma unroll
+                    for (int m = 0; m < 3; ++m) X[k][m] = 0.5 * (X[k][m] + GR[k][m]);
             } else if (bc == 0) {
-                const double* ud = a.UD + ((int64_t)E.face * a.nqf + g) * 5;
-                for (int k = 0; k < 5; ++k) UR[k] = ud[k] + (ud[k] - UL[k]);  // ghost
+                const double* ud = a.UD + (f * nqf + g) * 5;
+                #pragma unroll
+                for (int k = 0; k < 5; ++k) UR[k] = ud[k] + (ud[k] - UL[k]);  // ghost 2 U_D - U
             } else {
+                #pragma unroll
                 for (int k = 0; k < 5; ++k) UR[k] = UL[k];
                 UR[3] = -UL[3];
             }
             double Um[5];
+            #pragma unroll
             for (int k = 0; k < 5; ++k) Um[k] = 0.5 * (UL[k] + UR[k]);
             const ViscState st = visc_state(Um);
-            // averaged flux and penalty
-            double X[5][3], Fa[5], Fb[5];
-            for (int k = 0; k < 5; ++k)
-                for (int m = 0; m < 3; ++m) X[k][m] = interior ? 0.5 * (GL[k][m] + GR[k][m]) : GL[k][m];
-            visc_contract(st, a.mu, a.cq, X, n, Fa);
+            double Fa[5], Fb[5];
+            visc_contract(st, a.mu, a.cq, X, n, Fa);  // averaged (boundary: inner) gradient flux
+            #pragma unroll
             for (int k = 0; k < 5; ++k) {
                 const double dU = interior ? UL[k] - UR[k] : UL[k];
+                #pragma unroll
                 for (int m = 0; m < 3; ++m) X[k][m] = dU * n[m];
             }
-            visc_contract(st, a.mu, a.cq, X, n, Fb);
-            double Fl[5];
-            for (int k = 0; k < 5; ++k) Fl[k] = Fa[k] - beta * Fb[k];
-            // symmetric term, energy equation only
-            const double sfac = (interior ? 0.5 : 1.0) * a.mu * a.cq * st.irho * (UR[4] - UL[4]);
-            const double sgn = side == 0 ? 1.0 : -1.0;
-            const double* phS = side == 0 ? phL : phR;
-            for (int j = 0; j < NB; ++j) {
-                double sj = grad_phi_dot(JL, dpL + 3 * j, n);
-                if (interior) sj += grad_phi_dot(JR, dpR + 3 * j, n);
-                const double pj = phS[j];
-                #pragma unroll
-                for (int i = 0; i < 5; ++i) acc[5 * j + i] += sgn * pj * Fl[i] * jw;
-                acc[5 * j + 4] += sgn * sfac * sj * jw;
-            }
+            visc_contract(st, a.mu, a.cq, X, n, Fb);  // penalty
+            const double beta = beta_base / a.h[F.c0];
+            const double jw = a.w_f[g] * F.jw;
+            double* out = a.vf + f * 6 * nqf;
+            #pragma unroll
+            for (int k = 0; k < 5; ++k) out[k * nqf + g] = (Fa[k] - beta * Fb[k]) * jw;
+            out[5 * nqf + g] = (interior ? 0.5 : 1.0) * a.mu * a.cq * st.irho * (UR[4] - UL[4]) * jw;
         }
+        __syncwarp();
     }
-    double* r = a.R + e * (5 * NB);
-    for (int i = 0; i < 5 * NB; ++i) r[i] = acc[i];
 }
 
-inline int launch_viscous(int order, const ViscArgs& a, cudaStream_t s) {
-    const unsigned g = (unsigned)((a.ncell + 127) / 128);
+template <int NB>
+__global__ void __launch_bounds__(kViscWarps * 32) viscous_element(ViscArgs a) {
+    constexpr int NO = 5 * NB, OPL = (NO + 31) / 32;  // outputs (mode, variable) per lane
+    __shared__ double sc[kViscWarps][5 * NB];
+    __shared__ double sh[kViscWarps][kViscMaxQv * 15];  // per volume point: (J^T H)[d][i] w detJ
+    __shared__ double sv[kViscWarps][6 * kViscMaxQf];   // the face block
+    __shared__ double st_[kViscWarps][NB];              // symmetric term per mode
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nqv = a.nqv, nqf = a.nqf;
+    double* c = sc[w];
+    double* hs = sh[w];
+    double* vb = sv[w];
+    double* ts = st_[w];
+    for (int64_t e = (int64_t)blockIdx.x * kViscWarps + w; e < a.ncell; e += (int64_t)gridDim.x * kViscWarps) {
+        const double* ge = a.U + e * (5 * NB);
+        for (int i = lane; i < 5 * NB; i += 32) c[i] = ge[i];
+        double J[9];
+        #pragma unroll
+        for (int i = 0; i < 9; ++i) J[i] = a.geo[e * 10 + i];
+        const double detj = a.geo[e * 10 + 9];
+        __syncwarp();
+        // volume term: per point the flux H_n (n = x, y, z) pulled back to reference directions
+        for (int g = lane; g < nqv; g += 32) {
+            double Uv[5], G[5][3];
+            visc_trace_t<NB>(c, a.phiT_v, a.dphiT_v, nqv, g, J, Uv, G);
+            const ViscState s = visc_state(Uv);
+            double H[3][5];
+            #pragma unroll
+            for (int n = 0; n < 3; ++n) {
+                const double d[3] = {n == 0 ? 1.0 : 0.0, n == 1 ? 1.0 : 0.0, n == 2 ? 1.0 : 0.0};
+                visc_contract(s, a.mu, a.cq, G, d, H[n]);
+            }
+            const double wj = a.w_v[g] * detj;
+            #pragma unroll
+            for (int d = 0; d < 3; ++d)
+                #pragma unroll
+                for (int i = 0; i < 5; ++i)
+                    hs[g * 15 + d * 5 + i] = (J[d] * H[0][i] + J[3 + d] * H[1][i] + J[6 + d] * H[2][i]) * wj;
+        }
+        __syncwarp();
+        double acc[OPL];
+        #pragma unroll
+        for (int r = 0; r < OPL; ++r) {
+            acc[r] = 0.0;
+            const int o = lane + 32 * r;
+            if (o < NO) {
+                const int j = o / 5, i = o - 5 * (o / 5);
+                double v = 0.0;
+                for (int g = 0; g < nqv; ++g) {
+                    const double* dp = a.dphi_v + ((int64_t)g * NB + j) * 3;
+                    const double* hg = hs + g * 15 + i;
+                    v = fma(dp[0], hg[0], v);
+                    v = fma(dp[1], hg[5], v);
+                    v = fma(dp[2], hg[10], v);
+                }
+                acc[r] = -v;
+            }
+        }
+        // the element's faces
+        for (int q = 0; q < 4; ++q) {
+            const ElemFace E = a.ef[4 * e + q];
+            const FaceInfo F = a.fi[E.face];
+            if (!visc_face_active(F, a.UD)) continue;  // warp-uniform
+            const bool interior = F.c1 >= 0;
+            __syncwarp();
+            const double* src = a.vf + (int64_t)E.face * 6 * nqf;
+            for (int i = lane; i < 6 * nqf; i += 32) vb[i] = src[i];
+            // symmetric term T_j = sum_g sfac_g ((J_L^T n) . dphi_j^L(g) + (J_R^T n) . dphi_j^R(g))
+            double nL[3], nR[3] = {0.0, 0.0, 0.0};
+            {
+                const double* JL = a.geo + (int64_t)F.c0 * 10;
+                #pragma unroll
+                for (int d = 0; d < 3; ++d) nL[d] = JL[d] * F.n[0] + JL[3 + d] * F.n[1] + JL[6 + d] * F.n[2];
+                if (interior) {
+                    const double* JR = a.geo + (int64_t)F.c1 * 10;
+                    #pragma unroll
+                    for (int d = 0; d < 3; ++d) nR[d] = JR[d] * F.n[0] + JR[3 + d] * F.n[1] + JR[6 + d] * F.n[2];
+                }
+            }
+            __syncwarp();
+            const int pL = F.meta & 0xff, pR = (F.meta >> 8) & 0xff;
+            for (int j = lane; j < NB; j += 32) {
+                double t = 0.0;
+                for (int g = 0; g < nqf; ++g) {
+                    const double* dl = a.dphi_f + (((int64_t)pL * nqf + g) * NB + j) * 3;
+                    double sj = nL[0] * dl[0] + nL[1] * dl[1] + nL[2] * dl[2];
+                    if (interior) {
+                        const double* dr = a.dphi_f + (((int64_t)pR * nqf + g) * NB + j) * 3;
+                        sj += nR[0] * dr[0] + nR[1] * dr[1] + nR[2] * dr[2];
+                    }
+                    t = fma(vb[5 * nqf + g], sj, t);
+                }
+                ts[j] = t;
+            }
+            __syncwarp();
+            const double sgn = (E.meta >> 8) == 0 ? 1.0 : -1.0;
+            const double* ph = a.phi_f + (int64_t)(E.meta & 0xff) * nqf * NB;  // this side's basis values
+            #pragma unroll
+            for (int r = 0; r < OPL; ++r) {
+                const int o = lane + 32 * r;
+                if (o < NO) {
+                    const int j = o / 5, i = o - 5 * (o / 5);
+                    double v = 0.0;
+                    for (int g = 0; g < nqf; ++g) v = fma(ph[g * NB + j], vb[i * nqf + g], v);
+                    if (i == 4) v += ts[j];
+                    acc[r] += sgn * v;
+                }
+            }
+        }
+        double* out = a.R + e * (5 * NB);
+        #pragma unroll
+        for (int r = 0; r < OPL; ++r) {
+            const int o = lane + 32 * r;
+            if (o < NO) out[o] = acc[r];
+        }
+        __syncwarp();
+    }
+}
+
+inline int launch_viscous(int order, const ViscArgs& a, int sms, cudaStream_t s) {
+    if (a.nqv > kViscMaxQv || a.nqf > kViscMaxQf) return DG_E_ARG;
+    const unsigned gf = (unsigned)std::min<int64_t>((a.nface + kViscWarps - 1) / kViscWarps, (int64_t)sms * 32);
+    const unsigned ge = (unsigned)std::min<int64_t>((a.ncell + kViscWarps - 1) / kViscWarps, (int64_t)sms * 32);
+#define VISC_LAUNCH(NB)                                                 \
+    viscous_face<NB><<<gf, kViscWarps * 32, 0, s>>>(a);                 \
+    viscous_element<NB><<<ge, kViscWarps * 32, 0, s>>>(a);              \
+    break;
     switch (order) {
-        case 1: viscous_residual<4><<<g, 128, 0, s>>>(a); break;
-        case 2: viscous_residual<10><<<g, 128, 0, s>>>(a); break;
-        case 3: viscous_residual<20><<<g, 128, 0, s>>>(a); break;
-        case 4: viscous_residual<35><<<g, 128, 0, s>>>(a); break;
+        case 1: VISC_LAUNCH(4)
+        case 2: VISC_LAUNCH(10)
+        case 3: VISC_LAUNCH(20)
+        case 4: VISC_LAUNCH(35)
         default: return DG_E_ARG;
     }
+#undef VISC_LAUNCH
     return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;
 }
 
