@@ -102,6 +102,8 @@ struct dg_ctx {
     double* d_visc_dphiT_v = nullptr;
     double* d_visc_phiT_f = nullptr;
     double* d_visc_dphiT_f = nullptr;
+    double* d_visc_Av = nullptr;
+    double* d_visc_Pf = nullptr;
     double* d_visc_vf = nullptr;
     int sms = 148;
     // ensembles: instance element offsets, per-instance dt on the device, instance of each element
@@ -397,7 +399,8 @@ void free_ctx(dg_ctx* c) {
     if (c->d_dphi_v) cudaFree(c->d_dphi_v);
     if (c->d_dphi_f) cudaFree(c->d_dphi_f);
     if (c->d_h) cudaFree(c->d_h);
-    for (double* p : {c->d_visc_phiT_v, c->d_visc_dphiT_v, c->d_visc_phiT_f, c->d_visc_dphiT_f, c->d_visc_vf})
+    for (double* p : {c->d_visc_phiT_v, c->d_visc_dphiT_v, c->d_visc_phiT_f, c->d_visc_dphiT_f, c->d_visc_Av,
+                      c->d_visc_Pf, c->d_visc_vf})
         if (p) cudaFree(p);
     if (c->d_lim_prev) cudaFree(c->d_lim_prev);
     if (c->d_elem_inst) cudaFree(c->d_elem_inst);
@@ -745,10 +748,20 @@ int viscous_buffers(dg_ctx* c) {
                 for (int d = 0; d < 3; ++d)
                     dpf[(((size_t)p * nb + b) * 3 + d) * nqf + g] = t.dphi_f[(((size_t)p * nqf + g) * nb + b) * 3 + d];
             }
+    // A operands of the tensor-core contractions, rows padded to 4 and modes to 8 (zeros)
+    const int mp = visc_mp(nb), kpv = visc_kp(3 * nqv), kpf = visc_kp(nqf);
+    std::vector<double> av((size_t)kpv * mp, 0.0), apf((size_t)24 * kpf * mp, 0.0);
+    for (int k = 0; k < 3 * nqv; ++k)
+        for (int j = 0; j < nb; ++j) av[(size_t)k * mp + j] = t.dphi_v[((size_t)(k / 3) * nb + j) * 3 + k % 3];
+    for (int p = 0; p < 24; ++p)
+        for (int g = 0; g < nqf; ++g)
+            for (int j = 0; j < nb; ++j)
+                apf[((size_t)p * kpf + g) * mp + j] = t.phi_f[((size_t)p * nqf + g) * nb + j];
     int rc;
     if ((rc = upload(&c->d_visc_phiT_v, pv)) || (rc = upload(&c->d_visc_dphiT_v, dpv)) ||
         (rc = upload(&c->d_visc_phiT_f, pf)) || (rc = upload(&c->d_visc_dphiT_f, dpf)) ||
-        (rc = dev_alloc(&c->d_visc_vf, (size_t)c->nface * 6 * nqf)))
+        (rc = upload(&c->d_visc_Av, av)) || (rc = upload(&c->d_visc_Pf, apf)) ||
+        (rc = dev_alloc(&c->d_visc_vf, (size_t)c->nface * (5 * nqf + nb))))
         return rc;
     return DG_OK;
 }
@@ -765,6 +778,8 @@ int dg_viscous_residual_device(dg_ctx* c, const double* U, double* R, double mu,
     a.phi_f = c->d_phi_f; a.dphi_f = c->d_dphi_f; a.w_f = c->d_w_f; a.UD = c->d_UD;
     a.phiT_v = c->d_visc_phiT_v; a.dphiT_v = c->d_visc_dphiT_v;
     a.phiT_f = c->d_visc_phiT_f; a.dphiT_f = c->d_visc_dphiT_f; a.vf = c->d_visc_vf;
+    a.Av = c->d_visc_Av; a.Pf = c->d_visc_Pf;
+    a.mp = visc_mp(c->tab.nb); a.kpv = visc_kp(3 * c->tab.nqv); a.kpf = visc_kp(c->tab.nqf);
     a.ncell = c->nowned; a.nface = c->nface; a.nqv = c->tab.nqv; a.nqf = c->tab.nqf; a.order = c->cfg.order;
     a.mu = mu; a.cq = c->cfg.gamma / prandtl;
     g_launches += 2;

@@ -27,14 +27,16 @@
 //
 // Two launches, FP64:
 //   viscous_face     one warp per face, lanes over the face points: both traces (values and physical
-//                    gradients) once per face, the averaged flux with its penalty and the symmetric
-//                    term's scalar; stored per point as Fl w 2A (5 values) and sfac w 2A.
+//                    gradients) once per face, the averaged flux with its penalty (stored per point as
+//                    Fl w 2A), and the energy-only symmetric term per mode,
+//                    T_j = sum_g sfac_g w_g 2A n . (grad phi_j^L + grad phi_j^R), written as
+//                    (J_L^T n) . dphi^L + (J_R^T n) . dphi^R (the same for both sides, up to sign).
 //   viscous_element  one warp per element: the volume term (lanes over the volume points: J^T H w detJ
-//                    per point; then lanes over the outputs (mode j, variable i) contract it with the
-//                    reference gradients), then the element's four faces gathered with its side's basis
-//                    values, plus the energy-only symmetric term n . (grad phi_j^L + grad phi_j^R),
-//                    written as (J_L^T n) . dphi^L + (J_R^T n) . dphi^R. Each element writes its own
-//                    residual: no atomics, a deterministic result.
+//                    per point), then the contractions on the FP64 tensor cores (mma m8n8k4, modes x
+//                    variables): the volume term with the reference gradients over (point, direction),
+//                    and each of the four faces' fluxes with its side's basis values over the face
+//                    points; plus T_j in the energy column. Each element writes its own residual: no
+//                    atomics, a deterministic result.
 #pragma once
 #include "dg_kernels_fp64.cuh"
 
@@ -58,15 +60,28 @@ struct ViscArgs {
     const double* dphiT_v;  // [nb][3][nqv]
     const double* phiT_f;   // [24][nb][nqf]
     const double* dphiT_f;  // [24][nb][3][nqf]
-    double* vf;             // [nface][6][nqf] per face point: Fl w 2A (5), sfac w 2A
+    const double* Av;       // [kpv][mp] A of the volume contraction: dphi_v[k/3][j][k%3], zero-padded
+    const double* Pf;       // [24][kpf][mp] A of the face contraction: phi_f[p][g][j], zero-padded
+    double* vf;             // [nface][5 nqf + nb] per face: Fl w 2A [5][nqf], then T_j [nb]
     int64_t ncell, nface;
-    int nqv, nqf, order;
+    int nqv, nqf, order, kpv, kpf, mp;
     double mu, cq;          // viscosity and gamma / Pr
 };
 
 constexpr int kViscWarps = 4;
 constexpr int kViscMaxQv = 64;  // volume points an element warp stages (the largest rule has 57)
 constexpr int kViscMaxQf = 32;  // face points, one per lane (the largest rule has 24)
+
+inline int visc_mp(int nb) { return 8 * ((nb + 7) / 8); }  // modes padded to the 8-row tiles
+inline int visc_kp(int k) { return 4 * ((k + 3) / 4); }     // contraction length padded to 4
+
+// d (one 8 x 8 FP64 tile of D, two entries per lane) += A (8 x 4) B (4 x 8); lane l holds
+// A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void visc_dmma(double d[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
 
 struct ViscState {  // what K needs of the state it is taken at
     double u[3], e, irho;
@@ -147,10 +162,12 @@ __device__ __forceinline__ bool visc_face_active(const FaceInfo& F, const double
 template <int NB>
 __global__ void __launch_bounds__(kViscWarps * 32) viscous_face(ViscArgs a) {
     __shared__ double sc[kViscWarps][2][5 * NB];
+    __shared__ double ssf[kViscWarps][kViscMaxQf];  // sfac w 2A per face point
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double* cL = sc[w][0];
     double* cR = sc[w][1];
-    const int nqf = a.nqf;
+    double* ss = ssf[w];
+    const int nqf = a.nqf, bs = 5 * nqf + NB;
     const double beta_base = (double)((a.order + 1) * (a.order + 1));
     for (int64_t f = (int64_t)blockIdx.x * kViscWarps + w; f < a.nface; f += (int64_t)gridDim.x * kViscWarps) {
         const FaceInfo F = a.fi[f];
@@ -208,10 +225,37 @@ __global__ void __launch_bounds__(kViscWarps * 32) viscous_face(ViscArgs a) {
             visc_contract(st, a.mu, a.cq, X, n, Fb);  // penalty
             const double beta = beta_base / a.h[F.c0];
             const double jw = a.w_f[g] * F.jw;
-            double* out = a.vf + f * 6 * nqf;
+            double* out = a.vf + f * bs;
             #pragma unroll
             for (int k = 0; k < 5; ++k) out[k * nqf + g] = (Fa[k] - beta * Fb[k]) * jw;
-            out[5 * nqf + g] = (interior ? 0.5 : 1.0) * a.mu * a.cq * st.irho * (UR[4] - UL[4]) * jw;
+            ss[g] = (interior ? 0.5 : 1.0) * a.mu * a.cq * st.irho * (UR[4] - UL[4]) * jw;
+        }
+        __syncwarp();
+        // symmetric term per mode: T_j = sum_g ss_g ((J_L^T n) . dphi_j^L(g) + (J_R^T n) . dphi_j^R(g))
+        double nL[3], nR[3] = {0.0, 0.0, 0.0};
+        {
+            const double* JL = a.geo + (int64_t)F.c0 * 10;
+            #pragma unroll
+            for (int d = 0; d < 3; ++d) nL[d] = JL[d] * F.n[0] + JL[3 + d] * F.n[1] + JL[6 + d] * F.n[2];
+            if (interior) {
+                const double* JR = a.geo + (int64_t)F.c1 * 10;
+                #pragma unroll
+                for (int d = 0; d < 3; ++d) nR[d] = JR[d] * F.n[0] + JR[3 + d] * F.n[1] + JR[6 + d] * F.n[2];
+            }
+        }
+        const int pL = F.meta & 0xff, pR = (F.meta >> 8) & 0xff;
+        for (int j = lane; j < NB; j += 32) {
+            double t = 0.0;
+            for (int g = 0; g < nqf; ++g) {
+                const double* dl = a.dphi_f + (((int64_t)pL * nqf + g) * NB + j) * 3;
+                double sj = nL[0] * dl[0] + nL[1] * dl[1] + nL[2] * dl[2];
+                if (interior) {
+                    const double* dr = a.dphi_f + (((int64_t)pR * nqf + g) * NB + j) * 3;
+                    sj += nR[0] * dr[0] + nR[1] * dr[1] + nR[2] * dr[2];
+                }
+                t = fma(ss[g], sj, t);
+            }
+            a.vf[f * bs + 5 * nqf + j] = t;
         }
         __syncwarp();
     }
@@ -219,17 +263,15 @@ __global__ void __launch_bounds__(kViscWarps * 32) viscous_face(ViscArgs a) {
 
 template <int NB>
 __global__ void __launch_bounds__(kViscWarps * 32) viscous_element(ViscArgs a) {
-    constexpr int NO = 5 * NB, OPL = (NO + 31) / 32;  // outputs (mode, variable) per lane
+    constexpr int MT = (NB + 7) / 8;  // 8-mode tiles of the contractions
     __shared__ double sc[kViscWarps][5 * NB];
-    __shared__ double sh[kViscWarps][kViscMaxQv * 15];  // per volume point: (J^T H)[d][i] w detJ
-    __shared__ double sv[kViscWarps][6 * kViscMaxQf];   // the face block
-    __shared__ double st_[kViscWarps][NB];              // symmetric term per mode
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int nqv = a.nqv, nqf = a.nqf;
+    __shared__ double sh[kViscWarps][kViscMaxQv * 15];     // per volume point: (J^T H)[d][i] w detJ
+    __shared__ double sv[kViscWarps][5 * kViscMaxQf + NB];  // the face block
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, gid = lane >> 2, tq = lane & 3;
+    const int nqv = a.nqv, nqf = a.nqf, kv = 3 * nqv, mp = a.mp, bs = 5 * nqf + NB;
     double* c = sc[w];
     double* hs = sh[w];
     double* vb = sv[w];
-    double* ts = st_[w];
     for (int64_t e = (int64_t)blockIdx.x * kViscWarps + w; e < a.ncell; e += (int64_t)gridDim.x * kViscWarps) {
         const double* ge = a.U + e * (5 * NB);
         for (int i = lane; i < 5 * NB; i += 32) c[i] = ge[i];
@@ -238,7 +280,8 @@ __global__ void __launch_bounds__(kViscWarps * 32) viscous_element(ViscArgs a) {
         for (int i = 0; i < 9; ++i) J[i] = a.geo[e * 10 + i];
         const double detj = a.geo[e * 10 + 9];
         __syncwarp();
-        // volume term: per point the flux H_n (n = x, y, z) pulled back to reference directions
+        // volume term: per point the flux H_n (n = x, y, z) pulled back to reference directions,
+        // hs[k = 3 g + d][i]
         for (int g = lane; g < nqv; g += 32) {
             double Uv[5], G[5][3];
             visc_trace_t<NB>(c, a.phiT_v, a.dphiT_v, nqv, g, J, Uv, G);
@@ -257,80 +300,51 @@ __global__ void __launch_bounds__(kViscWarps * 32) viscous_element(ViscArgs a) {
                     hs[g * 15 + d * 5 + i] = (J[d] * H[0][i] + J[3 + d] * H[1][i] + J[6 + d] * H[2][i]) * wj;
         }
         __syncwarp();
-        double acc[OPL];
+        // R[j][i] = -sum_k Av[k][j] hs[k][i] on the tensor cores (B negated: exact)
+        double acc[MT][2];
         #pragma unroll
-        for (int r = 0; r < OPL; ++r) {
-            acc[r] = 0.0;
-            const int o = lane + 32 * r;
-            if (o < NO) {
-                const int j = o / 5, i = o - 5 * (o / 5);
-                double v = 0.0;
-                for (int g = 0; g < nqv; ++g) {
-                    const double* dp = a.dphi_v + ((int64_t)g * NB + j) * 3;
-                    const double* hg = hs + g * 15 + i;
-                    v = fma(dp[0], hg[0], v);
-                    v = fma(dp[1], hg[5], v);
-                    v = fma(dp[2], hg[10], v);
-                }
-                acc[r] = -v;
-            }
+        for (int mt = 0; mt < MT; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
+        for (int k0 = 0; k0 < kv; k0 += 4) {
+            const int k = k0 + tq;
+            const double b = (gid < 5 && k < kv) ? -hs[k * 5 + gid] : 0.0;
+            const double* ar = a.Av + (int64_t)k * mp + gid;
+            #pragma unroll
+            for (int mt = 0; mt < MT; ++mt) visc_dmma(acc[mt], ar[mt * 8], b);
         }
-        // the element's faces
+        // the element's faces: R[j][i] += sgn sum_g phi_j^side(g) (Fl w 2A)[i][g], R[j][4] += sgn T_j
         for (int q = 0; q < 4; ++q) {
             const ElemFace E = a.ef[4 * e + q];
             const FaceInfo F = a.fi[E.face];
             if (!visc_face_active(F, a.UD)) continue;  // warp-uniform
-            const bool interior = F.c1 >= 0;
             __syncwarp();
-            const double* src = a.vf + (int64_t)E.face * 6 * nqf;
-            for (int i = lane; i < 6 * nqf; i += 32) vb[i] = src[i];
-            // symmetric term T_j = sum_g sfac_g ((J_L^T n) . dphi_j^L(g) + (J_R^T n) . dphi_j^R(g))
-            double nL[3], nR[3] = {0.0, 0.0, 0.0};
-            {
-                const double* JL = a.geo + (int64_t)F.c0 * 10;
+            const double* src = a.vf + (int64_t)E.face * bs;
+            for (int i = lane; i < bs; i += 32) vb[i] = src[i];
+            __syncwarp();
+            const double sg = (E.meta >> 8) == 0 ? 1.0 : -1.0;
+            const double* pt = a.Pf + (int64_t)(E.meta & 0xff) * a.kpf * mp;  // this side's basis values
+            for (int g0 = 0; g0 < nqf; g0 += 4) {
+                const int g = g0 + tq;
+                const double b = (gid < 5 && g < nqf) ? sg * vb[gid * nqf + g] : 0.0;
+                const double* ar = pt + (int64_t)g * mp + gid;
                 #pragma unroll
-                for (int d = 0; d < 3; ++d) nL[d] = JL[d] * F.n[0] + JL[3 + d] * F.n[1] + JL[6 + d] * F.n[2];
-                if (interior) {
-                    const double* JR = a.geo + (int64_t)F.c1 * 10;
-                    #pragma unroll
-                    for (int d = 0; d < 3; ++d) nR[d] = JR[d] * F.n[0] + JR[3 + d] * F.n[1] + JR[6 + d] * F.n[2];
-                }
+                for (int mt = 0; mt < MT; ++mt) visc_dmma(acc[mt], ar[mt * 8], b);
             }
-            __syncwarp();
-            const int pL = F.meta & 0xff, pR = (F.meta >> 8) & 0xff;
-            for (int j = lane; j < NB; j += 32) {
-                double t = 0.0;
-                for (int g = 0; g < nqf; ++g) {
-                    const double* dl = a.dphi_f + (((int64_t)pL * nqf + g) * NB + j) * 3;
-                    double sj = nL[0] * dl[0] + nL[1] * dl[1] + nL[2] * dl[2];
-                    if (interior) {
-                        const double* dr = a.dphi_f + (((int64_t)pR * nqf + g) * NB + j) * 3;
-                        sj += nR[0] * dr[0] + nR[1] * dr[1] + nR[2] * dr[2];
-                    }
-                    t = fma(vb[5 * nqf + g], sj, t);
-                }
-                ts[j] = t;
-            }
-            __syncwarp();
-            const double sgn = (E.meta >> 8) == 0 ? 1.0 : -1.0;
-            const double* ph = a.phi_f + (int64_t)(E.meta & 0xff) * nqf * NB;  // this side's basis values
-            #pragma unroll
-            for (int r = 0; r < OPL; ++r) {
-                const int o = lane + 32 * r;
-                if (o < NO) {
-                    const int j = o / 5, i = o - 5 * (o / 5);
-                    double v = 0.0;
-                    for (int g = 0; g < nqf; ++g) v = fma(ph[g * NB + j], vb[i * nqf + g], v);
-                    if (i == 4) v += ts[j];
-                    acc[r] += sgn * v;
+            if (tq == 2) {  // lanes holding column i = 4
+                #pragma unroll
+                for (int mt = 0; mt < MT; ++mt) {
+                    const int j = mt * 8 + gid;
+                    if (j < NB) acc[mt][0] += sg * vb[5 * nqf + j];
                 }
             }
         }
         double* out = a.R + e * (5 * NB);
         #pragma unroll
-        for (int r = 0; r < OPL; ++r) {
-            const int o = lane + 32 * r;
-            if (o < NO) out[o] = acc[r];
+        for (int mt = 0; mt < MT; ++mt) {
+            const int j = mt * 8 + gid, i0 = 2 * tq;
+            if (j < NB) {
+                if (i0 < 5) out[5 * j + i0] = acc[mt][0];
+                if (i0 + 1 < 5) out[5 * j + i0 + 1] = acc[mt][1];
+            }
         }
         __syncwarp();
     }
