@@ -100,8 +100,7 @@ struct dg_ctx {
     // viscous operator, allocated by its first call: transposed basis tables, per-face-point fluxes
     double* d_visc_phiT_v = nullptr;
     double* d_visc_dphiT_v = nullptr;
-    double* d_visc_phiT_f = nullptr;
-    double* d_visc_dphiT_f = nullptr;
+    double* d_visc_Pt = nullptr;
     double* d_visc_Av = nullptr;
     double* d_visc_Pf = nullptr;
     double* d_visc_vf = nullptr;
@@ -399,8 +398,8 @@ void free_ctx(dg_ctx* c) {
     if (c->d_dphi_v) cudaFree(c->d_dphi_v);
     if (c->d_dphi_f) cudaFree(c->d_dphi_f);
     if (c->d_h) cudaFree(c->d_h);
-    for (double* p : {c->d_visc_phiT_v, c->d_visc_dphiT_v, c->d_visc_phiT_f, c->d_visc_dphiT_f, c->d_visc_Av,
-                      c->d_visc_Pf, c->d_visc_vf})
+    for (double* p : {c->d_visc_phiT_v, c->d_visc_dphiT_v, c->d_visc_Pt,
+                      c->d_visc_Av, c->d_visc_Pf, c->d_visc_vf})
         if (p) cudaFree(p);
     if (c->d_lim_prev) cudaFree(c->d_lim_prev);
     if (c->d_elem_inst) cudaFree(c->d_elem_inst);
@@ -728,28 +727,29 @@ int dg_residual(dg_ctx* c, const double* U, double* R, size_t stride, double t, 
     return cuda_ok(cudaStreamSynchronize(c->stream));
 }
 
-// The viscous operator's tables transposed so that lanes over points read rows, and its
-// per-face-point buffer; made by the first call on the context.
+// The viscous operator's tables (the volume ones transposed so that lanes over points read rows,
+// the A operands of its tensor-core products) and its per-face buffer; made by the first call.
 int viscous_buffers(dg_ctx* c) {
     if (c->d_visc_vf) return DG_OK;
     const Tables& t = c->tab;
     const int nb = t.nb, nqv = t.nqv, nqf = t.nqf;
-    std::vector<double> pv((size_t)nb * nqv), dpv((size_t)nb * 3 * nqv), pf((size_t)24 * nb * nqf),
-        dpf((size_t)24 * nb * 3 * nqf);
+    std::vector<double> pv((size_t)nb * nqv), dpv((size_t)nb * 3 * nqv);  // volume tables, transposed
     for (int g = 0; g < nqv; ++g)
         for (int b = 0; b < nb; ++b) {
             pv[(size_t)b * nqv + g] = t.phi_v[(size_t)g * nb + b];
             for (int d = 0; d < 3; ++d) dpv[((size_t)b * 3 + d) * nqv + g] = t.dphi_v[((size_t)g * nb + b) * 3 + d];
         }
+    // A operands of the tensor-core contractions, rows padded to 4 and modes to 8 (zeros)
+    const int mp = visc_mp(nb), kpv = visc_kp(3 * nqv), kpf = visc_kp(nqf), gp = visc_gp(nqf), kpb = visc_kp(nb);
+    if (gp > kViscMaxGp) return DG_E_ARG;
+    std::vector<double> apt((size_t)24 * 4 * gp * kpb, 0.0);  // face traces: [p][t][g][b]
     for (int p = 0; p < 24; ++p)
         for (int g = 0; g < nqf; ++g)
             for (int b = 0; b < nb; ++b) {
-                pf[((size_t)p * nb + b) * nqf + g] = t.phi_f[((size_t)p * nqf + g) * nb + b];
+                apt[(((size_t)p * 4 + 0) * gp + g) * kpb + b] = t.phi_f[((size_t)p * nqf + g) * nb + b];
                 for (int d = 0; d < 3; ++d)
-                    dpf[(((size_t)p * nb + b) * 3 + d) * nqf + g] = t.dphi_f[(((size_t)p * nqf + g) * nb + b) * 3 + d];
+                    apt[(((size_t)p * 4 + 1 + d) * gp + g) * kpb + b] = t.dphi_f[(((size_t)p * nqf + g) * nb + b) * 3 + d];
             }
-    // A operands of the tensor-core contractions, rows padded to 4 and modes to 8 (zeros)
-    const int mp = visc_mp(nb), kpv = visc_kp(3 * nqv), kpf = visc_kp(nqf);
     std::vector<double> av((size_t)kpv * mp, 0.0), apf((size_t)24 * kpf * mp, 0.0);
     for (int k = 0; k < 3 * nqv; ++k)
         for (int j = 0; j < nb; ++j) av[(size_t)k * mp + j] = t.dphi_v[((size_t)(k / 3) * nb + j) * 3 + k % 3];
@@ -759,8 +759,7 @@ int viscous_buffers(dg_ctx* c) {
                 apf[((size_t)p * kpf + g) * mp + j] = t.phi_f[((size_t)p * nqf + g) * nb + j];
     int rc;
     if ((rc = upload(&c->d_visc_phiT_v, pv)) || (rc = upload(&c->d_visc_dphiT_v, dpv)) ||
-        (rc = upload(&c->d_visc_phiT_f, pf)) || (rc = upload(&c->d_visc_dphiT_f, dpf)) ||
-        (rc = upload(&c->d_visc_Av, av)) || (rc = upload(&c->d_visc_Pf, apf)) ||
+        (rc = upload(&c->d_visc_Av, av)) || (rc = upload(&c->d_visc_Pf, apf)) || (rc = upload(&c->d_visc_Pt, apt)) ||
         (rc = dev_alloc(&c->d_visc_vf, (size_t)c->nface * (5 * nqf + nb))))
         return rc;
     return DG_OK;
@@ -777,9 +776,10 @@ int dg_viscous_residual_device(dg_ctx* c, const double* U, double* R, double mu,
     a.phi_v = c->d_phi_v; a.dphi_v = c->d_dphi_v; a.w_v = c->d_w_v;
     a.phi_f = c->d_phi_f; a.dphi_f = c->d_dphi_f; a.w_f = c->d_w_f; a.UD = c->d_UD;
     a.phiT_v = c->d_visc_phiT_v; a.dphiT_v = c->d_visc_dphiT_v;
-    a.phiT_f = c->d_visc_phiT_f; a.dphiT_f = c->d_visc_dphiT_f; a.vf = c->d_visc_vf;
-    a.Av = c->d_visc_Av; a.Pf = c->d_visc_Pf;
+    a.vf = c->d_visc_vf;
+    a.Av = c->d_visc_Av; a.Pf = c->d_visc_Pf; a.Pt = c->d_visc_Pt;
     a.mp = visc_mp(c->tab.nb); a.kpv = visc_kp(3 * c->tab.nqv); a.kpf = visc_kp(c->tab.nqf);
+    a.gp = visc_gp(c->tab.nqf); a.kpb = visc_kp(c->tab.nb);
     a.ncell = c->nowned; a.nface = c->nface; a.nqv = c->tab.nqv; a.nqf = c->tab.nqf; a.order = c->cfg.order;
     a.mu = mu; a.cq = c->cfg.gamma / prandtl;
     g_launches += 2;

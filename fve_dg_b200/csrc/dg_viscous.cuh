@@ -26,9 +26,10 @@
 // with u = U_1..3 / U_0, e = U_4 / U_0 and rho = max(U_0, 1e-8), as ExplicitDiffusion.h:28-31,69-73.
 //
 // Two launches, FP64:
-//   viscous_face     one warp per face, lanes over the face points: both traces (values and physical
-//                    gradients) once per face, the averaged flux with its penalty (stored per point as
-//                    Fl w 2A), and the energy-only symmetric term per mode,
+//   viscous_face     one warp per face: both traces (values and reference gradients at the face
+//                    points, on the FP64 tensor cores: points x variables over modes) once per face;
+//                    then lanes over the points: the averaged flux with its penalty (stored per point
+//                    as Fl w 2A); then the energy-only symmetric term per mode,
 //                    T_j = sum_g sfac_g w_g 2A n . (grad phi_j^L + grad phi_j^R), written as
 //                    (J_L^T n) . dphi^L + (J_R^T n) . dphi^R (the same for both sides, up to sign).
 //   viscous_element  one warp per element: the volume term (lanes over the volume points: J^T H w detJ
@@ -58,22 +59,23 @@ struct ViscArgs {
     const double* UD;       // [nface][nqf][5] Dirichlet data, or null
     const double* phiT_v;   // [nb][nqv] the volume tables transposed (lanes over points read rows)
     const double* dphiT_v;  // [nb][3][nqv]
-    const double* phiT_f;   // [24][nb][nqf]
-    const double* dphiT_f;  // [24][nb][3][nqf]
+    const double* Pt;       // [24][4][gp][kpb] A of the face traces: phi_f, then dphi_f[.][.][.][d], zero-padded
     const double* Av;       // [kpv][mp] A of the volume contraction: dphi_v[k/3][j][k%3], zero-padded
     const double* Pf;       // [24][kpf][mp] A of the face contraction: phi_f[p][g][j], zero-padded
     double* vf;             // [nface][5 nqf + nb] per face: Fl w 2A [5][nqf], then T_j [nb]
     int64_t ncell, nface;
-    int nqv, nqf, order, kpv, kpf, mp;
+    int nqv, nqf, order, kpv, kpf, mp, gp, kpb;
     double mu, cq;          // viscosity and gamma / Pr
 };
 
 constexpr int kViscWarps = 4;
 constexpr int kViscMaxQv = 64;  // volume points an element warp stages (the largest rule has 57)
 constexpr int kViscMaxQf = 32;  // face points, one per lane (the largest rule has 24)
+constexpr int kViscMaxGp = 24;  // face points padded to the 8-row tiles of the trace products
 
 inline int visc_mp(int nb) { return 8 * ((nb + 7) / 8); }  // modes padded to the 8-row tiles
 inline int visc_kp(int k) { return 4 * ((k + 3) / 4); }     // contraction length padded to 4
+inline int visc_gp(int nqf) { return 8 * ((nqf + 7) / 8); }  // face points padded to 8
 
 // d (one 8 x 8 FP64 tile of D, two entries per lane) += A (8 x 4) B (4 x 8); lane l holds
 // A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
@@ -153,6 +155,52 @@ __device__ __forceinline__ void visc_trace_t(const double* c, const double* __re
         for (int m = 0; m < 3; ++m) G[k][m] = J[3 * m] * R[k][0] + J[3 * m + 1] * R[k][1] + J[3 * m + 2] * R[k][2];
 }
 
+// One side's traces at the face points on the tensor cores: sd[t][g][i] = sum_b pt[t][g][b] c[b][i]
+// for t = 0 (values) and t = 1..3 (reference gradient components), g < gp, i < 5.
+template <int NB>
+__device__ __forceinline__ void visc_face_traces(const double* c, const double* __restrict__ pt, int gp, int kpb,
+                                                 double* sd, int lane) {
+    constexpr int KT = (NB + 3) / 4, MTMAX = kViscMaxGp / 8;
+    const int gid = lane >> 2, tq = lane & 3, mtn = gp / 8;
+    double d[4][MTMAX][2];
+    #pragma unroll
+    for (int t = 0; t < 4; ++t)
+        #pragma unroll
+        for (int mt = 0; mt < MTMAX; ++mt) d[t][mt][0] = d[t][mt][1] = 0.0;
+    #pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+        const int b = kt * 4 + tq;
+        const double bv = (gid < 5 && b < NB) ? c[5 * b + gid] : 0.0;
+        #pragma unroll
+        for (int t = 0; t < 4; ++t)
+            #pragma unroll
+            for (int mt = 0; mt < MTMAX; ++mt)
+                if (mt < mtn) visc_dmma(d[t][mt], pt[((t * gp) + mt * 8 + gid) * kpb + b], bv);
+    }
+    const int i0 = 2 * tq;
+    #pragma unroll
+    for (int t = 0; t < 4; ++t)
+        #pragma unroll
+        for (int mt = 0; mt < MTMAX; ++mt)
+            if (mt < mtn) {
+                double* row = sd + ((t * gp) + mt * 8 + gid) * 5;
+                if (i0 < 5) row[i0] = d[t][mt][0];
+                if (i0 + 1 < 5) row[i0 + 1] = d[t][mt][1];
+            }
+}
+
+// A point's value and physical gradient from traces staged by visc_face_traces.
+__device__ __forceinline__ void visc_trace_smem(const double* sd, int gp, int g, const double J[9], double Uv[5],
+                                                double G[5][3]) {
+    #pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        Uv[k] = sd[g * 5 + k];
+        const double r0 = sd[(gp + g) * 5 + k], r1 = sd[(2 * gp + g) * 5 + k], r2 = sd[(3 * gp + g) * 5 + k];
+        #pragma unroll
+        for (int m = 0; m < 3; ++m) G[k][m] = J[3 * m] * r0 + J[3 * m + 1] * r1 + J[3 * m + 2] * r2;
+    }
+}
+
 // Faces whose viscous terms act: interior, Dirichlet with data, Pseudo3DZ (ExplicitDiffusion.h:380-612).
 __device__ __forceinline__ bool visc_face_active(const FaceInfo& F, const double* UD) {
     const int bc = (F.meta >> 16) & 0xff;
@@ -160,14 +208,15 @@ __device__ __forceinline__ bool visc_face_active(const FaceInfo& F, const double
 }
 
 template <int NB>
-__global__ void __launch_bounds__(kViscWarps * 32) viscous_face(ViscArgs a) {
+__global__ void __launch_bounds__(kViscWarps * 32, 4) viscous_face(ViscArgs a) {
     __shared__ double sc[kViscWarps][2][5 * NB];
     __shared__ double ssf[kViscWarps][kViscMaxQf];  // sfac w 2A per face point
+    __shared__ double str[kViscWarps][2][4 * kViscMaxGp * 5];  // traces per side: [t][g][i]
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double* cL = sc[w][0];
     double* cR = sc[w][1];
     double* ss = ssf[w];
-    const int nqf = a.nqf, bs = 5 * nqf + NB;
+    const int nqf = a.nqf, bs = 5 * nqf + NB, gp = a.gp, kpb = a.kpb;
     const double beta_base = (double)((a.order + 1) * (a.order + 1));
     for (int64_t f = (int64_t)blockIdx.x * kViscWarps + w; f < a.nface; f += (int64_t)gridDim.x * kViscWarps) {
         const FaceInfo F = a.fi[f];
@@ -181,22 +230,25 @@ __global__ void __launch_bounds__(kViscWarps * 32) viscous_face(ViscArgs a) {
             for (int i = lane; i < 5 * NB; i += 32) cR[i] = gR[i];
         }
         __syncwarp();
+        {
+            const int pL0 = F.meta & 0xff, pR0 = (F.meta >> 8) & 0xff;
+            visc_face_traces<NB>(cL, a.Pt + (int64_t)pL0 * 4 * gp * kpb, gp, kpb, str[w][0], lane);
+            if (interior) visc_face_traces<NB>(cR, a.Pt + (int64_t)pR0 * 4 * gp * kpb, gp, kpb, str[w][1], lane);
+        }
+        __syncwarp();
         if (lane < nqf) {
             const int g = lane;
-            const int pL = F.meta & 0xff, pR = (F.meta >> 8) & 0xff;
             const double n[3] = {F.n[0], F.n[1], F.n[2]};
             double J[9];
             #pragma unroll
             for (int i = 0; i < 9; ++i) J[i] = a.geo[(int64_t)F.c0 * 10 + i];
             double UL[5], UR[5], X[5][3];
-            visc_trace_t<NB>(cL, a.phiT_f + (int64_t)pL * NB * nqf, a.dphiT_f + (int64_t)pL * NB * 3 * nqf, nqf, g, J,
-                             UL, X);
+            visc_trace_smem(str[w][0], gp, g, J, UL, X);
             if (interior) {
                 #pragma unroll
                 for (int i = 0; i < 9; ++i) J[i] = a.geo[(int64_t)F.c1 * 10 + i];
                 double GR[5][3];
-                visc_trace_t<NB>(cR, a.phiT_f + (int64_t)pR * NB * nqf, a.dphiT_f + (int64_t)pR * NB * 3 * nqf, nqf,
-                                 g, J, UR, GR);
+                visc_trace_smem(str[w][1], gp, g, J, UR, GR);
                 #pragma unroll
                 for (int k = 0; k < 5; ++k)
                     #pragma unroll
