@@ -537,7 +537,10 @@ def run_viscous(args, cfg, rank, world, local, dist):
                              f"{kk} evaluations, {el:.1f} s", "cpu_model": cpu_model()}
     if rank == 0:
         ms_each = ms / args.steps
-        bytes_each = 2 * dof * 8 + m.ncell * (80 + 8 + 32) + m.nface * 48 * 2
+        # the state read by both launches, the residual written, the per-face buffer written once and
+        # read from both sides, geometry and face records
+        face_block = 8 * (5 * conv.nq_face + nb)
+        bytes_each = 3 * dof * 8 + 3 * m.nface * face_block + m.ncell * (80 + 8 + 32) + m.nface * 48 * 2
         peak, peak_kind = read_peaks()
         line = {"metric": "viscous residual DOF evaluations/s", "value": value, "unit": "DOF-residual/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_each,
@@ -546,11 +549,12 @@ def run_viscous(args, cfg, rank, world, local, dist):
                 "config": {"workload": args.config + "-viscous", "desc": cfg["desc"] + "; ExplicitDiffusion, mu = Pr = 1",
                            "tets": m.ncell, "order": P, "parallelism": f"independent instance per GPU x{world}"},
                 "gpu_launches": launches,
-                "roofline": {"bound": "hbm", "kernel": "viscous_residual", "achieved": bytes_each / (ms_each / 1e3) / 1e9,
+                "roofline": {"bound": "hbm", "kernel": "viscous_face + viscous_element",
+                             "achieved": bytes_each / (ms_each / 1e3) / 1e9,
                              "peak": peak, "unit": "GB/s", "frac": bytes_each / (ms_each / 1e3) / 1e9 / peak,
                              "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": bytes_each,
-                             "note": "one thread per element recomputes its faces' neighbour traces in FP64: "
-                                     "FP64-arithmetic bound, not HBM bound"},
+                             "note": "FP64 traces and contractions (on the FP64 tensor cores) per face and per "
+                                     "element: bound by instruction issue and latency, not by HBM"},
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e, "unit": "DOF-residual/s", "h2d_bytes_per_step": dof * 8, "d2h_bytes_per_step": dof * 8,
                         "steps": k}}
