@@ -494,7 +494,20 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
     std::vector<double> hh(c->ncell);
     for (int64_t e = 0; e < c->ncell; ++e) {
         double area = 0.0;
-        for (int q = 0; q < fill[e]; ++q) area += geo.area[hef[4 * e + q].face];
+        if (fill[e] == 4 || !mesh->points || !mesh->cell_nodes) {
+            for (int q = 0; q < fill[e]; ++q) area += geo.area[hef[4 * e + q].face];
+        } else {  // a ghost without all its faces: the areas of its four sides from its vertices
+            const int64_t* cn = mesh->cell_nodes + 4 * e;
+            for (int o = 0; o < 4; ++o) {
+                const double* p[3];
+                for (int k = 0, m = 0; k < 4; ++k)
+                    if (k != o) p[m++] = mesh->points + 3 * cn[k];
+                const double a[3] = {p[1][0] - p[0][0], p[1][1] - p[0][1], p[1][2] - p[0][2]};
+                const double b[3] = {p[2][0] - p[0][0], p[2][1] - p[0][1], p[2][2] - p[0][2]};
+                const double n[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+                area += std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]) * 0.5;
+            }
+        }
         hh[e] = geo.detj[e] / 6.0 / area;
     }
     const size_t nstate = (size_t)c->ncell * 5 * nb;

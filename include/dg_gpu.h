@@ -96,7 +96,10 @@ typedef struct dg_mesh_desc {
      * shares with owned cells (1 to 4); the context holds its state and computes the fluxes of those
      * faces but no residual, limiting, viscous term or reduction for it: residual rows of ghosts are
      * left unwritten and dg_conservation / dg_max_wave_speed / dg_check_state cover owned cells.
-     * 0 for an ordinary mesh (zero-initialise the struct). */
+     * The viscous penalty of a face uses its cells[0]'s volume over the areas of its four sides:
+     * for a ghost with missing faces these come from its vertices (form (b)); in form (a) give the
+     * viscous operator ghosts with all four faces. 0 for an ordinary mesh (zero-initialise the
+     * struct). */
     int64_t nghost;
 } dg_mesh_desc;
 

@@ -97,3 +97,25 @@ def test_stage_entry_points_validate():
         assert lib.dg_state_device(conv._ctx, which)
     assert lib.dg_ssprk3_stage(conv._ctx, 1e-3, 0) == 0
     assert lib.dg_ssprk3(conv._ctx, 0.0, 0) == 0
+
+
+@pytest.mark.parametrize("P", [2, 3])
+def test_owned_viscous_and_limiter_equal_whole_mesh(P):
+    """The viscous operator and the standalone limiter on a part with ghost elements give the
+    whole mesh's owned rows: ghosts need only their faces to owned elements."""
+    from fve_dg_b200.partition import LocalMesh, partition_elements
+    m = box_mesh(6, jitter=0.1, seed=23, periodic=(1, 1, 0), bc="Pseudo3DZ")
+    U = problems.project(m, P, problems.density_wave(A=0.6, vel=(1.0, 0.5, 0.25), p=0.05))
+    rng = np.random.default_rng(P)
+    Ur = U + 0.05 * rng.standard_normal(U.shape) * (np.arange(U.shape[1]) >= 5) * np.abs(U[:, :5]).max()
+    whole = ExplicitConvection(m, order=P)
+    V = whole.viscous_eval(U, mu=0.01, prandtl=0.72)
+    Lw = whole.limit(Ur, U)
+    part = partition_elements(m, 3)
+    for r in range(3):
+        lm = LocalMesh(m, part, r)
+        conv = ExplicitConvection(lm.mesh, order=P)
+        Vl = conv.viscous_eval(U[lm.l2g], mu=0.01, prandtl=0.72)[: lm.n_owned]
+        assert rel_l2(Vl, V[lm.owned]) <= 1e-14, rel_l2(Vl, V[lm.owned])
+        Ll = conv.limit(Ur[lm.l2g], U[lm.l2g])[: lm.n_owned]
+        assert rel_l2(Ll, Lw[lm.owned]) == 0.0
