@@ -142,6 +142,8 @@ def kernel_bytes(name, P, ncell, nface, nqf):
         return 3 * state + ncell * elem_rec + nface * nqf * 5 * 8
     if name == "limiter":                # bounds from the stage input, the output read and written
         return 3 * state + nface * (48 + 80) + ncell * 32
+    if name == "viscous":                # state read by both launches, residual written, face blocks
+        return 3 * state + 3 * nface * 8 * (5 * nqf + nb) + ncell * (80 + 8 + 32) + nface * 96
     kf = (nqf + 7) // 8 * 8
     kb = (nb - 1 + 7) // 8 * 8
     fj = nface * (5 * kf * 4 + 2 * 5 * 8)  # split flux deviations (A rows) + FP64 reference and mode-0 sums
@@ -265,6 +267,10 @@ def main():
                     help="time the explicit viscous operator (ExplicitDiffusion::eval) on the workload's mesh instead")
     ap.add_argument("--limiter", default=None, choices=["positive", "positive-avg"],
                     help="positivity-preserving limiter after every RK stage (timed as its own kernel class)")
+    ap.add_argument("--mu", type=float, default=0.0,
+                    help="viscosity: > 0 steps compressible Navier-Stokes (the viscous residual every stage, "
+                         "timed as its own kernel class), e.g. 1/1600 for the Taylor-Green vortex at Re 1600")
+    ap.add_argument("--prandtl", type=float, default=0.71)
     ap.add_argument("--n", type=int, default=0, help="override the mesh size (cubes per side), for profiling")
     ap.add_argument("--split", action="store_true",
                     help="one mesh split across the N ranks (element slabs with ghost elements), SSP-RK3 one "
@@ -318,7 +324,8 @@ def main():
     # persistent tile queue serves ensembles of uneven meshes (--config ensemble)
     schedule = args.schedule or "two-launch"
     conv = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf,
-                              precision=args.precision, device=local, schedule=schedule, limiter=args.limiter)
+                              precision=args.precision, device=local, schedule=schedule, limiter=args.limiter,
+                              mu=args.mu, prandtl=args.prandtl)
     conv.set_state(U0)
     dt = problems.cfl_dt(CFL, cfg["L"] / cfg["n"], P, conv.max_wave_speed())
     nb = conv.num_basis
@@ -340,7 +347,7 @@ def main():
     forms = {args.precision: {"value": value, "ms_per_step": ms / args.steps, "schedule": schedule}}
     if args.precision == "mixed" and not args.no_compare:
         f64 = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf, precision="fp64",
-                                 device=local, limiter=args.limiter)
+                                 device=local, limiter=args.limiter, mu=args.mu, prandtl=args.prandtl)
         f64.set_state(U0)
         ms64, _ = time_steps(f64, dt, args.warmup, args.steps, dist, torch, launch_count)
         U64 = f64.get_state()  # before the per-kernel timing pass below advances it
@@ -374,7 +381,9 @@ def main():
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "bf16x3 contractions, f32 flux, f64 state",
                 "data": "synthetic",
-                "config": {"workload": args.config, "desc": cfg["desc"], "precision": args.precision, "limiter": args.limiter,
+                "config": {"workload": args.config + ("-ns" if args.mu > 0 else ""), "desc": cfg["desc"],
+                           "precision": args.precision, "limiter": args.limiter,
+                           "mu": args.mu, "prandtl": args.prandtl if args.mu > 0 else None,
                            "schedule": schedule, "tets": m.ncell, "order": P, "dof_per_stage": 5 * nb * m.ncell,
                            "dt": dt, "l2": "state larger than L2 (no flush needed)",
                            "parallelism": f"independent instance per GPU x{world}"},
@@ -387,9 +396,9 @@ def main():
         dist.destroy_process_group()
 
 
-KNAMES = {("fp64", "two-launch"): {0: "face_flux_fp64", 1: "element_fp64", 4: "limiter"},
-          ("mixed", "two-launch"): {0: "face_flux_mixed", 1: "element_mixed", 4: "limiter"},
-          ("mixed", "persistent"): {2: "stage_persistent_mixed", 4: "limiter"}}
+KNAMES = {("fp64", "two-launch"): {0: "face_flux_fp64", 1: "element_fp64", 3: "viscous", 4: "limiter"},
+          ("mixed", "two-launch"): {0: "face_flux_mixed", 1: "element_mixed", 3: "viscous", 4: "limiter"},
+          ("mixed", "persistent"): {2: "stage_persistent_mixed", 3: "viscous", 4: "limiter"}}
 
 
 def time_steps(conv, dt, warmup, steps, dist, torch, launch_count):

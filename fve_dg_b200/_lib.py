@@ -40,7 +40,8 @@ class MeshDesc(ctypes.Structure):
 class Config(ctypes.Structure):
     _fields_ = [("order", ctypes.c_int), ("flux", ctypes.c_int), ("quad_vol", ctypes.c_int),
                 ("quad_face", ctypes.c_int), ("gamma", ctypes.c_double), ("precision", ctypes.c_int),
-                ("device", ctypes.c_int), ("schedule", ctypes.c_int), ("limiter", ctypes.c_int)]
+                ("device", ctypes.c_int), ("schedule", ctypes.c_int), ("limiter", ctypes.c_int),
+                ("mu", ctypes.c_double), ("prandtl", ctypes.c_double)]
 
 
 _lib = None

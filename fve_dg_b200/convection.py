@@ -27,7 +27,10 @@ LIMITER = {None: 0, "none": 0, "positive": 1, "positive-avg": 2}
 
 class ExplicitConvection:
     def __init__(self, mesh, order=3, flux="LF", quad_vol=-1, quad_face=-1, gamma=1.4,
-                 precision="fp64", device=0, schedule="two-launch", limiter=None, _ensemble=None):
+                 precision="fp64", device=0, schedule="two-launch", limiter=None, mu=0.0, prandtl=1.0,
+                 _ensemble=None):
+        """mu > 0 steps the compressible Navier-Stokes equations: every SSP-RK3 stage adds the viscous
+        residual (viscous_eval with mu and prandtl) as the reference's viscous driver does."""
         self.mesh = mesh
         self.order = int(order)
         self.flux = flux
@@ -38,7 +41,9 @@ class ExplicitConvection:
                        quad_vol=int(quad_vol), quad_face=int(quad_face), gamma=self.gamma,
                        precision=PRECISION[precision] if isinstance(precision, str) else int(precision),
                        device=int(device), schedule=SCHEDULE[schedule] if isinstance(schedule, str) else int(schedule),
-                       limiter=LIMITER[limiter] if limiter is None or isinstance(limiter, str) else int(limiter))
+                       limiter=LIMITER[limiter] if limiter is None or isinstance(limiter, str) else int(limiter),
+                       mu=float(mu), prandtl=float(prandtl))
+        self.mu, self.prandtl = float(mu), float(prandtl)
         err = ctypes.c_int(0)
         if _ensemble is None:
             self._desc = mesh.desc()

@@ -104,6 +104,7 @@ struct dg_ctx {
     double* d_visc_Av = nullptr;
     double* d_visc_Pf = nullptr;
     double* d_visc_vf = nullptr;
+    double* d_Rv = nullptr;  // viscous residual of the current stage input (dg_config.mu > 0)
     int sms = 148;
     // ensembles: instance element offsets, per-instance dt on the device, instance of each element
     int ninst = 1;
@@ -248,6 +249,7 @@ StageArgs stage_args(dg_ctx* c, const double* U, const double* U0, double* out, 
     a.with_volume = with_volume;
     a.dt_inst = mode == 1 ? c->d_dt_inst : nullptr;
     a.elem_inst = c->d_elem_inst;
+    a.Rv = nullptr;
     return a;
 }
 
@@ -284,6 +286,54 @@ int timed(dg_ctx* c, int cls, cudaStream_t s, F&& fn) {
 
 // One SSP-RK3 step (Shu-Osher) on the device state, FP64 form:
 //   U1 = U + dt L(U);  U2 = 3/4 U + 1/4 (U1 + dt L(U1));  U = 1/3 U + 2/3 (U2 + dt L(U2)).
+// The viscous operator's tables (the volume ones transposed so that lanes over points read rows,
+// the A operands of its tensor-core products) and its per-face buffer; made by the first call.
+int viscous_buffers(dg_ctx* c) {
+    if (c->d_visc_vf) return DG_OK;
+    const Tables& t = c->tab;
+    const int nb = t.nb, nqv = t.nqv, nqf = t.nqf;
+    std::vector<double> pv((size_t)nb * nqv), dpv((size_t)nb * 3 * nqv);  // volume tables, transposed
+    for (int g = 0; g < nqv; ++g)
+        for (int b = 0; b < nb; ++b) {
+            pv[(size_t)b * nqv + g] = t.phi_v[(size_t)g * nb + b];
+            for (int d = 0; d < 3; ++d) dpv[((size_t)b * 3 + d) * nqv + g] = t.dphi_v[((size_t)g * nb + b) * 3 + d];
+        }
+    // A operands of the tensor-core contractions, rows padded to 4 and modes to 8 (zeros)
+    const int mp = visc_mp(nb), kpv = visc_kp(3 * nqv), kpf = visc_kp(nqf), gp = visc_gp(nqf), kpb = visc_kp(nb);
+    if (gp > kViscMaxGp) return DG_E_ARG;
+    std::vector<double> apt((size_t)24 * 4 * gp * kpb, 0.0);  // face traces: [p][t][g][b]
+    for (int p = 0; p < 24; ++p)
+        for (int g = 0; g < nqf; ++g)
+            for (int b = 0; b < nb; ++b) {
+                apt[(((size_t)p * 4 + 0) * gp + g) * kpb + b] = t.phi_f[((size_t)p * nqf + g) * nb + b];
+                for (int d = 0; d < 3; ++d)
+                    apt[(((size_t)p * 4 + 1 + d) * gp + g) * kpb + b] = t.dphi_f[(((size_t)p * nqf + g) * nb + b) * 3 + d];
+            }
+    std::vector<double> av((size_t)kpv * mp, 0.0), apf((size_t)24 * kpf * mp, 0.0);
+    for (int k = 0; k < 3 * nqv; ++k)
+        for (int j = 0; j < nb; ++j) av[(size_t)k * mp + j] = t.dphi_v[((size_t)(k / 3) * nb + j) * 3 + k % 3];
+    for (int p = 0; p < 24; ++p)
+        for (int g = 0; g < nqf; ++g)
+            for (int j = 0; j < nb; ++j)
+                apf[((size_t)p * kpf + g) * mp + j] = t.phi_f[((size_t)p * nqf + g) * nb + j];
+    int rc;
+    if ((rc = upload(&c->d_visc_phiT_v, pv)) || (rc = upload(&c->d_visc_dphiT_v, dpv)) ||
+        (rc = upload(&c->d_visc_Av, av)) || (rc = upload(&c->d_visc_Pf, apf)) || (rc = upload(&c->d_visc_Pt, apt)) ||
+        (rc = dev_alloc(&c->d_visc_vf, (size_t)c->nface * (5 * nqf + nb))))
+        return rc;
+    return DG_OK;
+}
+
+int viscous_launch(dg_ctx* c, const double* U, double* R, double mu, double prandtl, cudaStream_t s);
+
+// Navier-Stokes stepping (dg_config.mu > 0): the viscous residual of the stage input, which the
+// element kernels' update subtracts from the convective one: L = (R_visc - R_conv) / b, as the
+// reference's viscous driver steps (tests/test_diffusion.cpp:381-382).
+int viscous_stage(dg_ctx* c, const double* in, cudaStream_t s) {
+    if (!(c->cfg.mu > 0.0)) return DG_OK;
+    return timed(c, 3, s, [&] { return viscous_launch(c, in, c->d_Rv, c->cfg.mu, c->cfg.prandtl, s); });
+}
+
 // Limiter after stage st (dg_config.limiter): bounds from the stage input's statistics, the output
 // limited in place and its statistics written for the next stage; mir = the output's split rows in
 // the mixed form (refreshed where the limiter acted). The input's statistics come from the previous
@@ -317,10 +367,14 @@ int step_fp64(dg_ctx* c, double dt, cudaStream_t s, int st0, int st1) {
     const double* in[3] = {c->d_Un, c->d_Ua, c->d_Ub};
     double* out[3] = {c->d_Ua, c->d_Ub, c->d_Un};
     for (int st = st0; st < st1; ++st) {
-        int rc = timed(c, 0, s, [&] { return dispatch_face(c->cfg.order, c->qv, c->qf, face_args(c, in[st], 3), s); });
+        int rc = viscous_stage(c, in[st], s);
+        if (rc) return rc;
+        rc = timed(c, 0, s, [&] { return dispatch_face(c->cfg.order, c->qv, c->qf, face_args(c, in[st], 3), s); });
         if (rc) return rc;
         rc = timed(c, 1, s, [&] {
-            return dispatch_element(c->cfg.order, c->qv, c->qf, stage_args(c, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 1), s);
+            StageArgs sa = stage_args(c, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 1);
+            sa.Rv = c->cfg.mu > 0.0 ? c->d_Rv : nullptr;
+            return dispatch_element(c->cfg.order, c->qv, c->qf, sa, s);
         });
         if (rc) return rc;
         if ((rc = limit_stage(c, st, in[st], out[st], nullptr, s))) return rc;
@@ -337,16 +391,25 @@ int step(dg_ctx* c, double dt, cudaStream_t s, int st0 = 0, int st1 = 3) {
         auto post = [&](const double* in, double* out, int mir) {
             return limit_stage(c, (mir + 2) % 3, in, out, c->mixed.mir[mir], s);
         };
-        if (c->cfg.schedule == 1)
-            return step_persistent(c->mixed, c->d_queue, c->qs, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches,
-                                   tm, post, st0, st1);
-        return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm, post, st0, st1);
+        auto stages = [&](int a0, int a1) {
+            if (c->cfg.schedule == 1)
+                return step_persistent(c->mixed, c->d_queue, c->qs, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s,
+                                       &g_launches, tm, post, a0, a1);
+            return step_mixed(c->mixed, c->d_Un, c->d_Ua, c->d_Ub, dt, s, &g_launches, tm, post, a0, a1);
+        };
+        if (!(c->cfg.mu > 0.0)) return stages(st0, st1);
+        const double* in[3] = {c->d_Un, c->d_Ua, c->d_Ub};
+        for (int st = st0; st < st1; ++st) {  // the element kernels read the stage's viscous residual
+            int rc = viscous_stage(c, in[st], s);
+            if (rc || (rc = stages(st, st + 1))) return rc;
+        }
+        return DG_OK;
     }
     return step_fp64(c, dt, s, st0, st1);
 }
 
 int launches_per_step(const dg_ctx* c) {
-    const int lim = c->cfg.limiter ? (c->nowned < c->ncell ? 6 : 3) : 0;
+    const int lim = (c->cfg.limiter ? (c->nowned < c->ncell ? 6 : 3) : 0) + (c->cfg.mu > 0.0 ? 6 : 0);
     if (c->cfg.precision == DG_PREC_MIXED) return (c->cfg.schedule == 1 ? 3 : mixed_launches_per_step(c->mixed)) + lim;
     return 6 + lim;
 }
@@ -399,7 +462,7 @@ void free_ctx(dg_ctx* c) {
     if (c->d_dphi_f) cudaFree(c->d_dphi_f);
     if (c->d_h) cudaFree(c->d_h);
     for (double* p : {c->d_visc_phiT_v, c->d_visc_dphiT_v, c->d_visc_Pt,
-                      c->d_visc_Av, c->d_visc_Pf, c->d_visc_vf})
+                      c->d_visc_Av, c->d_visc_Pf, c->d_visc_vf, c->d_Rv})
         if (p) cudaFree(p);
     if (c->d_lim_prev) cudaFree(c->d_lim_prev);
     if (c->d_elem_inst) cudaFree(c->d_elem_inst);
@@ -447,6 +510,7 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
     if (tet_rule_npts(qv) <= 0 || tri_rule_npts(qf) <= 0) return fail(nullptr, DG_E_ARG);
     if (cfg->limiter < 0 || cfg->limiter > 2 || (cfg->limiter && !limiter_supported(cfg->order, qv)))
         return fail(nullptr, DG_E_ARG);
+    if (!(cfg->mu >= 0.0) || (cfg->mu > 0.0 && !(cfg->prandtl > 0.0))) return fail(nullptr, DG_E_ARG);
     if (mesh->ncell <= 0 || mesh->ncell > (int64_t)1 << 30 || mesh->nface <= 0 || mesh->nface > (int64_t)1 << 30)
         return fail(nullptr, DG_E_ARG);
     Geometry geo;
@@ -546,6 +610,11 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
         int dev = 0, sms = 148;
         if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
             c->sms = sms;
+    }
+    // Navier-Stokes stepping: the viscous buffers now, so that no step allocates (graph capture)
+    if (cfg->mu > 0.0) {
+        if ((rc = viscous_buffers(c)) || (rc = dev_alloc(&c->d_Rv, (size_t)c->ncell * 5 * nb))) return fail(c, rc);
+        c->mixed.Rv = c->d_Rv;
     }
     // the limiter's per-cell statistics, allocated here so that no step allocates (graph capture)
     if (cfg->limiter) {
@@ -740,50 +809,20 @@ int dg_residual(dg_ctx* c, const double* U, double* R, size_t stride, double t, 
     return cuda_ok(cudaStreamSynchronize(c->stream));
 }
 
-// The viscous operator's tables (the volume ones transposed so that lanes over points read rows,
-// the A operands of its tensor-core products) and its per-face buffer; made by the first call.
-int viscous_buffers(dg_ctx* c) {
-    if (c->d_visc_vf) return DG_OK;
-    const Tables& t = c->tab;
-    const int nb = t.nb, nqv = t.nqv, nqf = t.nqf;
-    std::vector<double> pv((size_t)nb * nqv), dpv((size_t)nb * 3 * nqv);  // volume tables, transposed
-    for (int g = 0; g < nqv; ++g)
-        for (int b = 0; b < nb; ++b) {
-            pv[(size_t)b * nqv + g] = t.phi_v[(size_t)g * nb + b];
-            for (int d = 0; d < 3; ++d) dpv[((size_t)b * 3 + d) * nqv + g] = t.dphi_v[((size_t)g * nb + b) * 3 + d];
-        }
-    // A operands of the tensor-core contractions, rows padded to 4 and modes to 8 (zeros)
-    const int mp = visc_mp(nb), kpv = visc_kp(3 * nqv), kpf = visc_kp(nqf), gp = visc_gp(nqf), kpb = visc_kp(nb);
-    if (gp > kViscMaxGp) return DG_E_ARG;
-    std::vector<double> apt((size_t)24 * 4 * gp * kpb, 0.0);  // face traces: [p][t][g][b]
-    for (int p = 0; p < 24; ++p)
-        for (int g = 0; g < nqf; ++g)
-            for (int b = 0; b < nb; ++b) {
-                apt[(((size_t)p * 4 + 0) * gp + g) * kpb + b] = t.phi_f[((size_t)p * nqf + g) * nb + b];
-                for (int d = 0; d < 3; ++d)
-                    apt[(((size_t)p * 4 + 1 + d) * gp + g) * kpb + b] = t.dphi_f[(((size_t)p * nqf + g) * nb + b) * 3 + d];
-            }
-    std::vector<double> av((size_t)kpv * mp, 0.0), apf((size_t)24 * kpf * mp, 0.0);
-    for (int k = 0; k < 3 * nqv; ++k)
-        for (int j = 0; j < nb; ++j) av[(size_t)k * mp + j] = t.dphi_v[((size_t)(k / 3) * nb + j) * 3 + k % 3];
-    for (int p = 0; p < 24; ++p)
-        for (int g = 0; g < nqf; ++g)
-            for (int j = 0; j < nb; ++j)
-                apf[((size_t)p * kpf + g) * mp + j] = t.phi_f[((size_t)p * nqf + g) * nb + j];
-    int rc;
-    if ((rc = upload(&c->d_visc_phiT_v, pv)) || (rc = upload(&c->d_visc_dphiT_v, dpv)) ||
-        (rc = upload(&c->d_visc_Av, av)) || (rc = upload(&c->d_visc_Pf, apf)) || (rc = upload(&c->d_visc_Pt, apt)) ||
-        (rc = dev_alloc(&c->d_visc_vf, (size_t)c->nface * (5 * nqf + nb))))
-        return rc;
-    return DG_OK;
-}
-
 int dg_viscous_residual_device(dg_ctx* c, const double* U, double* R, double mu, double prandtl, void* stream) {
     if (!c || !U || !R || !(mu >= 0.0) || !(prandtl > 0.0)) return DG_E_ARG;
     if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
     DG_CUDA(cudaSetDevice(c->cfg.device));
     int rc = viscous_buffers(c);
     if (rc) return rc;
+    return viscous_launch(c, U, R, mu, prandtl, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+namespace {
+// The viscous residual of U into R (two launches on stream s); the buffers exist.
+int viscous_launch(dg_ctx* c, const double* U, double* R, double mu, double prandtl, cudaStream_t s) {
     ViscArgs a;
     a.U = U; a.R = R; a.geo = c->d_geo; a.h = c->d_h; a.fi = c->d_fi; a.ef = c->d_ef;
     a.phi_v = c->d_phi_v; a.dphi_v = c->d_dphi_v; a.w_v = c->d_w_v;
@@ -796,8 +835,11 @@ int dg_viscous_residual_device(dg_ctx* c, const double* U, double* R, double mu,
     a.ncell = c->nowned; a.nface = c->nface; a.nqv = c->tab.nqv; a.nqf = c->tab.nqf; a.order = c->cfg.order;
     a.mu = mu; a.cq = c->cfg.gamma / prandtl;
     g_launches += 2;
-    return launch_viscous(c->cfg.order, a, c->sms, (cudaStream_t)stream);
+    return launch_viscous(c->cfg.order, a, c->sms, s);
 }
+}  // namespace
+
+extern "C" {
 
 int dg_viscous_residual(dg_ctx* c, const double* U, double* R, size_t stride, double mu, double prandtl) {
     if (!c || !U || !R) return DG_E_ARG;

@@ -47,6 +47,7 @@ struct StageArgs {
     int with_volume;      // 0 skips the volume term (eval_internals / eval_boundarys only)
     const double* dt_inst;  // optional per-instance time step (ensembles), indexed by elem_inst
     const int* elem_inst;   // [ncell] instance of each element
+    const double* Rv;       // RK stage: viscous residual subtracted from R (Navier-Stokes), or null
 };
 
 struct FaceArgs {
@@ -201,9 +202,10 @@ __global__ void __launch_bounds__(256) element_fp64(StageArgs a) {
             const double* u0 = a.U0 + (int64_t)ge * 5 * NB + 5 * j;
             const double* us = sC + e * 5 * NB + 5 * j;
             const double dt = a.dt_inst ? __ldg(a.dt_inst + __ldg(a.elem_inst + ge)) : a.dt;
+            const double* rv = a.Rv ? a.Rv + (int64_t)ge * 5 * NB + 5 * j : nullptr;
             #pragma unroll
             for (int k = 0; k < 5; ++k) {
-                const double L = -acc[k] * ib;
+                const double L = -(rv ? acc[k] - rv[k] : acc[k]) * ib;
                 o[k] = a.a0 * u0[k] + a.a1 * (us[k] + dt * L);
             }
         }
@@ -387,8 +389,10 @@ __global__ void __launch_bounds__(NT) element_fp64_fixed(StageArgs a) {
             const double* u0 = a.U0 + (int64_t)ge * B5 + 5 * j;
             const double* us = sC + e * B5 + 5 * j;
             const double dt = a.dt_inst ? __ldg(a.dt_inst + __ldg(a.elem_inst + ge)) : a.dt;
+            const double* rv = a.Rv ? a.Rv + (int64_t)ge * B5 + 5 * j : nullptr;
             #pragma unroll
-            for (int k = 0; k < 5; ++k) o[k] = a.a0 * u0[k] + a.a1 * (us[k] + dt * (-acc[k] * ib));
+            for (int k = 0; k < 5; ++k)
+                o[k] = a.a0 * u0[k] + a.a1 * (us[k] + dt * (-(rv ? acc[k] - rv[k] : acc[k]) * ib));
         }
     }
 }

@@ -139,6 +139,7 @@ struct MixedElemArgs {
     int mode;                // 0: out = R; 1: out = a0 U0 + a1 (U - dt M^-1 R)
     const double* dt_inst;   // optional per-instance time step (ensembles), indexed by elem_inst
     const int* elem_inst;    // [ncell] instance of each element
+    const double* Rv;        // RK mode: viscous residual subtracted from R (Navier-Stokes), or null
 };
 
 // ---- MMA helpers ----------------------------------------------------------------------------------
@@ -681,8 +682,8 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
         const int el = i / (5 * NB), r = i - el * (5 * NB);
         const int4 d = T.dof[r];  // j, k, hi offset, lo offset
         const int64_t e = sm.sE[el];
-        const double R = sR[(el * 5 + d.y) * LDR + d.x];
         const int64_t idx = e * (5 * NB) + r;
+        const double R = a.Rv ? sR[(el * 5 + d.y) * LDR + d.x] - a.Rv[idx] : sR[(el * 5 + d.y) * LDR + d.x];
         if (a.mode == 0) {
             a.out[idx] = R;
         } else {
@@ -739,6 +740,7 @@ struct MixedData {
     double* S0 = nullptr;
     const double* dt_inst = nullptr;  // ensembles: per-instance dt (device), else null
     const int* elem_inst = nullptr;
+    const double* Rv = nullptr;       // Navier-Stokes stepping: the stage input's viscous residual
     // A rows of the deviation coefficients of the states Un, Ua, Ub and of a residual input
     uint32_t* mir[4] = {nullptr, nullptr, nullptr, nullptr};
     // host copies the tile schedule of the persistent form is built from
@@ -968,6 +970,7 @@ inline MixedElemArgs elem_args(const MixedData& m, const double* U, const double
     ea.t = m.t; ea.ngroups = m.negroups; ea.gamma = m.gamma; ea.volume = with_volume;
     ea.dt = dt; ea.a0 = a0; ea.a1 = a1; ea.mode = mode;
     ea.dt_inst = mode == 1 ? m.dt_inst : nullptr; ea.elem_inst = m.elem_inst;
+    ea.Rv = mode == 1 ? m.Rv : nullptr;
     return ea;
 }
 

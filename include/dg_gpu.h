@@ -117,6 +117,10 @@ typedef struct dg_config {
     int limiter;     /* 0: none; 1: positivity-preserving limiter after every RK stage, bounds from
                         the stage input's values at the volume points; 2: the same with bounds from
                         the neighbours' means (PositiveLimiter<.., OnlyNeigbAvg = true>); see dg_limit */
+    double mu;       /* 0: Euler. > 0: compressible Navier-Stokes stepping: every SSP-RK3 stage adds the
+                        viscous residual of dg_viscous_residual with this viscosity, L = (R_visc -
+                        R_conv) / b as the reference's viscous driver (tests/test_diffusion.cpp:381-382) */
+    double prandtl;  /* Prandtl number of that viscous term (> 0 when mu > 0) */
 } dg_config;
 
 typedef struct dg_ctx dg_ctx;
