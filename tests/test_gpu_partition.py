@@ -42,6 +42,10 @@ CASES = [
     (dict(periodic=(1, 1, 1)), 2, dict(order=3, precision="mixed"), 1e-13),
     (dict(periodic=(1, 1, 1)), 3, dict(order=3, precision="mixed", schedule="persistent"), 1e-13),
     (dict(periodic=(1, 1, 0), bc="Pseudo3DZ"), 2, dict(order=4, precision="mixed"), 1e-13),
+    # Navier-Stokes: the viscous residual of each stage reads the exchanged ghost rows; a ghost's
+    # penalty length comes from its vertices (equal to the whole mesh's to rounding)
+    (dict(periodic=(1, 1, 0), bc="Pseudo3DZ"), 3, dict(order=2, mu=0.001, prandtl=0.72), 1e-12),
+    (dict(periodic=(1, 1, 1)), 2, dict(order=3, mu=3e-4, prandtl=0.72, precision="mixed"), 1e-12),
 ]
 
 
