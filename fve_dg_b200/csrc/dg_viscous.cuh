@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(kViscWarps * 32, 4) viscous_face(ViscArgs a) {
 }
 
 template <int NB>
-__global__ void __launch_bounds__(kViscWarps * 32) viscous_element(ViscArgs a) {
+__global__ void __launch_bounds__(kViscWarps * 32, 5) viscous_element(ViscArgs a) {
     constexpr int MT = (NB + 7) / 8;  // 8-mode tiles of the contractions
     __shared__ double sc[kViscWarps][5 * NB];
     __shared__ double sh[kViscWarps][kViscMaxQv * 15];     // per volume point: (J^T H)[d][i] w detJ
