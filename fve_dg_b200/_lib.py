@@ -79,6 +79,7 @@ def lib():
         "dg_state_device": (vp, [vp, ctypes.c_int]),
         "dg_refresh_split": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int64, vp]),
         "dg_ssprk3_stage": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int]),
+        "dg_ssprk3_stage_phase": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
         "dg_create_ensemble": (vp, [ctypes.POINTER(MeshDesc), ctypes.c_int, ctypes.POINTER(Config), c_int_p]),
         "dg_ensemble_offsets": (ctypes.c_int, [vp, c_int64_p]),
         "dg_ssprk3_ensemble": (ctypes.c_int, [vp, c_double_p, ctypes.c_int, ctypes.c_int]),
@@ -115,7 +116,7 @@ def exported_symbols():
     return ["dg_create", "dg_destroy", "dg_residual", "dg_residual_device", "dg_residual_device_static",
             "dg_static_scratch_capacity", "dg_set_state", "dg_get_state",
             "dg_ssprk3", "dg_ssprk3_graph", "dg_ssprk3_timed", "dg_stream", "dg_state_device",
-            "dg_refresh_split", "dg_ssprk3_stage", "dg_create_ensemble",
+            "dg_refresh_split", "dg_ssprk3_stage", "dg_ssprk3_stage_phase", "dg_create_ensemble",
             "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_mass", "dg_limit", "dg_limit_device", "dg_viscous_residual", "dg_viscous_residual_device",
             "dg_save_checkpoint", "dg_load_checkpoint",
             "dg_set_dirichlet", "dg_conservation",

@@ -408,6 +408,29 @@ int step(dg_ctx* c, double dt, cudaStream_t s, int st0 = 0, int st1 = 3) {
     return step_fp64(c, dt, s, st0, st1);
 }
 
+// Stage st of the mixed two-launch form in two phases around a halo exchange (a mesh with ghost
+// elements): phase 0 the fluxes of the faces between owned elements, which read no ghost row;
+// phase 1 the viscous residual, the faces touching ghosts, the element kernel and the limiter.
+// Together they launch what step() launches for the stage, with the same arguments.
+int stage_phase_mixed(dg_ctx* c, double dt, int st, int phase, cudaStream_t s) {
+    if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
+    MixedData& m = c->mixed;
+    const double A0[3] = {0.0, 0.75, 1.0 / 3.0};
+    const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
+    const double* in[3] = {c->d_Un, c->d_Ua, c->d_Ub};
+    double* out[3] = {c->d_Ua, c->d_Ub, c->d_Un};
+    const int mi = st, mo = (st + 1) % 3;
+    auto K = [&](int which, int g0, int g1) {
+        return mixed_kernel(m, which, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, &g_launches, mi, mo,
+                            g0, g1);
+    };
+    if (phase == 0) return timed(c, 0, s, [&] { return K(0, 0, m.nfgroups_inner); });
+    int rc = viscous_stage(c, in[st], s);
+    if (rc || (rc = timed(c, 0, s, [&] { return K(0, m.nfgroups_inner, m.nfgroups); }))) return rc;
+    if ((rc = timed(c, 1, s, [&] { return K(1, 0, -1); }))) return rc;
+    return limit_stage(c, st, in[st], out[st], m.mir[mo], s);
+}
+
 int launches_per_step(const dg_ctx* c) {
     const int lim = (c->cfg.limiter ? (c->nowned < c->ncell ? 6 : 3) : 0) + (c->cfg.mu > 0.0 ? 6 : 0);
     if (c->cfg.precision == DG_PREC_MIXED) return (c->cfg.schedule == 1 ? 3 : mixed_launches_per_step(c->mixed)) + lim;
@@ -604,7 +627,11 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
         c->mixed.elem_inst = c->d_elem_inst;
         if (cudaMalloc((void**)&c->d_queue, sizeof(QueueState)) != cudaSuccess) return fail(c, DG_E_NOMEM);
         if (cudaMemset(c->d_queue, 0, sizeof(QueueState)) != cudaSuccess) return fail(c, DG_E_CUDA);
-        if ((rc = build_schedule(c->mixed, c->qs, c->pp))) return fail(c, rc);
+        // the region order of the face groups (the persistent schedule's tiles; the two-launch face
+        // kernel runs them in any order), except where a two-launch context with ghost elements keeps
+        // the faces between owned elements first (dg_ssprk3_stage_phase)
+        if (cfg->schedule == 1 || c->nowned == c->ncell)
+            if ((rc = build_schedule(c->mixed, c->qs, c->pp))) return fail(c, rc);
     }
     {
         int dev = 0, sms = 148;
@@ -965,6 +992,15 @@ int dg_refresh_split(dg_ctx* c, int which, const int64_t* elems, int64_t n, void
     DG_CUDA(cudaSetDevice(c->cfg.device));
     const cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     return mixed_mirror_list(c->mixed, dg_state_device(c, which), which, elems, n, s, &g_launches);
+}
+
+int dg_ssprk3_stage_phase(dg_ctx* c, double dt, int stage, int phase) {
+    if (!c || stage < 0 || stage > 2 || phase < 0 || phase > 1 || !(dt >= 0)) return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    const bool split = c->cfg.precision == DG_PREC_MIXED && c->cfg.schedule == 0 && c->nowned < c->ncell;
+    if (!split) return phase == 0 ? DG_OK : step(c, dt, c->stream, stage, stage + 1);
+    return stage_phase_mixed(c, dt, stage, phase, c->stream);
 }
 
 int dg_ssprk3_stage(dg_ctx* c, double dt, int stage) {

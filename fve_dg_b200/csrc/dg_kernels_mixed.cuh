@@ -724,6 +724,7 @@ struct MixedData {
     int order = 0, qv = 0, qf = 0, nb = 0, nqv = 0, nqf = 0;
     int64_t ncell = 0, nface = 0;
     int nfgroups = 0, negroups = 0;
+    int nfgroups_inner = 0;  // face groups [0, nfgroups_inner) touch no ghost element
     float gamma = 1.4f;
     int flux = 0;
     int sms = 148;
@@ -826,21 +827,28 @@ inline void append_frag_table(const std::vector<double>& T, int N, int K, std::v
 // order: local face q is the one opposite local vertex q) are grouped in threes, in mesh order.
 // A partial group repeats its first member in the unused slots (never read as a row: rows of
 // unused slots are masked by the group size).
+// Face groups: faces of the same kind in threes, first the faces between owned elements, then
+// (from *nf_inner on) the faces touching a ghost element (cells >= ncell), whose fluxes need the
+// ghost rows of a halo exchange. Element groups: the owned elements [0, ncell).
 inline void build_groups(const std::vector<FaceInfo>& hfi, const std::vector<ElemFace>& hef, int64_t ncell,
-                         std::vector<FaceGroup>& fg, std::vector<ElemGroup>& eg) {
-    std::map<int64_t, FaceGroup> open_f;
-    for (int64_t f = 0; f < (int64_t)hfi.size(); ++f) {
-        const FaceInfo& F = hfi[f];
-        const int64_t key = (int64_t)(F.meta & 0xffffff) * 2 + (F.c1 >= 0 ? 1 : 0);
-        FaceGroup& g = open_f[key];
-        g.f[g.n++] = (int)f;
-        if (g.n == 3) { fg.push_back(g); g = FaceGroup{}; }
-    }
-    for (auto& kv : open_f)
-        if (kv.second.n > 0) {
-            for (int i = kv.second.n; i < 3; ++i) kv.second.f[i] = kv.second.f[0];
-            fg.push_back(kv.second);
+                         std::vector<FaceGroup>& fg, std::vector<ElemGroup>& eg, int* nf_inner) {
+    for (int halo = 0; halo < 2; ++halo) {
+        std::map<int64_t, FaceGroup> open_f;
+        for (int64_t f = 0; f < (int64_t)hfi.size(); ++f) {
+            const FaceInfo& F = hfi[f];
+            if ((F.c0 >= ncell || F.c1 >= ncell) != (halo == 1)) continue;
+            const int64_t key = (int64_t)(F.meta & 0xffffff) * 2 + (F.c1 >= 0 ? 1 : 0);
+            FaceGroup& g = open_f[key];
+            g.f[g.n++] = (int)f;
+            if (g.n == 3) { fg.push_back(g); g = FaceGroup{}; }
         }
+        for (auto& kv : open_f)
+            if (kv.second.n > 0) {
+                for (int i = kv.second.n; i < 3; ++i) kv.second.f[i] = kv.second.f[0];
+                fg.push_back(kv.second);
+            }
+        if (halo == 0) *nf_inner = (int)fg.size();
+    }
     std::map<std::vector<int>, ElemGroup> open_e;
     for (int64_t e = 0; e < ncell; ++e) {
         int face[4] = {-1, -1, -1, -1}, meta[4] = {0, 0, 0, 0};
@@ -921,7 +929,7 @@ inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>
         return rc;
     std::vector<FaceGroup> fg;
     std::vector<ElemGroup> eg;
-    build_groups(hfi, hef, nowned, fg, eg);  // element groups over owned cells only (no ghosts)
+    build_groups(hfi, hef, nowned, fg, eg, &m.nfgroups_inner);  // element groups: owned cells only
     m.nfgroups = (int)fg.size();
     m.negroups = (int)eg.size();
     if ((rc = mixed_upload(m, &m.fgroups, fg)) || (rc = mixed_upload(m, &m.egroups, eg))) return rc;
@@ -954,10 +962,15 @@ inline void free_mixed(MixedData& m) {
 
 inline void set_mixed_dirichlet(MixedData& m, const double* UD) { m.UD = UD; }
 
-inline MixedFaceArgs face_args(const MixedData& m, const double* U, int mir_in, int face_mask) {
+inline MixedFaceArgs face_args(const MixedData& m, const double* U, int mir_in, int face_mask, int g0 = 0,
+                               int g1 = -1) {
     MixedFaceArgs fa;
     fa.U = U; fa.mir = m.mir[mir_in]; fa.fi = m.fi; fa.groups = m.fgroups; fa.UD = m.UD; fa.dev = m.dev;
     fa.Fref = m.Fref; fa.S0 = m.S0; fa.t = m.t; fa.ngroups = m.nfgroups; fa.gamma = m.gamma; fa.flux = m.flux;
+    if (g1 >= 0) {  // face groups [g0, g1) only
+        fa.groups = m.fgroups + g0;
+        fa.ngroups = g1 - g0;
+    }
     fa.faces_mask = face_mask;
     return fa;
 }
@@ -991,14 +1004,15 @@ inline int ensure_smem(Kernel k, size_t smem, unsigned long long& done_mask) {
 template <int NB, int NQV, int NQF, int WE>
 inline int mixed_launch(MixedData& m, int which, const double* U, const double* U0, double* out, int mode,
                         double dt, double a0, double a1, int face_mask, int with_volume, cudaStream_t s,
-                        int mir_in, int mir_out) {
+                        int mir_in, int mir_out, int g0, int g1) {
     if (which == 4) {
         const int64_t n = m.ncell * 5 * (pad8(NB - 1) / 2);
         mirror_split<NB><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(U, m.mir[mir_in], m.ncell, nullptr);
     } else if (which == 0) {
         constexpr int W = 4;  // 4-warp CTAs: finer-grained scheduling than 8 at the same occupancy
-        const int g = (int)std::min<int64_t>((m.nfgroups + W - 1) / W, (int64_t)m.sms * 64);
-        face_flux_mixed<NB, NQF, W><<<g, W * 32, 0, s>>>(face_args(m, U, mir_in, face_mask));
+        const int n = g1 < 0 ? m.nfgroups : g1 - g0;
+        const int g = (int)std::min<int64_t>((n + W - 1) / W, (int64_t)m.sms * 64);
+        face_flux_mixed<NB, NQF, W><<<g, W * 32, 0, s>>>(face_args(m, U, mir_in, face_mask, g0, g1));
     } else {
         constexpr size_t smem = sizeof(ElemMixedSmem<NB, NQV, NQF>) * WE;
         static unsigned long long done = 0;
@@ -1012,15 +1026,17 @@ inline int mixed_launch(MixedData& m, int which, const double* U, const double* 
 }
 
 // mir_in: mirror of U (0..3); mir_out: mirror the update writes (RK mode), or -1.
+// Face launches (which 0) cover face groups [g0, g1) (g1 < 0: all of them).
 inline int mixed_kernel(MixedData& m, int which, const double* U, const double* U0, double* out, int mode,
                         double dt, double a0, double a1, int face_mask, int with_volume, cudaStream_t s,
-                        std::atomic<int64_t>* launches, int mir_in, int mir_out) {
+                        std::atomic<int64_t>* launches, int mir_in, int mir_out, int g0 = 0, int g1 = -1) {
     if (!m.ready) return DG_E_ARG;
+    if (which == 0 && g1 >= 0 && g1 <= g0) return DG_OK;  // an empty range: nothing to launch
     ++*launches;
 #define X(P, QV, QF, NB, NQV, NQF, W)                                                                           \
     if (m.order == P && m.qv == QV && m.qf == QF)                                                               \
         return mixed_launch<NB, NQV, NQF, W>(m, which, U, U0, out, mode, dt, a0, a1, face_mask, with_volume, s, \
-                                             mir_in, mir_out);
+                                             mir_in, mir_out, g0, g1);
     FVEDG_MIXED_COMBOS(X)
 #undef X
     return DG_E_ARG;

@@ -138,7 +138,7 @@ class PartitionedConvection:
         self.dist, self._exchange, self.device = dist, exchange, device
         self.mixed = self.conv.precision == "mixed"
         self._ghost_dev = None
-        self._idx = None
+        self._comm = None  # the exchange's stream when it overlaps the stage's first phase
 
     def torch_stream(self):
         import torch
@@ -183,15 +183,47 @@ class PartitionedConvection:
     def stage(self, dt, st):
         L.check(L.lib().dg_ssprk3_stage(self.conv._ctx, float(dt), int(st)), "dg_ssprk3_stage")
 
+    def phase(self, dt, st, ph):
+        """Phase 0 of stage st reads no ghost row (the faces between owned elements), phase 1 is the
+        rest (dg_ssprk3_stage_phase)."""
+        L.check(L.lib().dg_ssprk3_stage_phase(self.conv._ctx, float(dt), int(st), int(ph)),
+                "dg_ssprk3_stage_phase")
+
+    def overlapped_stage(self, dt, st):
+        """Stage st with the halo exchange of its input on a second stream, concurrent with phase 0
+        on the context's stream; phase 1 waits for the exchange (CUDA events, no host wait)."""
+        import torch
+        main = self.torch_stream()
+        if self._comm is None:
+            self._comm = torch.cuda.Stream(device=torch.device("cuda", self.device))
+        ready = torch.cuda.Event()
+        ready.record(main)              # the stage input is complete
+        self.phase(dt, st, 0)
+        self._comm.wait_event(ready)
+        with torch.cuda.stream(self._comm):
+            if self._exchange is not None:
+                self._exchange(st)
+            else:
+                halo_exchange(self.state_view(st), self.lm, self.dist)
+        done = torch.cuda.Event()
+        done.record(self._comm)
+        main.wait_event(done)
+        self._refresh(st)
+        self.phase(dt, st, 1)
+
     def wait(self):
         """Wait for the context's stream; reports a watchdog error of the persistent schedule."""
         L.check(L.lib().dg_ssprk3(self.conv._ctx, 0.0, 0), "dg_ssprk3")
 
-    def ssprk3(self, dt, nsteps=1):
+    def ssprk3(self, dt, nsteps=1, overlap=True):
+        """SSP-RK3 steps; with overlap the exchange of each stage runs beside its first phase."""
         for _ in range(nsteps):
             for st in range(3):
-                self.exchange(st)
-                self.stage(dt, st)
+                if overlap:
+                    self.overlapped_stage(dt, st)
+                else:
+                    self.exchange(st)
+                    self.stage(dt, st)
         self.wait()
 
 
@@ -218,16 +250,23 @@ def emulated_ranks(mesh, nparts, **kw):
     return ranks
 
 
-def step_emulated(ranks, dt, nsteps=1):
-    """SSP-RK3 on emulated ranks: all parts finish a stage before any exchange reads it."""
+def step_emulated(ranks, dt, nsteps=1, phased=False):
+    """SSP-RK3 on emulated ranks: all parts finish a stage before any exchange reads it. phased
+    runs each stage as its two phases with the exchange between them."""
     import torch
     for _ in range(nsteps):
         for st in range(3):
             torch.cuda.synchronize()
+            if phased:
+                for r in ranks:
+                    r.phase(dt, st, 0)
             for r in ranks:
                 r.exchange(st)
             torch.cuda.synchronize()
             for r in ranks:
-                r.stage(dt, st)
+                if phased:
+                    r.phase(dt, st, 1)
+                else:
+                    r.stage(dt, st)
     for r in ranks:
         r.wait()

@@ -203,6 +203,11 @@ int dg_refresh_split(dg_ctx* ctx, int which, const int64_t* elems_dev, int64_t n
  * context's stream and returns; dg_ssprk3(ctx, dt, 0) waits for it and reports a watchdog error.
  * Run the stages of a step in order 0, 1, 2; between them, write only ghost rows from outside. */
 int dg_ssprk3_stage(dg_ctx* ctx, double dt, int stage);
+/* The same stage in two phases, so that a halo exchange overlaps work: phase 0 enqueues what reads
+ * no ghost row (in the mixed two-launch form, the fluxes of the faces between owned elements;
+ * otherwise nothing), phase 1 the rest. Between them, write the ghost rows of the stage input (and
+ * call dg_refresh_split); phases 0 then 1 launch exactly what dg_ssprk3_stage launches. */
+int dg_ssprk3_stage_phase(dg_ctx* ctx, double dt, int stage, int phase);
 
 /* Explicit viscous operator, replaces ExplicitDiffusion<Order, QuadC, QuadF>::eval(mesh, U, t)
  * (include/DG/DG_Schemes/ExplicitDiffusion.h:133-626) with the context's order and rules: the
