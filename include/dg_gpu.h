@@ -182,8 +182,10 @@ int dg_ssprk3_ensemble(dg_ctx* ctx, const double* dt, int nsteps, int use_graph)
 int dg_autotune(dg_ctx* ctx, double dt, char* report, size_t len);
 
 /* Same as dg_ssprk3, with CUDA events around every kernel launch on the context's stream.
- * out[2k] = total milliseconds and out[2k+1] = launch count of kernel class k < nclass
- * (FP64 form: 0 = face flux, 1 = element volume/lift/update; mixed form: see DESIGN). */
+ * out[2k] = total milliseconds and out[2k+1] = launch count of kernel class k < nclass:
+ * 0 = face fluxes, 1 = element kernel (volume, face integrals, update), 2 = the persistent stage
+ * kernel (mixed form, persistent schedule), 3 = viscous residual (Navier-Stokes stepping),
+ * 4 = limiter. */
 int dg_ssprk3_timed(dg_ctx* ctx, double dt, int nsteps, double* out, int nclass);
 /* The context's CUDA stream (a cudaStream_t) on which every kernel of the context runs. */
 void* dg_stream(dg_ctx* ctx);
@@ -217,8 +219,10 @@ int dg_ssprk3_stage_phase(dg_ctx* ctx, double dt, int stage, int phase);
  * data of dg_set_dirichlet. Host buffers with the element stride of dg_residual. */
 int dg_viscous_residual(dg_ctx* ctx, const double* U, double* R, size_t elem_stride_bytes, double mu, double prandtl);
 /* Same on device buffers, enqueued on `stream` (a cudaStream_t, 0 = default). The first call on a
- * context allocates the operator's per-face buffer (nface * 6 * nqf doubles) and its tables; calls
- * on one context share that buffer, so calls whose kernels could overlap must be serialised. */
+ * context allocates the operator's per-face buffer (nface * (5 nqf + Nb) doubles) and its tables (a
+ * context with dg_config.mu > 0 has them from its creation); calls on one context share that buffer,
+ * so calls whose kernels could overlap, and Navier-Stokes steps of the same context, must be
+ * serialised with them. */
 int dg_viscous_residual_device(dg_ctx* ctx, const double* U_dev, double* R_dev, double mu, double prandtl,
                                void* stream);
 
