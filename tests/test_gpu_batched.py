@@ -71,3 +71,25 @@ def test_autotune_records_and_restores():
     assert rep["chosen"]["ms_per_step"] == min(x["ms_per_step"] for x in rep["candidates"])
     c.ssprk3(1e-3, 2)  # the chosen tiles run
     assert c.check_state() == 0
+
+
+@pytest.mark.parametrize("extra", [dict(mu=0.05, prandtl=0.72), dict(mu=0.05, prandtl=0.72, limiter="positive")])
+def test_ensemble_navier_stokes_matches_separate_solves(extra):
+    """Navier-Stokes stepping (and the limiter) in an ensemble: each instance, with its own dt,
+    steps exactly as it does alone."""
+    P, qv, qf = 2, 1, 2
+    sizes = [3, 4]
+    parts = [vortex_mesh_state(n, P, 20 + i) for i, n in enumerate(sizes)]
+    dts = np.array([1e-3, 1.5e-3])
+    for prec, sched in (("mixed", "two-launch"), ("fp64", "two-launch"), ("mixed", "persistent")):
+        ens = Ensemble([m for m, _ in parts], order=P, quad_vol=qv, quad_face=qf, precision=prec, schedule=sched,
+                       **extra)
+        ens.set_state(np.concatenate([U for _, U in parts]))
+        ens.ssprk3(dts, 3, graph=True)
+        got = ens.split(ens.get_state())
+        for i, (m, U) in enumerate(parts):
+            one = ExplicitConvection(m, order=P, quad_vol=qv, quad_face=qf, precision=prec, schedule=sched, **extra)
+            one.set_state(U)
+            one.ssprk3(dts[i], 3)
+            assert np.all(np.isfinite(got[i]))
+            assert np.array_equal(got[i], one.get_state()), (prec, sched, i)
