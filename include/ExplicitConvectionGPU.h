@@ -59,8 +59,9 @@ class ExplicitConvectionGPU {
 public:
     static constexpr uInt N = Basis::NumBasis;
 
-    explicit ExplicitConvectionGPU(int device = 0, int precision = DG_PREC_FP64, int flux = DG_FLUX_LF)
-        : device_(device), precision_(precision), flux_(flux) {}
+    explicit ExplicitConvectionGPU(int device = 0, int precision = DG_PREC_FP64, int flux = DG_FLUX_LF,
+                                   double gamma = Flux::gamma)
+        : device_(device), precision_(precision), flux_(flux), gamma_(gamma) {}
     ~ExplicitConvectionGPU() { release(); }
     ExplicitConvectionGPU(const ExplicitConvectionGPU&) = delete;
     ExplicitConvectionGPU& operator=(const ExplicitConvectionGPU&) = delete;
@@ -79,9 +80,16 @@ public:
     }
 
     dg_ctx* context() { return ctx_; }
+    // The context for `mesh` (made on the first call for a mesh) with the Dirichlet data at time t:
+    // what eval does before it evaluates; ExplicitDiffusionGPU and PositiveLimiterGPU use it.
+    void prepare(const ComputingMesh& mesh, Scalar t = 0.0) {
+        if (!ctx_ || mesh_ != &mesh) upload(mesh);
+        dirichlet(mesh, t);
+    }
 
 private:
     int device_, precision_, flux_;
+    double gamma_;
     dg_ctx* ctx_ = nullptr;
     const ComputingMesh* mesh_ = nullptr;
     std::vector<int64_t> dirichlet_faces_;
@@ -131,7 +139,7 @@ private:
         cfg.flux = flux_;
         cfg.quad_vol = kVol;
         cfg.quad_face = kFace;
-        cfg.gamma = Flux::gamma;
+        cfg.gamma = gamma_;
         cfg.precision = precision_;
         cfg.device = device_;
         int err = DG_OK;
@@ -165,8 +173,7 @@ private:
     }
 
     LongVector<5 * N> run(const ComputingMesh& mesh, const LongVector<5 * N>& U, Scalar t, int part) {
-        if (!ctx_ || mesh_ != &mesh) upload(mesh);
-        dirichlet(mesh, t);
+        prepare(mesh, t);
         LongVector<5 * N> R(U.size());
         if (U.size() == 0) return R;
         fvedg_adaptor::check(dg_residual(ctx_, U[0].data_ptr(), R[0].data_ptr(), sizeof(DenseMatrix<5 * N, 1>), t, part),

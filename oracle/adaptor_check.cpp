@@ -1,15 +1,20 @@
-// Test infrastructure: compiles the C++ drop-in include/ExplicitConvectionGPU.h against the
-// reference's own headers and checks it against the reference's ExplicitConvection on the same
-// ComputingMesh, the way a driver would swap the class. Built by `make -C oracle ref` into
+// Test infrastructure: compiles the C++ drop-ins include/ExplicitConvectionGPU.h,
+// ExplicitDiffusionGPU.h and PositiveLimiterGPU.h against the reference's own headers and checks
+// them against the reference's ExplicitConvection, ExplicitDiffusion and PositiveLimiter on the same
+// ComputingMesh, the way a driver would swap the classes. Built by `make -C oracle ref` into
 // oracle/_ref/adaptor_check (linked to fve_dg_b200/libfvedg_b200.so); run by
 // tests/test_gpu_adaptor.py on a GPU. Exit status 0 when every case agrees to 1e-12 (relative L2).
 #include "DG/DG_Schemes/ExplicitConvection.h"
+#include "DG/DG_Schemes/ExplicitDiffusion.h"
+#include "DG/DG_Schemes/PositiveLimiter.h"
 #include "src/DG/DG_Schemes/ExplicitConvection.cpp"
 
 #include <cstdio>
 #include <random>
 
 #include "ExplicitConvectionGPU.h"
+#include "ExplicitDiffusionGPU.h"
+#include "PositiveLimiterGPU.h"
 
 // Problem hooks of include/base/exact.h:32-52 (a travelling density wave) for Dirichlet faces.
 namespace {
@@ -92,6 +97,66 @@ static int check(const ComputingMesh& m, const char* name) {
     return bad;
 }
 
+template <uInt N>
+static double rel_l2(const LongVector<5 * N>& a, const LongVector<5 * N>& b) {
+    double num = 0, den = 0;
+    for (size_t c = 0; c < a.size(); ++c)
+        for (uInt i = 0; i < 5 * N; ++i) {
+            const double d = a[c](i, 0) - b[c](i, 0);
+            num += d * d;
+            den += a[c](i, 0) * a[c](i, 0);
+        }
+    return den > 0 ? std::sqrt(num / den) : std::sqrt(num);
+}
+
+// ExplicitDiffusionGPU against ExplicitDiffusion (mu = Pr = 1, as the reference fixes them).
+template <uInt P, class QC, class QF>
+static int check_diffusion(const ComputingMesh& m, const char* name) {
+    constexpr uInt N = DGBasisEvaluator<P>::NumBasis;
+    LongVector<5 * N> U(m.m_cells.size());
+    std::mt19937_64 rng(P * 29 + 5);
+    std::uniform_real_distribution<double> uni(-1e-2, 1e-2);
+    for (size_t c = 0; c < m.m_cells.size(); ++c) {
+        U[c](0, 0) = 1.0;
+        U[c](4, 0) = 2.5;
+        for (uInt i = 0; i < 5 * N; ++i) U[c](i, 0) += uni(rng);
+    }
+    ExplicitDiffusion<P, QC, QF> ref;
+    ExplicitDiffusionGPU<P, QC, QF> gpu;
+    const double t = 0.125;
+    const double rel = rel_l2<N>(ref.eval(m, U, t), gpu.eval(m, U, t));
+    std::printf("%s diffusion P%d rel L2 %.3e\n", name, (int)P, rel);
+    return rel < 1e-12 ? 0 : 1;
+}
+
+// PositiveLimiterGPU against PositiveLimiter: constructMinMax(current, previous), apply(current,
+// previous) on a state whose modes leave the bounds and whose points go non-physical.
+template <uInt P, class QC, bool Avg>
+static int check_limiter(const ComputingMesh& m, const char* name) {
+    constexpr uInt N = DGBasisEvaluator<P>::NumBasis;
+    const size_t nc = m.m_cells.size();
+    LongVector<5 * N> prev(nc), cur(nc);
+    std::mt19937_64 rng(P * 31 + (Avg ? 7 : 3));
+    std::uniform_real_distribution<double> uni(-1.0, 1.0);
+    for (size_t c = 0; c < nc; ++c) {
+        prev[c](0, 0) = 1.0 + 0.05 * uni(rng);
+        prev[c](4, 0) = 2.5 + 0.05 * uni(rng);
+        for (uInt i = 5; i < 5 * N; ++i) prev[c](i, 0) = 0.01 * uni(rng);
+        cur[c] = prev[c];
+        for (uInt i = 5; i < 5 * N; ++i) cur[c](i, 0) += 0.4 * uni(rng);
+    }
+    LongVector<5 * N> a = cur, b = cur;
+    PositiveLimiter<P, QC, Avg> ref(m, 1.4);
+    ref.constructMinMax(a, prev);
+    ref.apply(a, prev);
+    PositiveLimiterGPU<P, QC, Avg> gpu(m, 1.4);
+    gpu.constructMinMax(b, prev);
+    gpu.apply(b, prev);
+    const double rel = rel_l2<N>(a, b), acted = rel_l2<N>(a, cur);
+    std::printf("%s limiter P%d avg %d rel L2 %.3e (limited vs input %.3e)\n", name, (int)P, (int)Avg, rel, acted);
+    return (rel < 1e-12 && acted > 1e-3) ? 0 : 1;
+}
+
 int main() {
     int bad = 0;
     for (BoundaryType bt : {BoundaryType::Dirichlet, BoundaryType::Pseudo3DZ}) {
@@ -103,6 +168,12 @@ int main() {
         bad += check<3, T::Degree6Points23, F::Degree10Points24>(*m, name);
         bad += check<4, T::Degree8Points44, F::Degree10Points24>(*m, name);
         bad += check<3, GaussLegendreTet::Auto, GaussLegendreTri::Auto>(*m, name);
+        bad += check_diffusion<1, T::Degree2Points4, F::Degree3Points6>(*m, name);
+        bad += check_diffusion<2, T::Degree4Points11, F::Degree4Points7>(*m, name);
+        bad += check_diffusion<3, T::Degree6Points23, F::Degree10Points24>(*m, name);
+        bad += check_limiter<2, T::Degree4Points11, false>(*m, name);
+        bad += check_limiter<3, T::Degree6Points23, false>(*m, name);
+        bad += check_limiter<3, T::Degree6Points23, true>(*m, name);
         delete m;
     }
     std::printf("%s\n", bad ? "FAIL" : "OK");

@@ -1,6 +1,10 @@
-"""GPU: the C++ drop-in ExplicitConvectionGPU (include/ExplicitConvectionGPU.h), compiled against
-the reference's headers, against the reference's own ExplicitConvection on the same ComputingMesh
-(Dirichlet and Pseudo3DZ boundaries, P1..P4, eval and its three parts)."""
+"""GPU: the C++ drop-ins, compiled against the reference's headers, against the reference's own
+classes on the same ComputingMesh (Dirichlet and Pseudo3DZ boundaries):
+- ExplicitConvectionGPU (include/ExplicitConvectionGPU.h) against ExplicitConvection: P1..P4, eval
+  and its three parts;
+- ExplicitDiffusionGPU (include/ExplicitDiffusionGPU.h) against ExplicitDiffusion: P1..P3;
+- PositiveLimiterGPU (include/PositiveLimiterGPU.h) against PositiveLimiter: P2, P3, both bound
+  modes, on states the limiter changes."""
 import os
 import subprocess
 
@@ -16,4 +20,6 @@ def test_cpp_drop_in_matches_reference():
     r = subprocess.run([BIN], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.strip().endswith("OK")
-    assert r.stdout.count("rel L2") == 2 * 5 * 4
+    assert r.stdout.count(" part ") == 2 * 5 * 4
+    assert r.stdout.count(" diffusion ") == 2 * 3
+    assert r.stdout.count(" limiter ") == 2 * 3
