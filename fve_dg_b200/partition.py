@@ -164,9 +164,10 @@ class PartitionedConvection:
         if not self.mixed or not len(self.lm.ghosts):
             return
         import torch
-        if self._ghost_dev is None:
-            self._ghost_dev = torch.arange(self.lm.n_owned, self.lm.ncell, dtype=torch.int64,
-                                           device=torch.device("cuda", self.device))
+        if self._ghost_dev is None:  # made on the context's stream, which the refresh then runs on
+            with torch.cuda.stream(self.torch_stream()):
+                self._ghost_dev = torch.arange(self.lm.n_owned, self.lm.ncell, dtype=torch.int64,
+                                               device=torch.device("cuda", self.device))
         L.check(L.lib().dg_refresh_split(self.conv._ctx, int(which), ctypes.c_void_p(self._ghost_dev.data_ptr()),
                                          int(self._ghost_dev.numel()), None), "dg_refresh_split")
 
