@@ -551,6 +551,12 @@ def run_viscous(args, cfg, rank, world, local, dist):
         face_block = 8 * (5 * conv.nq_face + nb)
         bytes_each = 3 * dof * 8 + 3 * m.nface * face_block + m.ncell * (80 + 8 + 32) + m.nface * 48 * 2
         peak, peak_kind = read_peaks()
+        traffic = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+                traffic = json.load(f).get(args.config, {}).get("viscous")
+        except Exception:
+            pass
         line = {"metric": "viscous residual DOF evaluations/s", "value": value, "unit": "DOF-residual/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_each,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -561,7 +567,7 @@ def run_viscous(args, cfg, rank, world, local, dist):
                 "roofline": {"bound": "hbm", "kernel": "viscous_face + viscous_element",
                              "achieved": bytes_each / (ms_each / 1e3) / 1e9,
                              "peak": peak, "unit": "GB/s", "frac": bytes_each / (ms_each / 1e3) / 1e9 / peak,
-                             "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": bytes_each,
+                             "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": bytes_each,
                              "note": "FP64 traces and contractions (on the FP64 tensor cores) per face and per "
                                      "element: bound by instruction issue and latency, not by HBM"},
                 "cpu_baseline": cpu,
