@@ -220,6 +220,17 @@ __global__ void __launch_bounds__(kViscWarps * 32, 4) viscous_face(ViscArgs a) {
     const double beta_base = (double)((a.order + 1) * (a.order + 1));
     for (int64_t f = (int64_t)blockIdx.x * kViscWarps + w; f < a.nface; f += (int64_t)gridDim.x * kViscWarps) {
         const FaceInfo F = a.fi[f];
+        {   // the next face's state rows into L2 while this face is computed
+            constexpr int NL = (5 * NB * 8 + 127) / 128;
+            const int64_t fn = f + (int64_t)gridDim.x * kViscWarps;
+            if (fn < a.nface && lane < 2 * NL) {
+                const int side = lane / NL, part = lane - side * NL;
+                const int64_t cn = side ? a.fi[fn].c1 : a.fi[fn].c0;
+                if (cn >= 0)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(
+                        reinterpret_cast<const char*>(a.U + cn * (5 * NB)) + part * 128));
+            }
+        }
         if (!visc_face_active(F, a.UD)) continue;  // warp-uniform
         const bool interior = F.c1 >= 0;
         const int bc = (F.meta >> 16) & 0xff;
