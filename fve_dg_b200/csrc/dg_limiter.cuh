@@ -195,6 +195,14 @@ __global__ void __launch_bounds__(kLimWarps * 32)
     for (int64_t e0 = ((int64_t)blockIdx.x * kLimWarps + w) * CPW; e0 < ncell;
          e0 += (int64_t)gridDim.x * kLimWarps * CPW) {
         const int nc = (int)(ncell - e0 < CPW ? ncell - e0 : CPW);
+        {   // the next iteration's cells into L2 while these are limited
+            const int64_t en = e0 + (int64_t)gridDim.x * kLimWarps * CPW;
+            if (en < ncell) {
+                const int64_t bytes = (ncell - en < CPW ? ncell - en : CPW) * (5 * NB * 8);
+                for (int64_t off = (int64_t)lane * 128; off < bytes; off += 32 * 128)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char*>(U + en * (5 * NB)) + off));
+            }
+        }
         const double* ug0 = U + e0 * (5 * NB);
         for (int i = lane; i < nc * 5 * NB; i += 32) scoef[w][i] = ug0[i];  // the warp's cells, coalesced
         __syncwarp();
