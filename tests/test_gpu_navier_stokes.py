@@ -30,9 +30,11 @@ def cpu_ns_ssprk3(m, U0, P, qv, qf, dt, nsteps):
 
 
 @pytest.mark.skipif(not ref_available(), reason="reference library not built")
-@pytest.mark.parametrize("P,qv,qf", [(1, 0, 1), (2, 1, 2), (3, 3, 3)])
-def test_navier_stokes_stepping_matches_reference_loop(P, qv, qf):
-    m = box_mesh(4, jitter=0.1, seed=31)
+@pytest.mark.parametrize("P,qv,qf,walls", [(1, 0, 1, False), (2, 1, 2, False), (3, 3, 3, False), (2, 1, 2, True)])
+def test_navier_stokes_stepping_matches_reference_loop(P, qv, qf, walls):
+    """walls: Pseudo3DZ boundary faces in z (their viscous and convective terms), else periodic."""
+    m = (box_mesh(4, jitter=0.1, seed=33, periodic=(1, 1, 0), bc="Pseudo3DZ") if walls
+         else box_mesh(4, jitter=0.1, seed=31))
     U0 = problems.project(m, P, problems.density_wave(A=0.2, vel=(1.0, 0.5, 0.25)))
     dt, nsteps = 2e-5, 3
     want = cpu_ns_ssprk3(m, U0, P, qv, qf, dt, nsteps)
