@@ -91,12 +91,12 @@ struct ViscState {  // what K needs of the state it is taken at
 
 __device__ __forceinline__ ViscState visc_state(const double U[5]) {
     ViscState s;
-    const double rho = U[0] > 1e-8 ? U[0] : 1e-8;
-    s.irho = 1.0 / rho;
-    s.u[0] = U[1] / U[0];
-    s.u[1] = U[2] / U[0];
-    s.u[2] = U[3] / U[0];
-    s.e = U[4] / U[0];
+    const double inv = 1.0 / U[0];  // one division: the quotients below to within an ulp
+    s.irho = U[0] > 1e-8 ? inv : 1e8;
+    s.u[0] = U[1] * inv;
+    s.u[1] = U[2] * inv;
+    s.u[2] = U[3] * inv;
+    s.e = U[4] * inv;
     return s;
 }
 
