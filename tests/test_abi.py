@@ -118,3 +118,28 @@ def test_malformed_meshes_are_rejected():
     bad = Mesh(m.points, m.cells, m.faces, m.face_cells, m.face_nodes1, m.periodic, m.bc, geometry=geo)
     with pytest.raises(L.DGError):
         bad.face_perms()
+
+
+def test_c_header_compiles_as_c_and_links():
+    """include/dg_gpu.h is plain C: a C program that includes it and takes the address of every
+    entry point compiles with gcc (C11) and links against the library, as an FFI consumer would."""
+    import re
+    import shutil
+    import subprocess
+    import tempfile
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = open(os.path.join(root, "include", "dg_gpu.h")).read()
+    names = sorted(set(re.findall(r"\b(dg_[a-z0-9_]+)\s*\(", header)))
+    body = "\n".join(f"    p[n++] = (void*)&{nm};" for nm in names)
+    src = f'#include "dg_gpu.h"\n#include <stdio.h>\nint main(void) {{\n    void* p[{len(names) + 1}]; int n = 0;\n{body}\n    printf("%d %p\\n", n, p[0]);\n    return 0;\n}}\n'
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "abi.c")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "abi")
+        lib = os.path.join(root, "fve_dg_b200")
+        r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-I", os.path.join(root, "include"), c, "-o", exe,
+                            "-L", lib, "-lfvedg_b200", "-Wl,-rpath," + lib], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+    assert len(names) >= 30
