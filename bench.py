@@ -160,85 +160,117 @@ def kernel_bytes(name, P, ncell, nface, nqf):
     raise ValueError(name)
 
 
+def algorithmic_bytes(name, P, ncell, nface, nqf):
+    """The algorithm's minimum HBM bytes for the work one launch does, independent of how this
+    implementation stores its intermediates: the state rows the work must read and write (8 B per
+    DOF each), the element geometry (80 B: J^-T and det J) and the face records (42 B: normal, 2A,
+    two cell ids, two face maps). Face kernels: the stage input once plus the face records. Element
+    kernels: the stage input, U^n and the new stage plus the geometry. A whole stage (the persistent
+    kernel): both, with the stage input counted once. The limiter and the viscous operator have no
+    such minimum of their own; their implementation bytes stand in."""
+    state = ncell * 5 * nb_of(P) * 8
+    if name.startswith("face_flux"):
+        return state + 42 * nface
+    if name.startswith("element"):
+        return 3 * state + 80 * ncell
+    if name == "stage_persistent_mixed":
+        return 3 * state + 80 * ncell + 42 * nface
+    return kernel_bytes(name, P, ncell, nface, nqf)
+
+
+# Parameters of the problems for the oracle's own projection (ref_harness.cpp problem_state), equal
+# to the defaults of fve_dg_b200.problems that the GPU arm uses.
+ORACLE_PROBLEM = {
+    "taylor_green": [0.1, 1.4],
+    "density_wave": [0.2, 1.0, 1.0, 1.0, 1.0, 0.5, 0.25, 1.0, 1.4],
+    "vortex": [5.0, 5.0, 5.0, 0.0, 0.0, 1.0, 5.0, 1.4, 1.0, 1.0, 0.0, 0.0],
+}
+
+
+def oracle_setup(cfg, n=None):
+    """The workload's mesh and initial state built by the oracle alone: the periodic box made inside
+    the reference harness and the reference's func2coef projection (nothing of fve_dg_b200 is
+    loaded). Returns (RefLib, RefMesh, U0, mass, seconds)."""
+    from oracle.pyoracle import RefLib
+    t0 = time.perf_counter()
+    ref = RefLib()
+    ref.set_threads(os.cpu_count() or 1)
+    n = cfg["n"] if n is None else n
+    rm = ref.box(n, hi=(cfg["L"],) * 3, jitter=cfg["jitter"])
+    U = rm.project(cfg["P"], cfg["problem"], ORACLE_PROBLEM[cfg["problem"]])
+    b = rm.mass(cfg["P"], cfg["qv"])
+    return ref, rm, U, b, time.perf_counter() - t0
+
+
+def time_reference_steps(rm, U, b, cfg, dt, budget_s, max_steps):
+    """SSP-RK3 steps of the reference's own operator (ExplicitConvection::eval with LongVector stage
+    updates, ref_harness.cpp run_ssprk3) on the whole mesh: one untimed residual evaluation first,
+    then whole steps while the estimate stays within budget_s (at least one)."""
+    P, qv, qf = cfg["P"], cfg["qv"], cfg["qf"]
+    t0 = time.perf_counter()
+    rm.eval(U, P, qv, qf)
+    per_eval = time.perf_counter() - t0
+    k = int(max(1, min(max_steps, budget_s // max(3.2 * per_eval, 1e-9))))
+    t0 = time.perf_counter()
+    U = rm.ssprk3(U, b, P, qv, qf, dt, k)
+    return k, time.perf_counter() - t0, U
+
+
 def run_reference(args, cfg, rank):
-    """The reference's own CPU path on a bounded sample of the workload (rank 0 only)."""
+    """The reference's own CPU path on the whole workload mesh (rank 0 only): the oracle builds the
+    mesh and the initial state itself, so the product's library is never loaded in this arm."""
     if rank != 0:
         return
-    from fve_dg_b200 import box_mesh, problems
-    from oracle.pyoracle import RefLib, RefMesh, ref_available
+    from oracle.pyoracle import ref_available
     if not ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfvedg_ref.so was not built"}))
         return
-    ref = RefLib()
     threads = os.cpu_count() or 1
-    ref.set_threads(threads)
-    n_s = max(4, min(cfg["n"], 12))
-    m = box_mesh(n_s, hi=(cfg["L"],) * 3, jitter=cfg["jitter"])
-    P, qv, qf = cfg["P"], cfg["qv"], cfg["qf"]
-    U = problems.project(m, P, problem_fn(cfg["problem"], problems))
-    rm = RefMesh.from_mesh(ref, m)
-    b = rm.mass(P, qv)
-    dt = 1e-4
-    budget = 150.0
-    t0 = time.perf_counter()
-    for _ in range(args.warmup):
-        U = rm.ssprk3(U, b, P, qv, qf, dt, 1)
-    t_w = time.perf_counter() - t0
-    per = t_w / max(args.warmup, 1)
-    k = args.steps if per * args.steps <= budget else max(3, int(budget / max(per, 1e-9)))
-    t0 = time.perf_counter()
-    for _ in range(k):
-        U = rm.ssprk3(U, b, P, qv, qf, dt, 1)
-    el = time.perf_counter() - t0
-    dofs = 5 * nb_of(P) * m.ncell * 3 * k
+    ref, rm, U, b, setup_s = oracle_setup(cfg)
+    P = cfg["P"]
+    k, el, _ = time_reference_steps(rm, U, b, cfg, 1e-4, 150.0, args.steps)
+    dofs = 5 * nb_of(P) * rm.ncell * 3 * k
     val = dofs / el
-    sample = (f"{cfg['problem']} P{P} on {n_s}^3x6={m.ncell} tets (same rules; LF flux, the reference has no Roe), "
-              f"{k} SSP-RK3 steps of ExplicitConvection::eval + LongVector stage updates")
+    flux_note = "LF flux (the reference has no Roe solver)" if cfg["flux"] == "Roe" else "LF flux"
+    sample = (f"{cfg['problem']} P{P} on the whole {cfg['n']}^3x6={rm.ncell} tet mesh, same rules, {flux_note}; "
+              f"{k} SSP-RK3 step(s) of ExplicitConvection::eval + LongVector stage updates, {el:.1f} s on {threads} "
+              f"threads; mesh and func2coef projection made by the oracle ({setup_s:.1f} s, untimed)")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "DOF-stage/s", "n_gpus": args.gpus,
-            "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * el / k, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.config, "desc": cfg["desc"], "precision": "fp64"},
+            "steps": k, "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / k,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.config, "desc": cfg["desc"], "precision": "fp64", "tets": rm.ncell,
+                       "flux_timed": "LF", "same_mesh_and_rules": True},
             "cpu_baseline": {"value": val, "unit": "DOF-stage/s", "cores": threads, "kind": "reference",
-                             "sample": sample},
+                             "sample": sample, "cpu_model": cpu_model()},
             "e2e": {"value": val, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def cpu_baseline(cfg):
-    """About 10-30 s of the reference's CPU operator on a sample of the workload (rank 0, N=1)."""
-    from fve_dg_b200 import box_mesh, problems
-    from oracle.pyoracle import RefLib, RefMesh, ref_available
+    """The reference's CPU operator timed on the GPU box's host cores (rank 0, N=1): one SSP-RK3 step
+    of the whole workload mesh on all threads, and for context a one-thread figure on a 12^3x6 slice
+    of the same problem. Mesh and state come from the oracle alone."""
+    from oracle.pyoracle import ref_available
     if not ref_available():
         return None
-    ref = RefLib()
     threads = os.cpu_count() or 1
-    ref.set_threads(threads)
-    n_s = max(4, min(cfg["n"], 12))
-    m = box_mesh(n_s, hi=(cfg["L"],) * 3, jitter=cfg["jitter"])
-    P, qv, qf = cfg["P"], cfg["qv"], cfg["qf"]
-    U = problems.project(m, P, problem_fn(cfg["problem"], problems))
-    rm = RefMesh.from_mesh(ref, m)
-    b = rm.mass(P, qv)
-    U = rm.ssprk3(U, b, P, qv, qf, 1e-4, 1)  # warm-up step
-
-    def rate(seconds, max_steps):
-        nonlocal U
-        k, t0 = 0, time.perf_counter()
-        while True:
-            U = rm.ssprk3(U, b, P, qv, qf, 1e-4, 1)
-            k += 1
-            if time.perf_counter() - t0 > seconds or k >= max_steps:
-                break
-        el = time.perf_counter() - t0
-        return 5 * nb_of(P) * m.ncell * 3 * k / el, k, el
-
-    val, k, el = rate(10.0, 50)
-    ref.set_threads(1)
-    val1, k1, el1 = rate(4.0, 20)
-    ref.set_threads(threads)
+    ref, rm, U, b, setup_s = oracle_setup(cfg)
+    k, el, _ = time_reference_steps(rm, U, b, cfg, 1e-4, 40.0, 1)
+    ncell = rm.ncell
+    val = 5 * nb_of(cfg["P"]) * ncell * 3 * k / el
+    del rm
+    n1 = max(4, min(cfg["n"], 12))
+    ref1, rm1, U1, b1, _ = oracle_setup(cfg, n=n1)
+    ref1.set_threads(1)
+    k1, el1, _ = time_reference_steps(rm1, U1, b1, cfg, 1e-4, 8.0, 20)
+    ref1.set_threads(threads)
+    val1 = 5 * nb_of(cfg["P"]) * rm1.ncell * 3 * k1 / el1
+    flux_note = "LF flux (the reference has no Roe solver)" if cfg["flux"] == "Roe" else "LF flux"
     return {"value": val, "unit": "DOF-stage/s", "cores": threads, "kind": "reference",
-            "sample": f"{cfg['problem']} P{P}, {n_s}^3x6={m.ncell} tets, {k} SSP-RK3 steps (LF flux), {el:.1f} s",
-            "value_1_thread": val1, "sample_1_thread": f"{k1} steps, {el1:.1f} s", "cpu_model": cpu_model()}
+            "sample": f"{cfg['problem']} P{cfg['P']}, whole {cfg['n']}^3x6={ncell} tet mesh, {k} SSP-RK3 step(s), "
+                      f"{flux_note}, {el:.1f} s; mesh and func2coef projection made by the oracle",
+            "value_1_thread": val1, "sample_1_thread": f"{n1}^3x6={rm1.ncell} tets, {k1} steps, {el1:.1f} s",
+            "cpu_model": cpu_model()}
 
 
 def cpu_model():
@@ -345,6 +377,7 @@ def main():
 
     # the other form on the same problem, same dt and steps from the same initial state
     forms = {args.precision: {"value": value, "ms_per_step": ms / args.steps, "schedule": schedule}}
+    accuracy = None
     if args.precision == "mixed" and not args.no_compare:
         f64 = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf, precision="fp64",
                                  device=local, limiter=args.limiter, mu=args.mu, prandtl=args.prandtl)
@@ -355,13 +388,14 @@ def main():
         forms["fp64"] = {"value": dof_stage_per_step * args.steps * world / (ms64 / 1e3),
                          "ms_per_step": ms64 / args.steps, "schedule": "two-launch",
                          "kernels_ms_per_launch": {KNAMES[("fp64", "two-launch")].get(k, str(k)): v[0] / v[1]
-                                                   for k, v in kt64.items()}}
-        # both forms stepped (warmup + steps) from U0 with the same dt: compare the states
-        err = problems.l2_errors(m, P, U_head, Uref=U64)
-        forms["mixed"]["l2_vs_fp64"] = {"rho": float(err[0]), "rhou": float(err[1]), "rhov": float(err[2]),
-                                        "rhow": float(err[3]), "E": float(err[4]),
-                                        "after_steps": args.warmup + args.steps}
+                                                   for k, v in kt64.items()},
+                         "roofline": make_roofline(kt64, "fp64", "two-launch", P, m.ncell, m.nface, conv.nq_face, nb,
+                                                   args.config)}
         forms["mixed_over_fp64"] = forms["mixed"]["value"] / forms["fp64"]["value"]
+        # accuracy: both forms stepped the configuration's number of steps from U0 with the same dt
+        # (untimed, independent of --steps)
+        accuracy = accuracy_report(conv, f64, U0, dt, m, P, cfg, args.config, problems)
+        forms["mixed"]["l2_vs_fp64"] = accuracy.pop("l2_mixed_vs_fp64")
         f64.close()
     cons = conv.conservation()
 
@@ -387,13 +421,51 @@ def main():
                            "schedule": schedule, "tets": m.ncell, "order": P, "dof_per_stage": 5 * nb * m.ncell,
                            "dt": dt, "l2": "state larger than L2 (no flush needed)",
                            "parallelism": f"independent instance per GPU x{world}"},
-                "gpu_launches": launches, "roofline": roofline, "forms": forms, "autotune": tune,
+                "gpu_launches": launches, "roofline": roofline, "forms": forms, "accuracy": accuracy,
+                "autotune": tune,
                 "conservation": {"mass": cons[0], "energy": cons[4], "kinetic": cons[5]},
                 "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks}
         print(json.dumps(line), flush=True)
     conv.close()
     if dist:
         dist.destroy_process_group()
+
+
+# SSP-RK3 steps of each configuration's run (the accuracy figures are taken after them)
+RUN_STEPS = {"tgv": 100, "dwave": 200, "dwave_p4": 50, "vortex": 20, "ensemble": 20}
+
+
+def accuracy_report(conv, f64, U0, dt, m, P, cfg, config, problems):
+    """Both forms stepped RUN_STEPS[config] SSP-RK3 steps from U0 with the same dt: the mixed form's
+    relative L2 error against the FP64 form per variable (momenta also against the norm of the whole
+    momentum field), the drift of mass, energy and kinetic energy of each form over the run, and for
+    the density wave the error of each form against the exact translated solution."""
+    n = RUN_STEPS.get(config, 100)
+    f64.set_state(U0)
+    c0 = f64.conservation()
+    out = {"after_steps": n, "t": n * dt}
+    states, cons = {}, {}
+    for name, c in (("mixed", conv), ("fp64", f64)):
+        c.set_state(U0)
+        c.ssprk3(dt, n, graph=True)
+        states[name] = c.get_state()
+        cons[name] = c.conservation()
+    err = problems.l2_errors(m, P, states["mixed"], Uref=states["fp64"])
+    errm = problems.l2_errors(m, P, states["mixed"], Uref=states["fp64"], momentum_norm=True)
+    out["l2_mixed_vs_fp64"] = {"rho": float(err[0]), "rhou": float(err[1]), "rhov": float(err[2]),
+                               "rhow": float(err[3]), "E": float(err[4]),
+                               "momenta_over_momentum_norm": [float(x) for x in errm[1:4]], "after_steps": n}
+    for name in states:
+        c = cons[name]
+        out[name] = {"mass_drift": float((c[0] - c0[0]) / c0[0]), "energy_drift": float((c[4] - c0[4]) / c0[4]),
+                     "kinetic_energy_change": float((c[5] - c0[5]) / c0[5]),
+                     "momentum_drift": [float(c[i] - c0[i]) for i in (1, 2, 3)]}
+    if cfg["problem"] == "density_wave":
+        exact = problems.density_wave(t=n * dt)
+        for name in states:
+            e = problems.l2_errors(m, P, states[name], exact=exact)
+            out[name]["l2_vs_exact"] = {"rho": float(e[0]), "E": float(e[4])}
+    return out
 
 
 KNAMES = {("fp64", "two-launch"): {0: "face_flux_fp64", 1: "element_fp64", 3: "viscous", 4: "limiter"},
@@ -450,6 +522,12 @@ def time_e2e(conv, dt, steps, dof_stage_per_step, world, dist, torch):
 
 
 def make_roofline(kt, precision, schedule, P, ncell, nface, nqf, nb, config):
+    """Roofline object of the dominant kernel class of kt ({class: (total ms, launches)}): achieved GB/s
+    on the algorithm's minimum bytes of one launch (algorithmic_bytes) over its average CUDA-event
+    duration, against the measured HBM copy bandwidth. The bytes this implementation moves by design
+    (its intermediates included) and the DRAM traffic ncu measured for the kernel are reported beside
+    it, with their ratios to the algorithmic bytes. `stage` carries the stage-level figures on the
+    algorithm's minimum bytes and flops per DOF-stage."""
     names = KNAMES[(precision, schedule)]
     peak, peak_kind = read_peaks()
     dom = max(kt, key=lambda k: kt[k][0])
@@ -461,19 +539,23 @@ def make_roofline(kt, precision, schedule, P, ncell, nface, nqf, nb, config):
             traffic = json.load(f).get(config, {}).get(name)
     except Exception:
         pass
-    b = kernel_bytes(name, P, ncell, nface, nqf)
+    alg = algorithmic_bytes(name, P, ncell, nface, nqf)
+    impl = kernel_bytes(name, P, ncell, nface, nqf)
     stage_ms = sum(v[0] for v in kt.values()) / kt[dom][1]  # every kernel class launches once per stage
-    ach = b / (dom_ms / 1e3) / 1e9
+    ach = alg / (dom_ms / 1e3) / 1e9
+    dofs = 5 * nb * ncell
+    stage_gbs = MIN_BYTES_PER_DOF_STAGE[P] * dofs / (stage_ms / 1e3) / 1e9
+    stage_tf = FLOP_PER_DOF_STAGE[P] * dofs / (stage_ms / 1e3) / 1e12
     return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-            "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": b, "avg_launch_ms": dom_ms,
+            "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": alg,
+            "implementation_bytes_per_launch": impl, "implementation_over_algorithmic": impl / alg,
+            "traffic_over_algorithmic": (traffic / alg) if traffic else None,
+            "frac_on_implementation_bytes": impl / (dom_ms / 1e3) / 1e9 / peak, "avg_launch_ms": dom_ms,
             "stage": {"ms": stage_ms, "bytes_per_dof_stage_min": MIN_BYTES_PER_DOF_STAGE[P],
-                      "achieved_gbs_at_min_bytes": MIN_BYTES_PER_DOF_STAGE[P] * 5 * nb * ncell
-                      / (stage_ms / 1e3) / 1e9,
-                      "flop_per_dof_stage": FLOP_PER_DOF_STAGE[P],
-                      "achieved_tflops": FLOP_PER_DOF_STAGE[P] * 5 * nb * ncell / (stage_ms / 1e3) / 1e12,
+                      "achieved_gbs_at_min_bytes": stage_gbs, "frac_of_hbm": stage_gbs / peak,
+                      "flop_per_dof_stage": FLOP_PER_DOF_STAGE[P], "achieved_tflops": stage_tf,
                       "fp64_nominal_tflops": FP64_NOMINAL_TFLOPS,
-                      "frac_of_fp64_nominal": FLOP_PER_DOF_STAGE[P] * 5 * nb * ncell / (stage_ms / 1e3) / 1e12
-                      / FP64_NOMINAL_TFLOPS},
+                      "frac_of_fp64_nominal": stage_tf / FP64_NOMINAL_TFLOPS},
             "kernels_ms_per_launch": {names.get(k, str(k)): v[0] / v[1] for k, v in kt.items()}}
 
 
@@ -525,24 +607,20 @@ def run_viscous(args, cfg, rank, world, local, dist):
     e2e = dof * k * world / (time.perf_counter() - t0)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        from oracle.pyoracle import RefLib, RefMesh, ref_available
+        from oracle.pyoracle import ref_available
         if ref_available():
-            ref = RefLib()
             threads = os.cpu_count() or 1
-            ref.set_threads(threads)
             n_s = max(4, min(cfg["n"], 12))
-            ms_ = box_mesh(n_s, hi=(cfg["L"],) * 3, jitter=cfg["jitter"])
-            Us = problems.project(ms_, P, problem_fn(cfg["problem"], problems))
-            rm = RefMesh.from_mesh(ref, ms_)
+            _, rm, Us, _, _ = oracle_setup(cfg, n=n_s)
             rm.diffusion(Us, P, qv, qf)
             kk, t0 = 0, time.perf_counter()
             while time.perf_counter() - t0 < 5.0 and kk < 50:
                 rm.diffusion(Us, P, qv, qf)
                 kk += 1
             el = time.perf_counter() - t0
-            cpu = {"value": 5 * nb * ms_.ncell * kk / el, "unit": "DOF-residual/s", "cores": threads,
+            cpu = {"value": 5 * nb * rm.ncell * kk / el, "unit": "DOF-residual/s", "cores": threads,
                    "kind": "reference",
-                   "sample": f"ExplicitDiffusion::eval, {cfg['problem']} P{P} on {n_s}^3x6={ms_.ncell} tets, "
+                   "sample": f"ExplicitDiffusion::eval, {cfg['problem']} P{P} on {n_s}^3x6={rm.ncell} tets, "
                              f"{kk} evaluations, {el:.1f} s", "cpu_model": cpu_model()}
     if rank == 0:
         ms_each = ms / args.steps

@@ -15,6 +15,8 @@ c_int8_p = ctypes.POINTER(ctypes.c_int8)
 c_int_p = ctypes.POINTER(ctypes.c_int)
 
 DG_OK = 0
+DG_E_ARG = -1
+DG_E_WATCHDOG = -6
 STATUS = {0: "DG_OK", -1: "DG_E_ARG", -2: "DG_E_MESH", -3: "DG_E_CUDA", -4: "DG_E_NOMEM",
           -5: "DG_E_NONPHYSICAL", -6: "DG_E_WATCHDOG", -7: "DG_E_STATE", -8: "DG_E_IO"}
 
@@ -61,6 +63,7 @@ def lib():
         "dg_residual": (ctypes.c_int, [vp, c_double_p, c_double_p, ctypes.c_size_t, ctypes.c_double, ctypes.c_int]),
         "dg_residual_device": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, ctypes.c_int, vp]),
         "dg_residual_device_static": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp]),
+        "dg_watchdog_selftest": (ctypes.c_int, [vp, ctypes.c_int64]),
         "dg_static_scratch_capacity": (ctypes.c_int64, []),
         "dg_set_state": (ctypes.c_int, [vp, c_double_p, ctypes.c_size_t]),
         "dg_get_state": (ctypes.c_int, [vp, c_double_p, ctypes.c_size_t]),
@@ -117,7 +120,7 @@ def exported_symbols():
             "dg_static_scratch_capacity", "dg_set_state", "dg_get_state",
             "dg_ssprk3", "dg_ssprk3_graph", "dg_ssprk3_timed", "dg_stream", "dg_state_device",
             "dg_refresh_split", "dg_ssprk3_stage", "dg_ssprk3_stage_phase", "dg_create_ensemble",
-            "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_mass", "dg_limit", "dg_limit_device", "dg_viscous_residual", "dg_viscous_residual_device",
+            "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_watchdog_selftest", "dg_mass", "dg_limit", "dg_limit_device", "dg_viscous_residual", "dg_viscous_residual_device",
             "dg_save_checkpoint", "dg_load_checkpoint",
             "dg_set_dirichlet", "dg_conservation",
             "dg_max_wave_speed", "dg_check_state", "dg_info", "dg_mesh_geometry", "dg_face_perms", "dg_basis",

@@ -1,7 +1,8 @@
 """Build the native library in-tree: fve_dg_b200/libfvedg_b200.so (host C++ + sm_100a CUDA).
 
-Host sources are compiled with g++ -ffp-contract=off so that mesh geometry reproduces the
-reference's arithmetic bit for bit; CUDA sources with nvcc for sm_100a only. The oracle
+Host sources are compiled with g++ (-O3 -mfma; geometry from raw topology then agrees with the
+reference's to a few ulp, connectivity and face maps bit for bit); CUDA sources with nvcc for
+sm_100a only. The oracle
 (oracle/liboracle.so) and, when the reference sources are present, oracle/_ref/libfvedg_ref.so
 are built by oracle/Makefile; `build_all()` drives both.
 """

@@ -606,7 +606,8 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
         (rc = upload(&c->d_w_v, c->tab.w_v)) || (rc = upload(&c->d_phi_f, c->tab.phi_f)) ||
         (rc = upload(&c->d_phi_fT, c->tab.phi_fT)) || (rc = upload(&c->d_phi_vT, c->tab.phi_vT)) ||
         (rc = upload(&c->d_w_f, c->tab.w_f)) || (rc = upload(&c->d_mass_ref, c->tab.mass_ref)) ||
-        (rc = dev_alloc(&c->d_Fh, (size_t)c->nface * nqf * 5)) || (rc = dev_alloc(&c->d_Un, nstate)) ||
+        (rc = dev_alloc(&c->d_Fh, cfg->precision == DG_PREC_FP64 ? (size_t)c->nface * nqf * 5 : 0)) ||
+        (rc = dev_alloc(&c->d_Un, nstate)) ||
         (rc = dev_alloc(&c->d_Ua, nstate)) || (rc = dev_alloc(&c->d_Ub, nstate)) ||
         (rc = dev_alloc(&c->d_red, (size_t)kRedBlocks * 8)) || (rc = dev_alloc(&c->d_red_out, 8)))
         return fail(c, rc);
@@ -1030,6 +1031,30 @@ int dg_ssprk3_timed(dg_ctx* c, double dt, int nsteps, double* out, int nclass) {
         if (k < nclass) { out[2 * k] += ms; out[2 * k + 1] += 1.0; }
     }
     return DG_OK;
+}
+
+int dg_watchdog_selftest(dg_ctx* c, int64_t polls) {
+    if (!c || polls < 1) return DG_E_ARG;
+    if (c->cfg.precision != DG_PREC_MIXED || c->cfg.schedule != 1 || !c->qs.ready || c->qs.nregions < 1)
+        return DG_E_ARG;
+    if (!c->have_state) return DG_E_STATE;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    DG_CUDA(cudaStreamSynchronize(c->stream));
+    unsigned int need = 0;
+    DG_CUDA(cudaMemcpy(&need, c->qs.total, sizeof(unsigned int), cudaMemcpyDeviceToHost));
+    const unsigned int never = need + 1u;  // one face group more than region 0 has: no wait on it can end
+    DG_CUDA(cudaMemcpy(c->qs.total, &never, sizeof(unsigned int), cudaMemcpyHostToDevice));
+    PersistentParams pp = c->pp;
+    pp.spin_limit = polls;
+    auto untimed = [&](int, auto&& fn) { return fn(); };
+    auto no_post = [&](const double*, double*, int) { return DG_OK; };
+    int rc = step_persistent(c->mixed, c->d_queue, c->qs, pp, c->d_Un, c->d_Ua, c->d_Ub, 0.0, c->stream, &g_launches,
+                             untimed, no_post, 0, 1);
+    const cudaError_t se = cudaStreamSynchronize(c->stream);
+    const cudaError_t re = cudaMemcpy(c->qs.total, &need, sizeof(unsigned int), cudaMemcpyHostToDevice);
+    if (rc) return rc;
+    if (se != cudaSuccess || re != cudaSuccess) return DG_E_CUDA;
+    return check_queue(c);
 }
 
 int dg_autotune(dg_ctx* c, double dt, char* report, size_t len) {

@@ -11,8 +11,9 @@
 // waits for was taken before it, every wait ends; no cooperative launch is needed, and uneven work
 // (an ensemble of meshes of different sizes laid end to end) balances itself.
 //
-// Every wait is bounded: a CTA that spins longer than kSpinLimit polls records DG_E_WATCHDOG in
-// the queue state and goes on; the host reads that word after the step and reports the error. The
+// Every wait is bounded: a CTA that spins longer than the poll limit (kSpinLimit unless the context
+// sets another) records DG_E_WATCHDOG in the queue state and goes on; the host reads that word after
+// the step and reports the error. The
 // last CTA to leave re-arms the ticket and the completion counters for the next launch, so a CUDA
 // graph replays the three launches of a step as they are.
 #pragma once
@@ -38,6 +39,7 @@ struct PersistentParams {
     int max_blocks = 0;  // CTAs per SM cap (0 = as many as fit)
     int regions = 32;    // element regions (1 .. kMaxRegions)
     int lag = 1;         // face regions between an element tile's last dependency and its place
+    long long spin_limit = kSpinLimit;  // polls before a wait gives up (not part of the tile list)
     bool operator==(const PersistentParams& o) const {
         return tile_f == o.tile_f && tile_e == o.tile_e && regions == o.regions && lag == o.lag;
     }
@@ -62,7 +64,7 @@ template <int NB, int NQV, int NQF, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, WARPS == 8 ? 4 : 6)
     stage_persistent_mixed(MixedFaceArgs fa, MixedElemArgs ea, QueueState* q, const int4* __restrict__ tiles,
                            int ntiles, const unsigned long long* __restrict__ deps,
-                           const unsigned int* __restrict__ total) {
+                           const unsigned int* __restrict__ total, long long spin_limit) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ ElemTables<NB> tabs;
     __shared__ int4 s_tile;
@@ -81,7 +83,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 8 ? 4 : 6)
                     long long spins = 0;
                     while (*d < total[f]) {
                         __nanosleep(64);
-                        if (++spins > kSpinLimit) {
+                        if (++spins > spin_limit) {
                             atomicExch(&q->error, DG_E_WATCHDOG);
                             break;
                         }
@@ -234,7 +236,8 @@ inline int persistent_launch(MixedData& m, QueueState* q, const QueueSchedule& q
     const int bps = pp.max_blocks > 0 ? std::min(per_sm[dev & 63], pp.max_blocks) : per_sm[dev & 63];
     const MixedFaceArgs fa = face_args(m, U, mir_in, face_mask);
     const MixedElemArgs ea = elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out);
-    kern<<<m.sms * bps, W * 32, smem, s>>>(fa, ea, q, qs.tiles, qs.ntiles, qs.deps, qs.total);
+    kern<<<m.sms * bps, W * 32, smem, s>>>(fa, ea, q, qs.tiles, qs.ntiles, qs.deps, qs.total,
+                                           pp.spin_limit > 0 ? pp.spin_limit : kSpinLimit);
     return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;
 }
 

@@ -1,6 +1,9 @@
-// Host side: periodic box mesh generator, mesh validation, geometry with the reference's
-// arithmetic, and face maps. Built with -ffp-contract=off so geometry matches the reference bit
-// for bit (the reference is compiled in ISO C++17 mode, where GCC does not contract a*b+c).
+// Host side: periodic box mesh generator, mesh validation, geometry with the reference's formulas
+// and operation order, and face maps. Connectivity, orientation and face maps come out bit for bit;
+// normals, areas, det J and J^-T agree with the reference to a few ulp, because GCC decides per
+// expression where to contract a*b+c into an FMA (both builds use -mfma) and those choices differ
+// between the two code bases. Given the reference's own geometry (dg_mesh_desc form (a)) the device
+// numbers are the reference's exactly.
 #include <algorithm>
 #include <array>
 #include <cmath>

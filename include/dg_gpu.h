@@ -72,7 +72,9 @@ enum dg_tri_rule { DG_TRI_D3P4 = 0, DG_TRI_D3P6 = 1, DG_TRI_D4P7 = 2, DG_TRI_D10
  *      m_natural_coords, m_normal, m_area, m_invJac, compute_jacobian_det());
  *  (b) from raw topology: leave the geometry pointers NULL and give points, cell_nodes,
  *      face_nodes (and, for periodic faces, face_nodes1 + face_periodic). The library then
- *      computes the geometry with the reference's formulas, bit for bit. */
+ *      computes the geometry with the reference's formulas and operation order: connectivity,
+ *      orientation and face maps bit for bit, normals, areas and J^-T to a few ulp (the two builds
+ *      contract different a*b+c into FMAs). */
 typedef struct dg_mesh_desc {
     int64_t ncell;
     int64_t nface;
@@ -139,17 +141,21 @@ int dg_residual(dg_ctx* ctx, const double* U, double* R, size_t elem_stride_byte
 int dg_residual_device(dg_ctx* ctx, const double* U_dev, double* R_dev, double t, int part, void* stream);
 
 /* Residual on device buffers that allocates nothing. This entry point has no counterpart in the
- * reference. It is for callers that must not allocate device memory at the point of the call:
- * code running inside a CUDA stream-capture region or a host callback, where cudaMalloc would
- * break the capture or deadlock, and frameworks that own all device memory through their own pool
- * and forbid raw cudaMalloc once set-up is over. Such a caller creates the context at set-up time
- * and may then call this any number of times.
- * It computes exactly what dg_residual_device computes with the FP64 kernels, but the face-flux
- * scratch (nface * nqf * 5 doubles) lives in one fixed device array of this library,
+ * reference. It is for callers that cannot call cudaMalloc once they are running: applications and
+ * frameworks that hand all device memory to their own pool allocator at start-up and forbid raw
+ * cudaMalloc afterwards (a raw allocation there either fails, because the pool already holds the
+ * memory, or takes memory the pool has counted as free), and time-critical loops that must not
+ * allocate because cudaMalloc and cudaFree can synchronise the device. Such a caller creates the
+ * context during its set-up and may then call this any number of times.
+ * It computes what dg_residual_device computes with the FP64 kernels, but the face-flux scratch
+ * (nface * nqf * 5 doubles) lives in one fixed device array of this library,
  * dg_static_scratch_capacity() doubles (32 MiB), that every GPU which loads the library holds
- * until the process exits. Meshes whose face fluxes do not fit are rejected with DG_E_ARG.
+ * until the process exits. Meshes whose face fluxes do not fit are rejected with DG_E_ARG. On a
+ * context created with DG_PREC_MIXED it still runs the FP64 kernels, so its result is the FP64
+ * residual (what dg_residual_device returns on an FP64 context), not the mixed-precision one.
  * The first call on a device looks up that device's copy of the array (cudaGetSymbolAddress with
- * the context's device current); make that first call before any stream capture begins.
+ * the context's device current) and keeps the address for the life of the process; make that first
+ * call before any stream capture begins, and do not call this after cudaDeviceReset on that device.
  * Every call shares the one array and it keeps the last call's contents; nothing in it has to start
  * at zero (each call writes every entry it reads). Calls whose kernels overlap on the GPU (on
  * different streams, or from several contexts on one device) race on the array: serialise them. */
@@ -180,6 +186,15 @@ int dg_ssprk3_ensemble(dg_ctx* ctx, const double* dt, int nsteps, int use_graph)
  * CTAs per SM, mesh regions, lag) on the current state (restored afterwards), keeps the fastest and
  * writes a JSON record of every candidate and the choice into report[len]. */
 int dg_autotune(dg_ctx* ctx, double dt, char* report, size_t len);
+
+/* Self-test of the failure detection of the batched persistent form (mixed precision, schedule 1):
+ * runs stage 0 of one SSP-RK3 step with the completion count that face region 0 must reach raised
+ * by one, so every wait of an element tile on that region runs out after `polls` polls (each about
+ * 64 ns) instead of ending; the count is restored afterwards. Returns what the stage reports:
+ * DG_E_WATCHDOG when the expired waits were recorded on the device and read back by the host. The
+ * stage writes only U^(1), so U^n is unchanged and the context stays usable. New: the reference has
+ * no device code and no such check. */
+int dg_watchdog_selftest(dg_ctx* ctx, int64_t polls);
 
 /* Same as dg_ssprk3, with CUDA events around every kernel launch on the context's stream.
  * out[2k] = total milliseconds and out[2k+1] = launch count of kernel class k < nclass:
@@ -265,7 +280,7 @@ int dg_check_state(dg_ctx* ctx, int64_t* bad_points);
 /* Sizes and the rules actually used. */
 int dg_info(const dg_ctx* ctx, int* num_basis, int* nq_vol, int* nq_face, int* quad_vol, int* quad_face);
 
-/* Geometry exactly as the reference's ComputingMesh computes it from raw topology (form (b) of
+/* Geometry as the reference's ComputingMesh computes it from raw topology (form (b) of
  * dg_mesh_desc): unit normals, areas, natural coordinates [nface][2][3][3], J^{-T} [ncell][9],
  * detJ, centroids. Host-only; no device needed. */
 int dg_mesh_geometry(const dg_mesh_desc* mesh, double* normal, double* area, double* natural,

@@ -1,7 +1,9 @@
 // Test infrastructure: compiles the C++ drop-ins include/ExplicitConvectionGPU.h,
 // ExplicitDiffusionGPU.h and PositiveLimiterGPU.h against the reference's own headers and checks
 // them against the reference's ExplicitConvection, ExplicitDiffusion and PositiveLimiter on the same
-// ComputingMesh, the way a driver would swap the classes. Built by `make -C oracle ref` into
+// ComputingMesh, the way a driver would swap the classes: on Kuhn boxes passed through
+// ComputingMesh(const DGMesh&), and on the reference's own OrthHexMesh + split_hex6_scan mesh passed
+// through ComputingMesh(const GeneralMesh&). Built by `make -C oracle ref` into
 // oracle/_ref/adaptor_check (linked to fve_dg_b200/libfvedg_b200.so); run by
 // tests/test_gpu_adaptor.py on a GPU. Exit status 0 when every case agrees to 1e-12 (relative L2).
 #include "DG/DG_Schemes/ExplicitConvection.h"
@@ -60,6 +62,22 @@ static ComputingMesh* make_mesh(int n, BoundaryType bt) {
     dg_box_mesh_destroy(bm);
     ComputingMesh* m = new ComputingMesh(g);
     m->m_boundaryTypes.assign(m->m_faces.size(), bt);
+    return m;
+}
+
+// The reference's own route, as its drivers build a box (examples/Vortex/123/Vortex.cpp:101-106):
+// OrthHexMesh -> split_hex6_scan -> rebuild_cell_topology -> validate_mesh -> ComputingMesh(GeneralMesh);
+// boundary faces with |n_z| > 0.5 get Pseudo3DZ, the others bt.
+static ComputingMesh* make_mesh_orthhex(int n, BoundaryType bt) {
+    GeneralMesh g = OrthHexMesh({0.0, 0.0, 0.0}, {1.0, 1.0, 0.5}, {(uInt)n, (uInt)n, (uInt)n});
+    g.split_hex6_scan();
+    g.rebuild_cell_topology();
+    g.validate_mesh();
+    ComputingMesh* m = new ComputingMesh(g);
+    m->m_boundaryTypes.assign(m->m_faces.size(), BoundaryType::Pseudo3DZ);
+    for (size_t f = 0; f < m->m_faces.size(); ++f)
+        if (m->m_faces[f].m_neighbor_cells[1] == uInt(-1) && std::abs(m->m_faces[f].m_normal[2]) <= 0.5)
+            m->m_boundaryTypes[f] = bt;
     return m;
 }
 
@@ -159,10 +177,11 @@ static int check_limiter(const ComputingMesh& m, const char* name) {
 
 int main() {
     int bad = 0;
-    for (BoundaryType bt : {BoundaryType::Dirichlet, BoundaryType::Pseudo3DZ}) {
-        ComputingMesh* m = make_mesh(2, bt);
+    for (int which = 0; which < 3; ++which) {
+        const BoundaryType bt = which == 1 ? BoundaryType::Pseudo3DZ : BoundaryType::Dirichlet;
+        ComputingMesh* m = which < 2 ? make_mesh(2, bt) : make_mesh_orthhex(3, bt);
         if (!m) return 2;
-        const char* name = bt == BoundaryType::Dirichlet ? "dirichlet" : "pseudo3dz";
+        const char* name = which == 0 ? "dirichlet" : which == 1 ? "pseudo3dz" : "orthhex-split6";
         bad += check<1, T::Degree2Points4, F::Degree3Points6>(*m, name);
         bad += check<2, T::Degree4Points11, F::Degree4Points7>(*m, name);
         bad += check<3, T::Degree6Points23, F::Degree10Points24>(*m, name);

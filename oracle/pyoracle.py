@@ -152,6 +152,14 @@ class RefLib:
         L.fveref_block_bytes.argtypes = [ctypes.c_int]
         L.fveref_set_dirichlet.argtypes = [dp]
         L.fveref_set_threads.argtypes = [ctypes.c_int]
+        L.fveref_box_create.restype = ctypes.c_void_p
+        L.fveref_box_create.argtypes = [ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_uint64,
+                                        ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        L.fveref_orthhex_create.restype = ctypes.c_void_p
+        L.fveref_orthhex_create.argtypes = [ctypes.c_int, dp, dp, ctypes.c_int, ctypes.c_int]
+        L.fveref_mesh_sizes.argtypes = [ctypes.c_void_p, u64p]
+        L.fveref_mesh_topology.argtypes = [ctypes.c_void_p, dp, u64p, u64p, u64p, u64p, u64p, u64p, u8p, u8p]
+        L.fveref_project.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp, dp]
         self.L = L
 
     def set_threads(self, n):
@@ -188,6 +196,28 @@ class RefLib:
     def mesh(self, points, cells, faces, face_cells, cell_faces, cell_cells, face_nodes1=None, periodic=None, bc=None):
         return RefMesh(self, points, cells, faces, face_cells, cell_faces, cell_cells, face_nodes1, periodic, bc)
 
+    def box(self, n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), jitter=0.0, seed=20261203, periodic=(1, 1, 1), bc=5):
+        """The periodic Kuhn box made by the oracle itself (ref_harness.cpp build_box), as a reference
+        ComputingMesh; same mesh as the product's box_mesh with the same arguments."""
+        lo_a, hi_a = np.array(lo, dtype=np.float64), np.array(hi, dtype=np.float64)
+        per = (ctypes.c_int * 3)(*[int(p) for p in periodic])
+        h = self.L.fveref_box_create(int(n), lo_a.ctypes.data_as(dp), hi_a.ctypes.data_as(dp), float(jitter),
+                                     int(seed), per, int(bc))
+        if not h:
+            raise RuntimeError("fveref_box_create failed")
+        return RefMesh.from_handle(self, h)
+
+    def orthhex(self, n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), bc_z=5, bc_side=0):
+        """The reference's own mesh route OrthHexMesh -> split_hex6_scan -> ComputingMesh(GeneralMesh)
+        (ref_harness.cpp build_orthhex): n^3 hexahedra, boundary faces with |n_z| > 0.5 typed bc_z, the
+        others bc_side."""
+        lo_a, hi_a = np.array(lo, dtype=np.float64), np.array(hi, dtype=np.float64)
+        h = self.L.fveref_orthhex_create(int(n), lo_a.ctypes.data_as(dp), hi_a.ctypes.data_as(dp), int(bc_z),
+                                         int(bc_side))
+        if not h:
+            raise RuntimeError("fveref_orthhex_create failed")
+        return RefMesh.from_handle(self, h)
+
 
 class RefMesh:
     def __init__(self, ref, points, cells, faces, face_cells, cell_faces, cell_cells, face_nodes1, periodic, bc):
@@ -218,6 +248,46 @@ class RefMesh:
     def from_mesh(cls, ref, m):
         return cls(ref, m.points, m.cells, m.faces, m.face_cells, m.cell_faces, m.cell_cells, m.face_nodes1,
                    m.periodic, m.bc)
+
+    @classmethod
+    def from_handle(cls, ref, h):
+        """A mesh the harness built itself; its flat topology is exported into numpy arrays (int64, -1 for
+        a missing neighbour) with the attribute names of the product's Mesh."""
+        self = cls.__new__(cls)
+        self.ref, self.h, self._keep = ref, h, []
+        sz = np.zeros(3, dtype=np.uint64)
+        if ref.L.fveref_mesh_sizes(h, sz.ctypes.data_as(u64p)) != 0:
+            raise RuntimeError("fveref_mesh_sizes failed")
+        npts, nc, nf = (int(v) for v in sz)
+        self.ncell, self.nface = nc, nf
+        U64 = np.uint64
+        pts = np.zeros((npts, 3))
+        cells, cf, cc = (np.zeros((nc, 4), dtype=U64) for _ in range(3))
+        faces, fn1 = np.zeros((nf, 3), dtype=U64), np.zeros((nf, 3), dtype=U64)
+        fc = np.zeros((nf, 2), dtype=U64)
+        per, bc = np.zeros(nf, dtype=np.uint8), np.zeros(nf, dtype=np.uint8)
+        ref.L.fveref_mesh_topology(h, pts.ctypes.data_as(dp), *[a.ctypes.data_as(u64p) for a in (cells, cf, cc, faces,
+                                                                                                  fc, fn1)],
+                                   per.ctypes.data_as(u8p), bc.ctypes.data_as(u8p))
+        self.points = pts
+        self.cells, self.cell_faces, self.cell_cells = (a.astype(np.int64) for a in (cells, cf, cc))
+        self.faces, self.face_cells, self.face_nodes1 = (a.astype(np.int64) for a in (faces, fc, fn1))
+        self.periodic, self.bc = per, bc
+        return self
+
+    PROBLEMS = {"vortex": 0, "density_wave": 1, "taylor_green": 2}
+
+    def project(self, order, problem, params):
+        """Initial coefficients by the reference's DGBasisEvaluator<P>::func2coef, per cell (ref_harness.cpp
+        run_project): problem 'vortex' params (cx,cy,cz, ax,ay,az, beta, gamma, ux,uy,uz, period or 0),
+        'density_wave' (A, kx,ky,kz, ux,uy,uz, p, gamma), 'taylor_green' (Mach, gamma)."""
+        U = np.zeros((self.ncell, 5 * nb_of(order)))
+        prm = np.ascontiguousarray(params, dtype=np.float64)
+        rc = self.ref.L.fveref_project(self.h, order, self.PROBLEMS[problem], prm.ctypes.data_as(dp),
+                                       U.ctypes.data_as(dp))
+        if rc != 0:
+            raise RuntimeError(f"fveref_project rc={rc}")
+        return U
 
     def __del__(self):
         if getattr(self, "h", None):

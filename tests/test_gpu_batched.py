@@ -93,3 +93,29 @@ def test_ensemble_navier_stokes_matches_separate_solves(extra):
             one.ssprk3(dts[i], 3)
             assert np.all(np.isfinite(got[i]))
             assert np.array_equal(got[i], one.get_state()), (prec, sched, i)
+
+
+def test_bounded_wait_expires_and_context_stays_usable():
+    """Failure detection of the persistent schedule without a GPU fault: a wait whose completion
+    count can never be reached (dg_watchdog_selftest raises face region 0's required count by one)
+    gives up after a few thousand polls; the kernel returns, the host reads DG_E_WATCHDOG, and the
+    same context then steps exactly like one that never saw the expired wait."""
+    import ctypes
+    from fve_dg_b200 import _lib as L
+    P, qv, qf = 2, 1, 2
+    m, U = vortex_mesh_state(4, P, 3)
+    a = ExplicitConvection(m, order=P, quad_vol=qv, quad_face=qf, precision="mixed", schedule="persistent")
+    b = ExplicitConvection(m, order=P, quad_vol=qv, quad_face=qf, precision="mixed", schedule="persistent")
+    a.set_state(U)
+    assert L.lib().dg_watchdog_selftest(a._ctx, ctypes.c_int64(4096)) == L.DG_E_WATCHDOG
+    assert L.lib().dg_watchdog_selftest(a._ctx, ctypes.c_int64(0)) == L.DG_E_ARG
+    b.set_state(U)
+    for c in (a, b):
+        c.ssprk3(1e-3, 3)
+    assert np.array_equal(a.get_state(), b.get_state())
+    a.ssprk3(1e-3, 2, graph=True)  # graph replay on the same context after the expired wait
+    b.ssprk3(1e-3, 2, graph=True)
+    assert np.array_equal(a.get_state(), b.get_state())
+    two = ExplicitConvection(m, order=P, quad_vol=qv, quad_face=qf, precision="mixed")
+    two.set_state(U)
+    assert L.lib().dg_watchdog_selftest(two._ctx, ctypes.c_int64(4096)) == L.DG_E_ARG  # two-launch form: no waits
