@@ -136,6 +136,11 @@ def kernel_bytes(name, P, ncell, nface, nqf):
     nb = nb_of(P)
     state = ncell * 5 * nb * 8
     face_rec, elem_rec = 48, 80 + 32     # face record; element geometry + face list
+    gp = (nqf + 7) // 8 * 8
+    if name == "face_flux_tc":           # state read, face records + group records, FP64 face fluxes written
+        return state + nface * face_rec + nface * 16 // 3 + nface * 5 * gp * 8
+    if name == "element_tc":             # stage state + U^n read, new stage written, det J J^-T + 1/det J,
+        return 3 * state + ncell * 80 + ncell * 96 // 3 + nface * 5 * gp * 8 * 2  # group records, Fh from both sides
     if name == "face_flux_fp64":         # state read, face records, FP64 face fluxes written
         return state + nface * face_rec + nface * nqf * 5 * 8
     if name == "element_fp64":           # stage state + U^n read, new stage written, face fluxes read
@@ -304,6 +309,9 @@ def main():
                          "timed as its own kernel class), e.g. 1/1600 for the Taylor-Green vortex at Re 1600")
     ap.add_argument("--prandtl", type=float, default=0.71)
     ap.add_argument("--n", type=int, default=0, help="override the mesh size (cubes per side), for profiling")
+    ap.add_argument("--order-sweep", action="store_true",
+                    help="P1..P4 on the workload's mesh: the mixed form (two-launch, and batched with the autotuner's "
+                         "tiles) against the FP64 form per order, with the autotuner's record per order")
     ap.add_argument("--split", action="store_true",
                     help="one mesh split across the N ranks (element slabs with ghost elements), SSP-RK3 one "
                          "stage at a time with the NCCL halo exchange before every stage (strong scaling)")
@@ -333,6 +341,11 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    if args.order_sweep:
+        run_order_sweep(args, cfg, rank, world, local, dist)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.config == "ensemble":
         run_ensemble(args, rank, world, local, dist)
         if dist:
@@ -392,11 +405,32 @@ def main():
                          "roofline": make_roofline(kt64, "fp64", "two-launch", P, m.ncell, m.nface, conv.nq_face, nb,
                                                    args.config)}
         forms["mixed_over_fp64"] = forms["mixed"]["value"] / forms["fp64"]["value"]
-        # accuracy: both forms stepped the configuration's number of steps from U0 with the same dt
+        ctxs = {"mixed": conv, "fp64": f64}
+        if schedule == "two-launch":
+            # the batched form: one persistent launch per RK stage over the tile queue, the tiles chosen
+            # by the autotuner on this mesh, one CUDA graph per step
+            bat = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf, precision="mixed",
+                                     device=local, schedule="persistent", limiter=args.limiter, mu=args.mu,
+                                     prandtl=args.prandtl)
+            bat.set_state(U0)
+            tune = bat.autotune(dt)
+            ms_b, _ = time_steps(bat, dt, args.warmup, args.steps, dist, torch, launch_count)
+            ktb = bat.ssprk3_timed(dt, 3)
+            vb = dof_stage_per_step * args.steps * world / (ms_b / 1e3)
+            forms["mixed_batched"] = {"value": vb, "ms_per_step": ms_b / args.steps, "schedule": "persistent",
+                                      "kernels_ms_per_launch": {KNAMES[("mixed", "persistent")].get(k, str(k)):
+                                                                v[0] / v[1] for k, v in ktb.items()}}
+            forms["mixed_batched_over_fp64"] = vb / forms["fp64"]["value"]
+            ctxs["mixed_batched"] = bat
+        # accuracy: every form stepped the configuration's number of steps from U0 with the same dt
         # (untimed, independent of --steps)
-        accuracy = accuracy_report(conv, f64, U0, dt, m, P, cfg, args.config, problems)
-        forms["mixed"]["l2_vs_fp64"] = accuracy.pop("l2_mixed_vs_fp64")
-        f64.close()
+        accuracy = accuracy_report(ctxs, U0, dt, m, P, cfg, args.config, problems)
+        for name in ctxs:
+            if name != "fp64":
+                forms[name]["l2_vs_fp64"] = accuracy.pop("l2_" + name + "_vs_fp64")
+        for name, c in ctxs.items():
+            if c is not conv:
+                c.close()
     cons = conv.conservation()
 
     # end to end through the public API: H2D of the state from pinned memory, one SSP-RK3 step,
@@ -435,26 +469,32 @@ def main():
 RUN_STEPS = {"tgv": 100, "dwave": 200, "dwave_p4": 50, "vortex": 20, "ensemble": 20}
 
 
-def accuracy_report(conv, f64, U0, dt, m, P, cfg, config, problems):
-    """Both forms stepped RUN_STEPS[config] SSP-RK3 steps from U0 with the same dt: the mixed form's
-    relative L2 error against the FP64 form per variable (momenta also against the norm of the whole
-    momentum field), the drift of mass, energy and kinetic energy of each form over the run, and for
-    the density wave the error of each form against the exact translated solution."""
+def accuracy_report(ctxs, U0, dt, m, P, cfg, config, problems):
+    """Every form in ctxs ({name: context}, one named 'fp64') stepped RUN_STEPS[config] SSP-RK3 steps
+    from U0 with the same dt: each other form's relative L2 error against the FP64 form per variable
+    (momenta also against the norm of the whole momentum field), the drift of mass, energy and kinetic
+    energy of each form over the run, and for the density wave the error of each form against the
+    exact translated solution."""
     n = RUN_STEPS.get(config, 100)
+    f64 = ctxs["fp64"]
     f64.set_state(U0)
     c0 = f64.conservation()
     out = {"after_steps": n, "t": n * dt}
     states, cons = {}, {}
-    for name, c in (("mixed", conv), ("fp64", f64)):
+    for name, c in ctxs.items():
         c.set_state(U0)
         c.ssprk3(dt, n, graph=True)
         states[name] = c.get_state()
         cons[name] = c.conservation()
-    err = problems.l2_errors(m, P, states["mixed"], Uref=states["fp64"])
-    errm = problems.l2_errors(m, P, states["mixed"], Uref=states["fp64"], momentum_norm=True)
-    out["l2_mixed_vs_fp64"] = {"rho": float(err[0]), "rhou": float(err[1]), "rhov": float(err[2]),
-                               "rhow": float(err[3]), "E": float(err[4]),
-                               "momenta_over_momentum_norm": [float(x) for x in errm[1:4]], "after_steps": n}
+    for name in states:
+        if name == "fp64":
+            continue
+        err = problems.l2_errors(m, P, states[name], Uref=states["fp64"])
+        errm = problems.l2_errors(m, P, states[name], Uref=states["fp64"], momentum_norm=True)
+        out["l2_" + name + "_vs_fp64"] = {"rho": float(err[0]), "rhou": float(err[1]), "rhov": float(err[2]),
+                                          "rhow": float(err[3]), "E": float(err[4]),
+                                          "momenta_over_momentum_norm": [float(x) for x in errm[1:4]],
+                                          "after_steps": n}
     for name in states:
         c = cons[name]
         out[name] = {"mass_drift": float((c[0] - c0[0]) / c0[0]), "energy_drift": float((c[4] - c0[4]) / c0[4]),
@@ -468,7 +508,7 @@ def accuracy_report(conv, f64, U0, dt, m, P, cfg, config, problems):
     return out
 
 
-KNAMES = {("fp64", "two-launch"): {0: "face_flux_fp64", 1: "element_fp64", 3: "viscous", 4: "limiter"},
+KNAMES = {("fp64", "two-launch"): {0: "face_flux_tc", 1: "element_tc", 3: "viscous", 4: "limiter"},
           ("mixed", "two-launch"): {0: "face_flux_mixed", 1: "element_mixed", 3: "viscous", 4: "limiter"},
           ("mixed", "persistent"): {2: "stage_persistent_mixed", 3: "viscous", 4: "limiter"}}
 
@@ -751,6 +791,64 @@ def run_split(args, cfg, rank, world, local, dist):
                 "gpu_launches": launches, "halo": halo, "e2e": None}
         print(json.dumps(line), flush=True)
     pc.conv.close()
+
+
+# the configurations' rules per order: (tet rule, triangle rule)
+ORDER_RULES = {1: (0, 1), 2: (1, 2), 3: (3, 3), 4: (5, 3)}
+
+
+def run_order_sweep(args, cfg, rank, world, local, dist):
+    """P1..P4 on the workload's mesh and problem with each order's configuration rules: DOF-stage/s of
+    the FP64 form, the mixed form with two launches per stage and the batched mixed form (one
+    persistent launch per stage, tiles chosen by the autotuner, whose record is kept per order), and
+    the density/energy error of the mixed form against FP64 after RUN_STEPS of the workload (at most
+    50). One JSON line; rank 0 prints."""
+    import torch
+    from fve_dg_b200 import ExplicitConvection, box_mesh, launch_count, problems
+    m = box_mesh(cfg["n"], hi=(cfg["L"],) * 3, jitter=cfg["jitter"])
+    rows = []
+    for P in (1, 2, 3, 4):
+        qv, qf = ORDER_RULES[P]
+        U0 = problems.project(m, P, problem_fn(cfg["problem"], problems))
+        ctxs = {}
+        for name, prec, sched in (("fp64", "fp64", "two-launch"), ("mixed", "mixed", "two-launch"),
+                                  ("mixed_batched", "mixed", "persistent")):
+            ctxs[name] = ExplicitConvection(m, order=P, flux=cfg["flux"], quad_vol=qv, quad_face=qf, precision=prec,
+                                            device=local, schedule=sched)
+            ctxs[name].set_state(U0)
+        dt = problems.cfl_dt(CFL, cfg["L"] / cfg["n"], P, ctxs["fp64"].max_wave_speed())
+        tune = ctxs["mixed_batched"].autotune(dt)
+        dof = 5 * ctxs["fp64"].num_basis * m.ncell * 3
+        row = {"order": P, "quad_vol": qv, "quad_face": qf, "dof_per_stage": dof // 3}
+        for name, c in ctxs.items():
+            ms, _ = time_steps(c, dt, args.warmup, args.steps, dist, torch, launch_count)
+            row[name] = {"value": dof * args.steps * world / (ms / 1e3), "ms_per_step": ms / args.steps}
+        row["mixed_over_fp64"] = row["mixed"]["value"] / row["fp64"]["value"]
+        row["mixed_batched_over_fp64"] = row["mixed_batched"]["value"] / row["fp64"]["value"]
+        n = min(50, RUN_STEPS.get(args.config, 50))
+        states = {}
+        for name, c in ctxs.items():
+            c.set_state(U0)
+            c.ssprk3(dt, n, graph=True)
+            states[name] = c.get_state()
+        for name in ("mixed", "mixed_batched"):
+            e = problems.l2_errors(m, P, states[name], Uref=states["fp64"])
+            row[name]["l2_vs_fp64"] = {"rho": float(e[0]), "E": float(e[4]), "after_steps": n}
+        row["autotune"] = tune
+        rows.append(row)
+        for c in ctxs.values():
+            c.close()
+    if rank == 0:
+        best = max(rows, key=lambda r: r["mixed_batched"]["value"])
+        line = {"metric": METRIC, "value": rows[-1]["mixed_batched"]["value"], "unit": "DOF-stage/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": rows[-1]["mixed_batched"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16x3 contractions, f32 flux, f64 state", "data": "synthetic",
+                "config": {"workload": args.config + "-order-sweep", "desc": cfg["desc"] + "; orders 1..4 with the "
+                           "configurations' rules", "tets": m.ncell, "value_is": "P4 batched mixed form",
+                           "fastest_batched_order": best["order"]},
+                "orders": rows}
+        print(json.dumps(line), flush=True)
 
 
 def run_ensemble(args, rank, world, local, dist):

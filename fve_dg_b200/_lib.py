@@ -24,7 +24,10 @@ STATUS = {0: "DG_OK", -1: "DG_E_ARG", -2: "DG_E_MESH", -3: "DG_E_CUDA", -4: "DG_
 class DGError(RuntimeError):
     def __init__(self, code, what):
         self.code = code
-        super().__init__(f"{what}: {STATUS.get(code, code)}")
+        msg = f"{what}: {STATUS.get(code, code)}"
+        if code == -3 and _lib is not None:  # DG_E_CUDA: name the CUDA error behind it
+            msg += f" ({_lib.dg_last_cuda_error().decode()})"
+        super().__init__(msg)
 
 
 class MeshDesc(ctypes.Structure):
@@ -64,6 +67,7 @@ def lib():
         "dg_residual_device": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, ctypes.c_int, vp]),
         "dg_residual_device_static": (ctypes.c_int, [vp, vp, vp, ctypes.c_int, vp]),
         "dg_watchdog_selftest": (ctypes.c_int, [vp, ctypes.c_int64]),
+        "dg_last_cuda_error": (ctypes.c_char_p, []),
         "dg_static_scratch_capacity": (ctypes.c_int64, []),
         "dg_set_state": (ctypes.c_int, [vp, c_double_p, ctypes.c_size_t]),
         "dg_get_state": (ctypes.c_int, [vp, c_double_p, ctypes.c_size_t]),
@@ -124,7 +128,7 @@ def exported_symbols():
             "dg_save_checkpoint", "dg_load_checkpoint",
             "dg_set_dirichlet", "dg_conservation",
             "dg_max_wave_speed", "dg_check_state", "dg_info", "dg_mesh_geometry", "dg_face_perms", "dg_basis",
-            "dg_quad_rule", "dg_auto_rules", "dg_status_string", "dg_launch_count", "dg_box_mesh_create",
+            "dg_quad_rule", "dg_auto_rules", "dg_status_string", "dg_last_cuda_error", "dg_launch_count", "dg_box_mesh_create",
             "dg_box_mesh_destroy", "dg_box_mesh_view"]
 
 

@@ -14,6 +14,7 @@
 #include "dg_internal.h"
 #include "dg_kernels_fp64.cuh"
 #include "dg_kernels_mixed.cuh"
+#include "dg_kernels_fp64_tc.cuh"
 #include "dg_persistent.cuh"
 #include "dg_limiter.cuh"
 #include "dg_viscous.cuh"
@@ -24,11 +25,11 @@ using namespace fvedg;
 namespace {
 std::atomic<int64_t> g_launches{0};
 
-inline int cuda_ok(cudaError_t e) { return e == cudaSuccess ? DG_OK : DG_E_CUDA; }
+inline int cuda_ok(cudaError_t e) { return cuda_status(e); }
 #define DG_CUDA(x)                                   \
     do {                                             \
         cudaError_t e_ = (x);                        \
-        if (e_ != cudaSuccess) return DG_E_CUDA;     \
+        if (e_ != cudaSuccess) return cuda_status(e_); \
     } while (0)
 
 template <typename T>
@@ -74,6 +75,7 @@ struct dg_ctx {
     double* d_red = nullptr;       // reduction partials
     double* d_red_out = nullptr;
     MixedData mixed;               // mixed-precision form buffers
+    TcData tc;                     // FP64 form on the FP64 tensor cores (the configurations' rules)
     bool have_state = false;
     bool has_dirichlet = false;    // some boundary face is Dirichlet: U_D must be set first
     cudaGraphExec_t graph = nullptr;
@@ -253,14 +255,54 @@ StageArgs stage_args(dg_ctx* c, const double* U, const double* U0, double* out, 
     return a;
 }
 
+TcFaceArgs tc_face_args(dg_ctx* c, const double* U, int mask) {
+    TcFaceArgs a;
+    a.U = U; a.fi = c->d_fi; a.groups = c->tc.fgroups; a.ngroups = c->tc.nfgroups; a.UD = c->d_UD; a.Fh = c->tc.Fh;
+    a.t = c->tc.t; a.gamma = c->cfg.gamma; a.flux = c->cfg.flux; a.faces_mask = mask; a.chk = c->tc.chk;
+    return a;
+}
+
+TcElemArgs tc_elem_args(dg_ctx* c, const double* U, const double* U0, double* out, int mode, double dt, double a0,
+                        double a1, int with_volume) {
+    TcElemArgs a;
+    a.U = U; a.U0 = U0; a.out = out; a.Fh = c->tc.Fh; a.jd = c->tc.jd; a.inv_detj = c->tc.inv_detj;
+    a.groups = c->tc.egroups; a.ngroups = c->tc.negroups; a.t = c->tc.t; a.gamma = c->cfg.gamma;
+    a.with_volume = with_volume; a.mode = mode; a.dt = dt; a.a0 = a0; a.a1 = a1;
+    a.dt_inst = mode == 1 ? c->d_dt_inst : nullptr; a.elem_inst = c->d_elem_inst;
+    a.Rv = (mode == 1 && c->cfg.mu > 0.0) ? c->d_Rv : nullptr;
+    a.chk = c->tc.chk;
+    return a;
+}
+
+// Face-flux launch of the FP64 form (tensor-core kernels where the rules have them).
+int fp64_face(dg_ctx* c, const double* U, int mask, cudaStream_t s) {
+    if (c->tc.ready) {
+        ++g_launches;
+        return tc_kernel(c->tc, 0, tc_face_args(c, U, mask), TcElemArgs{}, s);
+    }
+    return dispatch_face(c->cfg.order, c->qv, c->qf, face_args(c, U, mask), s);
+}
+
+// Element launch of the FP64 form: R (mode 0) or the RK stage out = a0 U0 + a1 (U + dt L) (mode 1).
+int fp64_element(dg_ctx* c, const double* U, const double* U0, double* out, int mode, double dt, double a0,
+                 double a1, int with_volume, cudaStream_t s) {
+    if (c->tc.ready) {
+        ++g_launches;
+        return tc_kernel(c->tc, 1, TcFaceArgs{}, tc_elem_args(c, U, U0, out, mode, dt, a0, a1, with_volume), s);
+    }
+    StageArgs sa = stage_args(c, U, U0, out, mode, dt, a0, a1, with_volume);
+    sa.Rv = (mode == 1 && c->cfg.mu > 0.0) ? c->d_Rv : nullptr;
+    return dispatch_element(c->cfg.order, c->qv, c->qf, sa, s);
+}
+
 // One residual evaluation on device buffers (packed layout), FP64 form.
 int residual_fp64(dg_ctx* c, const double* U, double* R, int part, cudaStream_t s) {
     if (c->cfg.flux != DG_FLUX_LF && c->cfg.flux != DG_FLUX_ROE) return DG_E_ARG;
     if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
     const int mask = part == 0 ? 3 : part == 1 ? 0 : part == 2 ? 1 : 2;
-    int rc = dispatch_face(c->cfg.order, c->qv, c->qf, face_args(c, U, mask), s);
+    int rc = fp64_face(c, U, mask, s);
     if (rc) return rc;
-    return dispatch_element(c->cfg.order, c->qv, c->qf, stage_args(c, U, U, R, 0, 0.0, 0.0, 0.0, part == 0 || part == 1), s);
+    return fp64_element(c, U, U, R, 0, 0.0, 0.0, 0.0, part == 0 || part == 1, s);
 }
 
 // Launch `fn` (which enqueues one kernel on stream s), bracketed by timing events when enabled.
@@ -369,13 +411,9 @@ int step_fp64(dg_ctx* c, double dt, cudaStream_t s, int st0, int st1) {
     for (int st = st0; st < st1; ++st) {
         int rc = viscous_stage(c, in[st], s);
         if (rc) return rc;
-        rc = timed(c, 0, s, [&] { return dispatch_face(c->cfg.order, c->qv, c->qf, face_args(c, in[st], 3), s); });
+        rc = timed(c, 0, s, [&] { return fp64_face(c, in[st], 3, s); });
         if (rc) return rc;
-        rc = timed(c, 1, s, [&] {
-            StageArgs sa = stage_args(c, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 1);
-            sa.Rv = c->cfg.mu > 0.0 ? c->d_Rv : nullptr;
-            return dispatch_element(c->cfg.order, c->qv, c->qf, sa, s);
-        });
+        rc = timed(c, 1, s, [&] { return fp64_element(c, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 1, s); });
         if (rc) return rc;
         if ((rc = limit_stage(c, st, in[st], out[st], nullptr, s))) return rc;
     }
@@ -475,6 +513,7 @@ void free_ctx(dg_ctx* c) {
         if (p) cudaFree(p);
     free_schedule(c->qs);
     free_mixed(c->mixed);
+    free_tc(c->tc);
     if (c->d_queue) cudaFree(c->d_queue);
     if (c->d_dt_inst) cudaFree(c->d_dt_inst);
     if (c->d_lim_bnd) cudaFree(c->d_lim_bnd);
@@ -513,6 +552,11 @@ const char* dg_status_string(int s) {
 }
 
 int64_t dg_launch_count(void) { return g_launches.load(); }
+
+const char* dg_last_cuda_error(void) {
+    const int e = last_cuda_error_slot().load();
+    return e ? cudaGetErrorName((cudaError_t)e) : "cudaSuccess";
+}
 
 }  // extern "C"
 
@@ -606,7 +650,8 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
         (rc = upload(&c->d_w_v, c->tab.w_v)) || (rc = upload(&c->d_phi_f, c->tab.phi_f)) ||
         (rc = upload(&c->d_phi_fT, c->tab.phi_fT)) || (rc = upload(&c->d_phi_vT, c->tab.phi_vT)) ||
         (rc = upload(&c->d_w_f, c->tab.w_f)) || (rc = upload(&c->d_mass_ref, c->tab.mass_ref)) ||
-        (rc = dev_alloc(&c->d_Fh, cfg->precision == DG_PREC_FP64 ? (size_t)c->nface * nqf * 5 : 0)) ||
+        (rc = dev_alloc(&c->d_Fh, (cfg->precision == DG_PREC_FP64 && !tc_supported(cfg->order, qv, qf))
+                                      ? (size_t)c->nface * nqf * 5 : 0)) ||
         (rc = dev_alloc(&c->d_Un, nstate)) ||
         (rc = dev_alloc(&c->d_Ua, nstate)) || (rc = dev_alloc(&c->d_Ub, nstate)) ||
         (rc = dev_alloc(&c->d_red, (size_t)kRedBlocks * 8)) || (rc = dev_alloc(&c->d_red_out, 8)))
@@ -619,6 +664,9 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
             for (int64_t e = (*inst_off)[i]; e < (*inst_off)[i + 1]; ++e) inst[e] = i;
         std::vector<double> dts(c->ninst, 0.0);
         if ((rc = upload(&c->d_elem_inst, inst)) || (rc = upload(&c->d_dt_inst, dts))) return fail(c, rc);
+    }
+    if (cfg->precision == DG_PREC_FP64 && tc_supported(cfg->order, qv, qf)) {
+        if ((rc = init_tc(c->tc, c->tab, hgeo, hfi, hef, c->ncell, c->nowned, c->nface, qv, qf))) return fail(c, rc);
     }
     if (cfg->precision == DG_PREC_MIXED) {
         rc = init_mixed(c->mixed, c->tab, hgeo, hfi, hef, c->ncell, c->nowned, c->nface, cfg->gamma, cfg->flux, qv, qf,
@@ -1032,6 +1080,17 @@ int dg_ssprk3_timed(dg_ctx* c, double dt, int nsteps, double* out, int nclass) {
     }
     return DG_OK;
 }
+
+#ifdef FVEDG_TC_CHECK
+// Checked builds only: the first failed bounds or alignment check of the tensor-core FP64 kernels
+// (code, index), cleared on read.
+int dg_debug_tc_check(dg_ctx* c, int* out) {
+    if (!c || !c->tc.chk.err) return DG_E_ARG;
+    if (cudaDeviceSynchronize() != cudaSuccess) return DG_E_CUDA;
+    if (cudaMemcpy(out, c->tc.chk.err, 2 * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return DG_E_CUDA;
+    return cudaMemset(c->tc.chk.err, 0, 2 * sizeof(int)) == cudaSuccess ? DG_OK : DG_E_CUDA;
+}
+#endif
 
 int dg_watchdog_selftest(dg_ctx* c, int64_t polls) {
     if (!c || polls < 1) return DG_E_ARG;

@@ -8,6 +8,7 @@
 // averages, the five characteristic waves of 3D Euler, Harten's entropy fix on the acoustic waves
 // with delta = 0.1 c_roe.
 #pragma once
+#include "dg_status.cuh"
 
 namespace fvedg {
 
@@ -115,6 +116,99 @@ struct Phys {
         for (int k = 0; k < 5; ++k) Fh[k] = T(0.5) * (FL[k] + FR[k]) - T(0.5) * D[k];
     }
 };
+
+// FP64 forms for the tensor-core FP64 kernels: the same fluxes as Phys<double> with fewer divisions
+// and square roots (each costs a multi-instruction sequence in FP64). One reciprocal square root per
+// state gives both sqrt(rho) = rho q and 1/rho = q^2 (q = rsqrt(rho)); H = (E + p)/rho uses that
+// reciprocal; the Roe sound speed and 1/c^2 come from one rsqrt of c^2; the LF wave speeds from
+// rsqrt as well. Agreement with Phys<double> is a few ulp per point, far inside the 1e-12 parity bar.
+struct StateF64 {
+    double r, ir, u[3], p, e, un, mn;  // clamped density, 1/rho, velocity, pressure, E + p, u.n, m.n
+};
+
+__device__ __forceinline__ StateF64 state_f64(const double U[5], const double n[3], double gm1, double& q) {
+    StateF64 s;
+    s.r = U[0] > 1e-16 ? U[0] : 1e-16;
+    q = rsqrt(s.r);
+    s.ir = q * q;
+    #pragma unroll
+    for (int i = 0; i < 3; ++i) s.u[i] = U[1 + i] * s.ir;
+    const double k = s.u[0] * U[1] + s.u[1] * U[2] + s.u[2] * U[3];  // rho |u|^2
+    s.p = gm1 * fma(-0.5, k, U[4]);
+    s.e = U[4] + s.p;
+    s.mn = U[1] * n[0] + U[2] * n[1] + U[3] * n[2];
+    s.un = s.mn * s.ir;
+    return s;
+}
+
+__device__ __forceinline__ void roe_f64(const double UL[5], const double UR[5], const double n[3], double gam,
+                                        double Fh[5]) {
+    const double gm1 = gam - 1.0;
+    double qL, qR;
+    const StateF64 L = state_f64(UL, n, gm1, qL), R = state_f64(UR, n, gm1, qR);
+    const double sL = L.r * qL, sR = R.r * qR;  // sqrt(rho)
+    const double iden = 1.0 / (sL + sR);
+    const double wL = sL * iden, wR = sR * iden;
+    double ut[3];
+    #pragma unroll
+    for (int i = 0; i < 3; ++i) ut[i] = fma(wL, L.u[i], wR * R.u[i]);
+    const double Ht = fma(wL, L.e * L.ir, wR * (R.e * R.ir));
+    const double q2 = ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2];
+    const double c2r = gm1 * fma(-0.5, q2, Ht);
+    const double c2 = c2r > 1e-16 ? c2r : 1e-16;
+    const double qc = rsqrt(c2);
+    const double ct = c2 * qc, ic2 = qc * qc;
+    const double rt = sL * sR;
+    const double unt = ut[0] * n[0] + ut[1] * n[1] + ut[2] * n[2];
+    const double dr = R.r - L.r, dp = R.p - L.p, dun = R.un - L.un;
+    double l1 = fabs(unt - ct), l5 = fabs(unt + ct);
+    const double l2 = fabs(unt);
+    const double delta = 0.1 * ct, d2 = delta * delta;
+    if (l1 < delta || l5 < delta) {  // Harten's fix, rarely active
+        const double ihd = 0.5 / delta;
+        if (l1 < delta) l1 = fma(l1, l1, d2) * ihd;
+        if (l5 < delta) l5 = fma(l5, l5, d2) * ihd;
+    }
+    const double rcd = rt * ct * dun, h2 = 0.5 * ic2;
+    const double w1 = l1 * ((dp - rcd) * h2), w5 = l5 * ((dp + rcd) * h2), w2 = l2 * fma(-dp, ic2, dr);
+    const double W = w1 + w5 + w2, cw = ct * (w5 - w1), lrt = l2 * rt;
+    double uds = 0.0, D[5];
+    D[0] = W;
+    #pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const double sh = fma(-dun, n[i], R.u[i] - L.u[i]);
+        uds = fma(ut[i], sh, uds);
+        D[1 + i] = fma(W, ut[i], fma(cw, n[i], lrt * sh));
+    }
+    D[4] = fma(w1 + w5, Ht, fma(cw, unt, fma(0.5 * w2, q2, lrt * uds)));
+    const double ps = L.p + R.p;
+    Fh[0] = 0.5 * (L.mn + R.mn - D[0]);
+    #pragma unroll
+    for (int i = 0; i < 3; ++i) Fh[1 + i] = 0.5 * (fma(UL[1 + i], L.un, fma(UR[1 + i], R.un, ps * n[i])) - D[1 + i]);
+    Fh[4] = 0.5 * (fma(L.un, L.e, R.un * R.e) - D[4]);
+}
+
+__device__ __forceinline__ void lax_friedrichs_f64(const double UL[5], const double UR[5], const double n[3],
+                                                   double gam, double Fh[5]) {
+    const double gm1 = gam - 1.0;
+    double qL, qR;
+    const StateF64 L = state_f64(UL, n, gm1, qL), R = state_f64(UR, n, gm1, qR);
+    auto speed = [&](const StateF64& s) {  // |u| + sqrt(gamma max(p/rho, 1e-16)) (EulerPhysicalFlux.cpp:70-81)
+        const double v2 = s.u[0] * s.u[0] + s.u[1] * s.u[1] + s.u[2] * s.u[2];
+        const double pr = s.p * s.ir;
+        const double c2 = gam * (pr > 1e-16 ? pr : 1e-16);
+        const double v = v2 > 0.0 ? v2 * rsqrt(v2) : 0.0;
+        return v + c2 * rsqrt(c2);
+    };
+    const double a = speed(L), b = speed(R);
+    const double lam = a > b ? a : b;
+    Fh[0] = 0.5 * fma(lam, UL[0] - UR[0], L.mn + R.mn);
+    const double ps = L.p + R.p;
+    #pragma unroll
+    for (int i = 0; i < 3; ++i)
+        Fh[1 + i] = 0.5 * fma(lam, UL[1 + i] - UR[1 + i], fma(UL[1 + i], L.un, fma(UR[1 + i], R.un, ps * n[i])));
+    Fh[4] = 0.5 * fma(lam, UL[4] - UR[4], fma(L.un, L.e, R.un * R.e));
+}
 
 // FP32 forms for the mixed-precision kernels: the same fluxes as Phys<float>, reorganised for fewer
 // instructions. The momenta are used directly (rho u = m, rho u.n = m.n, rho e = E), each state

@@ -1022,7 +1022,7 @@ inline int mixed_launch(MixedData& m, int which, const double* U, const double* 
         element_mixed<NB, NQV, NQF, WE><<<g, WE * 32, smem, s>>>(
             elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out));
     }
-    return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;
+    return cuda_status(cudaGetLastError());
 }
 
 // mir_in: mirror of U (0..3); mir_out: mirror the update writes (RK mode), or -1.
@@ -1071,7 +1071,7 @@ inline int mixed_mirror_list(MixedData& m, const double* U, int mir, const int64
         const int64_t nt = n * 5 * (pad8(NB - 1) / 2);                                                  \
         ++*launches;                                                                                    \
         mirror_split<NB><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(U, m.mir[mir], n, list);          \
-        return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;                                   \
+        return cuda_status(cudaGetLastError());                                   \
     }
     FVEDG_MIXED_COMBOS(X)
 #undef X

@@ -25,6 +25,7 @@
 #include <cfloat>
 
 #include "dg_kernels_fp64.cuh"
+#include "dg_status.cuh"
 #include "dg_kernels_mixed.cuh"
 
 namespace fvedg {
@@ -372,7 +373,7 @@ inline int launch_limiter(int order, int qv, double* U, const double* Uprev, con
         limiter_cell_stats<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(Uprev, phi_v, 0, ncell, only_avg, stats);      \
         limiter_apply<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(U, nbr, stats, phi_v, napply, gamma, only_avg, mir,  \
                                                              nullptr);                                           \
-        return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;                                            \
+        return cuda_status(cudaGetLastError());                                            \
     }
     FVEDG_LIMITER_COMBOS(X)
 #undef X
@@ -390,7 +391,7 @@ inline int launch_limiter_stats(int order, int qv, const double* U, const double
         const unsigned gs = (unsigned)std::min<int64_t>((n + kLimWarps - 1) / kLimWarps, (int64_t)sms * 16);    \
         limiter_cell_stats<NB, NQV><<<gs, kLimWarps * 32, 0, s>>>(U, phi_v, c_begin, c_end, only_avg, stats);   \
         ++*launches;                                                                                            \
-        return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;                                           \
+        return cuda_status(cudaGetLastError());                                           \
     }
     FVEDG_LIMITER_COMBOS(X)
 #undef X
@@ -414,7 +415,7 @@ inline int launch_limiter_stage(int order, int qv, double* U, const double* Uin,
         limiter_apply<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(U, nbr, stats_in, phi_v, napply, gamma, only_avg,    \
                                                              mir, stats_out);                                     \
         ++*launches;                                                                                              \
-        return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;                                             \
+        return cuda_status(cudaGetLastError());                                             \
     }
     FVEDG_LIMITER_COMBOS(X)
 #undef X

@@ -238,7 +238,7 @@ inline int persistent_launch(MixedData& m, QueueState* q, const QueueSchedule& q
     const MixedElemArgs ea = elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out);
     kern<<<m.sms * bps, W * 32, smem, s>>>(fa, ea, q, qs.tiles, qs.ntiles, qs.deps, qs.total,
                                            pp.spin_limit > 0 ? pp.spin_limit : kSpinLimit);
-    return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;
+    return cuda_status(cudaGetLastError());
 }
 
 inline int persistent_kernel(MixedData& m, QueueState* q, const QueueSchedule& qs, const PersistentParams& pp,

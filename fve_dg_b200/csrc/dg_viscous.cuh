@@ -40,6 +40,7 @@
 //                    atomics, a deterministic result.
 #pragma once
 #include "dg_kernels_fp64.cuh"
+#include "dg_status.cuh"
 
 namespace fvedg {
 
@@ -429,7 +430,7 @@ inline int launch_viscous(int order, const ViscArgs& a, int sms, cudaStream_t s)
         default: return DG_E_ARG;
     }
 #undef VISC_LAUNCH
-    return cudaGetLastError() == cudaSuccess ? DG_OK : DG_E_CUDA;
+    return cuda_status(cudaGetLastError());
 }
 
 }  // namespace fvedg

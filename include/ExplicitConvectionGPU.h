@@ -39,6 +39,8 @@ template <> struct rule_id<GaussLegendreTri::Degree4Points7> { static constexpr 
 template <> struct rule_id<GaussLegendreTri::Degree10Points24> { static constexpr int value = DG_TRI_D10P24; };
 
 inline void check(int rc, const char* what) {
+    if (rc == DG_E_CUDA)
+        throw std::runtime_error(std::string(what) + ": " + dg_status_string(rc) + " (" + dg_last_cuda_error() + ")");
     if (rc != DG_OK) throw std::runtime_error(std::string(what) + ": " + dg_status_string(rc));
 }
 

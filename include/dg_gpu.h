@@ -301,6 +301,9 @@ int dg_quad_rule(int kind, int id, double* pts, double* w);
 int dg_auto_rules(int order, int* quad_vol, int* quad_face);
 
 const char* dg_status_string(int status);
+/* Name of the CUDA error behind the most recent DG_E_CUDA of this process (cudaGetErrorName), or
+ * "cudaSuccess" if there was none. */
+const char* dg_last_cuda_error(void);
 
 /* Device name of the active context's GPU and the number of CUDA kernel launches issued by this
  * library since load (for launch accounting in benchmarks). */
