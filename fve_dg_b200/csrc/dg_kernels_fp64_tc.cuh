@@ -34,9 +34,31 @@ __host__ __device__ constexpr int pad4(int x) { return (x + 3) / 4 * 4; }
 // A shared-memory row stride >= n with stride % 16 == 8 doubles: the 16-byte stores of the
 // accumulator pattern (two rows x four column pairs per quarter warp) touch all 32 banks once.
 __host__ __device__ constexpr int ld_acc(int n) { return n % 16 == 8 ? n : n + ((8 - n % 16) + 16) % 16; }
-// A stride with stride % 16 == 4 doubles: the A-fragment loads (four rows x four consecutive
-// doubles per half warp) touch all 32 banks once.
-__host__ __device__ constexpr int ld_afrag(int n) { return n % 16 == 4 ? n : n + ((4 - n % 16) + 16) % 16; }
+// The smallest stride >= n with stride % 16 == 4 or 12 doubles: the A-fragment loads (four rows x
+// four consecutive doubles per half warp) then touch all 32 banks once.
+__host__ __device__ constexpr int ld_afrag(int n) {
+    return (n % 16 == 4 || n % 16 == 12) ? n : ld_afrag(n + 1);
+}
+
+// Launch bounds. The face kernel asks for five resident 4-warp CTAs per SM up to P3 (96 registers,
+// 3 % faster than the compiler's own 106-register choice on the Taylor-Green P3 mesh). The element
+// kernel gives only the block size: capping it at 72 or 64 registers (7 or 8 CTAs) spilled and took
+// 2.57 / 2.75 ms per launch against 1.66 ms. (An explicit minimum of one CTA per SM makes the compiler
+// spend up to 255 registers on unrolled loads, so the one-argument form is the default.)
+// FVEDG_TC_FACE_MINB = 0 / FVEDG_TC_ELEM_MINB select other budgets at build time.
+#ifndef FVEDG_TC_FACE_MINB
+#define FVEDG_TC_FACE_MINB 5
+#endif
+#if FVEDG_TC_FACE_MINB > 0
+#define TC_FACE_BOUNDS(W, NB) __launch_bounds__(W * 32, NB <= 20 ? FVEDG_TC_FACE_MINB : 4)
+#else
+#define TC_FACE_BOUNDS(W, NB) __launch_bounds__(W * 32)
+#endif
+#ifdef FVEDG_TC_ELEM_MINB
+#define TC_ELEM_BOUNDS(W, NB) __launch_bounds__(W * 32, NB <= 20 ? FVEDG_TC_ELEM_MINB : 4)
+#else
+#define TC_ELEM_BOUNDS(W, NB) __launch_bounds__(W * 32)
+#endif
 
 // Debug builds (-DFVEDG_TC_CHECK) check every global index against its buffer's length and every
 // 16-byte shared store for alignment: the first failure is recorded in a device word and the access
@@ -207,7 +229,7 @@ __device__ __forceinline__ void face_group_tc(const TcFaceArgs& a, int gi, TcFac
 }
 
 template <int NB, int NQF, int W>
-__global__ void __launch_bounds__(W * 32) face_flux_tc(TcFaceArgs a) {
+__global__ void TC_FACE_BOUNDS(W, NB) face_flux_tc(TcFaceArgs a) {
     __shared__ TcFaceSmem<NB, NQF> sm[W];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int gi = blockIdx.x * W + warp; gi < a.ngroups; gi += gridDim.x * W)
@@ -386,7 +408,7 @@ __device__ __forceinline__ void element_group_tc(const TcElemArgs& a, int gi, Tc
 }
 
 template <int NB, int NQV, int NQF, int W>
-__global__ void __launch_bounds__(W * 32) element_tc(TcElemArgs a) {
+__global__ void TC_ELEM_BOUNDS(W, NB) element_tc(TcElemArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double s_inv_mass[NB];
     for (int j = threadIdx.x; j < NB; j += blockDim.x) s_inv_mass[j] = a.t.inv_mass[j];
