@@ -233,7 +233,7 @@ def run_reference(args, cfg, rank):
     threads = os.cpu_count() or 1
     ref, rm, U, b, setup_s = oracle_setup(cfg)
     P = cfg["P"]
-    k, el, _ = time_reference_steps(rm, U, b, cfg, 1e-4, 150.0, args.steps)
+    k, el, _ = time_reference_steps(rm, U, b, cfg, 1e-4, 90.0, args.steps)
     dofs = 5 * nb_of(P) * rm.ncell * 3 * k
     val = dofs / el
     flux_note = "LF flux (the reference has no Roe solver)" if cfg["flux"] == "Roe" else "LF flux"

@@ -60,8 +60,11 @@ __host__ __device__ constexpr size_t persistent_warp_smem() {
     return ((a > b ? a : b) + 15) / 16 * 16;
 }
 
+#ifndef FVEDG_PERSIST_MINB8
+#define FVEDG_PERSIST_MINB8 4
+#endif
 template <int NB, int NQV, int NQF, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 8 ? 4 : 6)
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 8 ? FVEDG_PERSIST_MINB8 : 6)
     stage_persistent_mixed(MixedFaceArgs fa, MixedElemArgs ea, QueueState* q, const int4* __restrict__ tiles,
                            int ntiles, const unsigned long long* __restrict__ deps,
                            const unsigned int* __restrict__ total, long long spin_limit) {
