@@ -107,12 +107,17 @@ class ExplicitConvection:
         return t.value, step.value
 
     def autotune(self, dt):
-        """Time the persistent schedule's tile candidates on the current state (which is restored)
-        and keep the fastest; returns the JSON record of all candidates and the choice."""
+        """Time the mixed form's candidates on the current state (which is restored) and keep the
+        fastest: the tile queue of the persistent schedule, or the element kernel's shape of the
+        two-launch schedule. Returns the JSON record of all candidates and the choice."""
         buf = ctypes.create_string_buffer(1 << 14)
         L.check(L.lib().dg_autotune(self._ctx, float(dt), buf, len(buf)), "dg_autotune")
         import json
         return json.loads(buf.value.decode())
+
+    def set_element_shape(self, staged, ctas_per_sm=1):
+        """Pin the two-launch element kernel's shape (a choice dg_autotune records)."""
+        L.check(L.lib().dg_set_element_shape(self._ctx, int(bool(staged)), int(ctas_per_sm)), "dg_set_element_shape")
 
     def _state(self, U):
         U = L.as_f64(U)

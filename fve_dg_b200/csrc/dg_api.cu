@@ -475,10 +475,18 @@ int launches_per_step(const dg_ctx* c) {
     return 6 + lim;
 }
 
-// After a synchronize: the watchdog word of the persistent queue (DG_OK or DG_E_WATCHDOG).
+// After a synchronize: the watchdog words of the persistent queue and of the mixed kernels' bounded
+// waits (DG_OK or DG_E_WATCHDOG); a set word is cleared.
 int check_queue(dg_ctx* c) {
-    if (!c->d_queue) return DG_OK;
     int err = 0;
+    if (c->mixed.err) {
+        if (cudaMemcpy(&err, c->mixed.err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return DG_E_CUDA;
+        if (err != DG_OK) {
+            cudaMemset(c->mixed.err, 0, sizeof(int));
+            return DG_E_WATCHDOG;
+        }
+    }
+    if (!c->d_queue) return DG_OK;
     if (cudaMemcpy(&err, &c->d_queue->error, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return DG_E_CUDA;
     if (err == DG_OK) return DG_OK;
     cudaMemset(c->d_queue, 0, sizeof(QueueState));
@@ -913,6 +921,62 @@ int viscous_launch(dg_ctx* c, const double* U, double* R, double mu, double pran
     g_launches += 2;
     return launch_viscous(c->cfg.order, a, c->sms, s);
 }
+
+// dg_autotune for the two-launch mixed schedule: times each element-kernel shape (mixed_elem_shapes:
+// the kernel, warps per CTA, CTAs per SM) over two SSP-RK3 steps after one warm-up step, keeps the
+// fastest, restores U^n from `save` (which it frees) and writes the JSON record.
+int autotune_two_launch(dg_ctx* c, double dt, double* save, size_t nstate, char* report, size_t len) {
+    ElemShape shapes[3];
+    const int ns = mixed_elem_shapes(c->mixed, shapes);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::string js = "{\"schedule\": \"two-launch\", \"order\": " + std::to_string(c->cfg.order) +
+                     ", \"quad_vol\": " + std::to_string(c->qv) + ", \"quad_face\": " + std::to_string(c->qf) +
+                     ", \"ncell\": " + std::to_string(c->ncell) + ", \"knob\": \"element kernel shape\", \"candidates\": [";
+    const int keep_k = c->mixed.elem_kernel, keep_c = c->mixed.elem_ctas;
+    float best = 1e30f;
+    int bi = -1, rc = DG_OK;
+    auto name = [](const ElemShape& e) { return std::string(e.kernel == 2 ? "rows staged by TMA bulk copies" : "loads phase by phase"); };
+    for (int i = 0; i < ns && rc == DG_OK; ++i) {
+        c->mixed.elem_kernel = shapes[i].kernel;
+        c->mixed.elem_ctas = shapes[i].ctas;
+        rc = step(c, dt, c->stream);  // warm-up
+        cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < 2 && rc == DG_OK; ++r) rc = step(c, dt, c->stream);
+        cudaEventRecord(e1, c->stream);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = DG_E_CUDA;
+        if (rc == DG_OK) rc = check_queue(c);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms *= 0.5f;
+        js += std::string(i ? ", " : "") + "{\"element_kernel\": \"" + name(shapes[i]) + "\", \"warps_per_cta\": " +
+              std::to_string(shapes[i].warps) + ", \"elements_per_cta\": " + std::to_string(3 * shapes[i].warps) +
+              ", \"ctas_per_sm\": " + std::to_string(shapes[i].ctas) + ", \"ms_per_step\": " + std::to_string(ms) + "}";
+        if (rc == DG_OK && ms < best) { best = ms; bi = i; }
+    }
+    c->mixed.elem_kernel = bi >= 0 ? shapes[bi].kernel : keep_k;
+    c->mixed.elem_ctas = bi >= 0 ? shapes[bi].ctas : keep_c;
+    js += "], \"chosen\": ";
+    js += bi >= 0 ? "{\"element_kernel\": \"" + name(shapes[bi]) + "\", \"elements_per_cta\": " +
+                        std::to_string(3 * shapes[bi].warps) + ", \"ctas_per_sm\": " + std::to_string(shapes[bi].ctas) +
+                        ", \"ms_per_step\": " + std::to_string(best) + "}}"
+                  : std::string("null}");
+    cudaMemcpyAsync(c->d_Un, save, nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    mixed_mirror(c->mixed, c->d_Un, 0, c->stream, &g_launches);
+    c->lim_valid = false;
+    cudaStreamSynchronize(c->stream);
+    cudaFree(save);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    if (report && len > 0) {
+        const size_t n = std::min(len - 1, js.size());
+        std::memcpy(report, js.data(), n);
+        report[n] = 0;
+    }
+    return rc;
+}
 }  // namespace
 
 extern "C" {
@@ -1116,15 +1180,27 @@ int dg_watchdog_selftest(dg_ctx* c, int64_t polls) {
     return check_queue(c);
 }
 
+int dg_set_element_shape(dg_ctx* c, int staged, int ctas_per_sm) {
+    if (!c || c->cfg.precision != DG_PREC_MIXED || (staged != 0 && staged != 1)) return DG_E_ARG;
+    if (staged && ctas_per_sm != 1 && ctas_per_sm != 2) return DG_E_ARG;
+    if (staged && (5 * c->tab.nb * 8) % 16 != 0) return DG_E_ARG;  // state rows not whole 16-byte units
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    c->mixed.elem_kernel = staged ? 2 : 0;
+    c->mixed.elem_ctas = staged ? ctas_per_sm : 1;
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }  // a captured step used the old shape
+    return DG_OK;
+}
+
 int dg_autotune(dg_ctx* c, double dt, char* report, size_t len) {
     if (!c || !(dt >= 0)) return DG_E_ARG;
     if (!c->have_state) return DG_E_STATE;
-    if (c->cfg.precision != DG_PREC_MIXED || c->cfg.schedule != 1) return DG_E_ARG;
+    if (c->cfg.precision != DG_PREC_MIXED) return DG_E_ARG;
     DG_CUDA(cudaSetDevice(c->cfg.device));
     const size_t nstate = (size_t)c->ncell * 5 * c->tab.nb;
     double* save = nullptr;
     if (dev_alloc(&save, nstate)) return DG_E_NOMEM;
     DG_CUDA(cudaMemcpyAsync(save, c->d_Un, nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    if (c->cfg.schedule == 0) return autotune_two_launch(c, dt, save, nstate, report, len);
     // {face groups per tile, element groups per tile, CTAs per SM cap, regions, lag}
     static const int cand[][5] = {{32, 16, 0, 32, 1}, {16, 8, 0, 32, 1}, {64, 32, 0, 32, 1}, {32, 16, 0, 16, 1},
                                   {32, 16, 0, 64, 1}, {64, 32, 0, 64, 1}, {32, 16, 0, 32, 2}, {32, 16, 0, 64, 2},

@@ -42,6 +42,7 @@
 #include "dg_flux.cuh"
 #include "dg_internal.h"
 #include "dg_kernels_fp64.cuh"
+#include "dg_tma.cuh"
 
 namespace fvedg {
 
@@ -80,6 +81,22 @@ __host__ __device__ __forceinline__ int arow_lo_word(int x) {
     return arow_hi_word<K>(x) + ((x >> 4) < K / 16 ? 2 : 1);
 }
 
+// Face record of the mixed form, written by the face kernel and read by both elements of the face:
+//   words [0, 5 KF)        A rows (one per variable) of the split flux deviations 2A F(x_g) - Fref
+//   doubles [0, 5) after   Fref: the reference flux 2A F(c_0 of cells[0]) . n
+//   doubles [5, 10) after  S0: the mode-0 face integral sum_g w_g 2A F
+// face_rec_words(NQF) 32-bit words per face, a multiple of 4 (16 bytes) so that a face record is
+// one bulk copy.
+__host__ __device__ constexpr int face_rec_words(int nqf) { return 5 * pad8(nqf) + 20; }
+template <int NQF>
+__host__ __device__ __forceinline__ double* face_rec_fs(uint32_t* rec) {
+    return reinterpret_cast<double*>(rec + 5 * pad8(NQF));
+}
+template <int NQF>
+__host__ __device__ __forceinline__ const double* face_rec_fs(const uint32_t* rec) {
+    return reinterpret_cast<const double*>(rec + 5 * pad8(NQF));
+}
+
 struct MixedTables {  // device pointers
     const uint32_t* tfa;     // [24 maps] B fragments of the face traces: n = face point, k = mode - 1
     const uint32_t* tva;     // B fragments of the volume values: n = volume point, k = mode - 1
@@ -109,9 +126,7 @@ struct MixedFaceArgs {
     const FaceInfo* fi;
     const FaceGroup* groups;
     const double* UD;
-    uint32_t* dev;          // [nface][5][KF] A rows: 2A F(x_g) - Fref, the element kernel's operand
-    double* Fref;           // [nface][5] reference flux 2A F(c0 of cells[0]) . n
-    double* S0;             // [nface][5] sum_g w_g 2A F (the mode-0 face integral)
+    uint32_t* dev;          // [nface][face_rec_words] face records (layout at face_rec_words)
     MixedTables t;
     int ngroups;
     float gamma;
@@ -125,9 +140,7 @@ struct MixedElemArgs {
     double* out;
     const uint32_t* mir;     // U's split deviation coefficients
     uint32_t* mir_out;       // RK mode: the new stage's split deviation coefficients
-    const uint32_t* dev;     // face flux deviations (written by the face kernel)
-    const double* Fref;
-    const double* S0;
+    const uint32_t* dev;     // face records (written by the face kernel)
     const double* geo;       // [ncell][10] J^-T row-major, detJ
     const double* inv_detj;  // [ncell]
     const ElemGroup* groups;
@@ -140,6 +153,7 @@ struct MixedElemArgs {
     const double* dt_inst;   // optional per-instance time step (ensembles), indexed by elem_inst
     const int* elem_inst;    // [ncell] instance of each element
     const double* Rv;        // RK mode: viscous residual subtracted from R (Navier-Stokes), or null
+    int* err;                // device status word (DG_E_WATCHDOG when a bounded wait ran out), or null
 };
 
 // ---- MMA helpers ----------------------------------------------------------------------------------
@@ -283,14 +297,11 @@ __device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi,
     const bool interior = f0.c1 >= 0;
     const bool active = interior ? (a.faces_mask & 1)
                                  : ((a.faces_mask & 2) && ((bc == 0 && a.UD != nullptr) || bc == 5));
+    constexpr int FR = face_rec_words(NQF);
     if (!active) {
-        for (int i = lane; i < grp.n * 5 * KF; i += 32) {
-            const int fl = i / (5 * KF);
-            a.dev[(int64_t)grp.f[fl] * 5 * KF + (i - fl * 5 * KF)] = 0u;
-        }
-        for (int i = lane; i < grp.n * 5; i += 32) {
-            a.Fref[(int64_t)grp.f[i / 5] * 5 + i % 5] = 0.0;
-            a.S0[(int64_t)grp.f[i / 5] * 5 + i % 5] = 0.0;
+        for (int i = lane; i < grp.n * FR; i += 32) {
+            const int fl = i / FR;
+            a.dev[(int64_t)grp.f[fl] * FR + (i - fl * FR)] = 0u;
         }
         return;
     }
@@ -365,7 +376,7 @@ __device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi,
         if (a.flux == 1) roe_f32(UL, UR, n, a.gamma, Fh);
         else lax_friedrichs_f32(UL, UR, n, a.gamma, Fh);
         const float jw = sm.sN[fl][3], w = __ldg(a.t.wf32 + g);
-        unsigned short* drow = reinterpret_cast<unsigned short*>(a.dev + (int64_t)f * 5 * KF);
+        unsigned short* drow = reinterpret_cast<unsigned short*>(a.dev + (int64_t)f * FR);
         const int hw = 2 * arow_hi_word<KF>(g) + (g & 1), lw = 2 * arow_lo_word<KF>(g) + (g & 1);
         #pragma unroll
         for (int k = 0; k < 5; ++k) {
@@ -391,10 +402,10 @@ __device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi,
         const float tot = s + __shfl_xor_sync(0xffffffffu, s, 1);
         if (h == 0 && r < 5 * grp.n) {
             const int fl = r / 5, k = r - 5 * fl;
-            const int64_t o = (int64_t)grp.f[fl] * 5 + k;
+            double* fs = face_rec_fs<NQF>(a.dev + (int64_t)grp.f[fl] * FR);
             const double ref = (double)sm.sRef[fl][k];
-            a.Fref[o] = ref;
-            a.S0[o] = ref * a.t.wsum + (double)tot;
+            fs[k] = ref;
+            fs[5 + k] = ref * a.t.wsum + (double)tot;
         }
     }
     __syncwarp();
@@ -463,9 +474,17 @@ __device__ __forceinline__ void dmma884(double d[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
+// The element kernel's B tables (fragment order): volume values, volume integral, the 24 face-integral
+// tables.
+struct ElemBTabs {
+    const uint32_t* tva;
+    const uint32_t* tvp;
+    const uint32_t* tfl;
+};
+
 template <int NB, int NQV, int NQF>
 __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int gi, ElemMixedSmem<NB, NQV, NQF>& sm,
-                                                    const ElemTables<NB>& T, int lane) {
+                                                    const ElemTables<NB>& T, int lane, const ElemBTabs& bt) {
     using S = ElemMixedSmem<NB, NQV, NQF>;
     constexpr int KB = pad8(NB - 1), MV = S::MV, KV = S::KV, MJ = S::MJ, KF = pad8(NQF), NT = MJ / 8, LDR = S::LDR;
     const int gid = lane >> 2, tq = lane & 3;
@@ -477,13 +496,13 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
     // from the group record): the face data, the state rows of the update and the split rows of the
     // volume term arrive while the earlier phases run, instead of one dependent DRAM round trip per
     // phase. Prefetches take no registers; every address lies inside its row.
+    constexpr int FR = face_rec_words(NQF);
     {
-        constexpr int DB = 5 * KF * 4, NL = (DB + 127) / 128, PER = NL + 2;
-        for (int i = lane; i < ne * 4 * PER; i += 32) {
-            const int fq = i / PER, part = i - fq * PER;
+        constexpr int NL = (FR * 4 + 127) / 128;
+        for (int i = lane; i < ne * 4 * NL; i += 32) {
+            const int fq = i / NL, part = i - fq * NL;
             const int64_t f = grp.face[fq >> 2][fq & 3];
-            const char* addr = part < NL ? reinterpret_cast<const char*>(a.dev + f * 5 * KF) + part * 128
-                                         : reinterpret_cast<const char*>((part == NL ? a.Fref : a.S0) + f * 5);
+            const char* addr = reinterpret_cast<const char*>(a.dev + f * FR) + part * 128;
             asm volatile("prefetch.global.L2 [%0];" ::"l"(addr));
         }
     }
@@ -560,7 +579,7 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
             #pragma unroll
             for (int nt = 0; nt < MV / 8; ++nt) {
                 float o[4] = {0.f, 0.f, 0.f, 0.f};
-                mma_bt<KB>(o, A, a.t.tva, nt, lane);
+                mma_bt<KB>(o, A, bt.tva, nt, lane);
                 *reinterpret_cast<float2*>(&sm.sU[r0][nt * 8 + 2 * tq]) = make_float2(o[0] + c00, o[1] + c00);
                 *reinterpret_cast<float2*>(&sm.sU[r1][nt * 8 + 2 * tq]) = make_float2(o[2] + c01, o[3] + c01);
             }
@@ -606,7 +625,7 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
                 split2(y.x, y.y, h[3], l[3]);
             }
             #pragma unroll
-            for (int nt = 0; nt < NT; ++nt) mma3_tile(acc[nt], h, l, a.t.tvp + nt * KTiles<KV>::NT_U32, t, lane);
+            for (int nt = 0; nt < NT; ++nt) mma3_tile(acc[nt], h, l, bt.tvp + nt * KTiles<KV>::NT_U32, t, lane);
         }
         if constexpr (KTiles<KV>::TAIL) {
             const int c = KTiles<KV>::N16 * 16 + 2 * tq;
@@ -620,18 +639,20 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
                 split2(x.x, x.y, h[1], l[1]);
             }
             #pragma unroll
-            for (int nt = 0; nt < NT; ++nt) mma3_tail<KV>(acc[nt], h, l, a.t.tvp + nt * KTiles<KV>::NT_U32, lane);
+            for (int nt = 0; nt < NT; ++nt) mma3_tail<KV>(acc[nt], h, l, bt.tvp + nt * KTiles<KV>::NT_U32, lane);
         }
     }
     // face integrals: the flux deviations arrive split, in fragment order; side 1 negated exactly
+    auto face_rows = [&](AFrag<KF>& A, int q) {
+        const uint32_t flip = (grp.meta[q] >> 8) ? 0x80008000u : 0u;
+        load_afrag<KF, true>(A, v0 ? a.dev + (int64_t)grp.face[r0 / 5][q] * FR + (r0 % 5) * KF : nullptr,
+                             v1 ? a.dev + (int64_t)grp.face[r1 / 5][q] * FR + (r1 % 5) * KF : nullptr, lane, flip);
+    };
     #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const int perm = grp.meta[q] & 0xff;
-        const uint32_t flip = (grp.meta[q] >> 8) ? 0x80008000u : 0u;
         AFrag<KF> A;
-        load_afrag<KF, true>(A, v0 ? a.dev + ((int64_t)grp.face[r0 / 5][q] * 5 + r0 % 5) * KF : nullptr,
-                             v1 ? a.dev + ((int64_t)grp.face[r1 / 5][q] * 5 + r1 % 5) * KF : nullptr, lane, flip);
-        const uint32_t* tb = a.t.tfl + perm * NT * KTiles<KF>::NT_U32;
+        face_rows(A, q);
+        const uint32_t* tb = bt.tfl + (grp.meta[q] & 0xff) * NT * KTiles<KF>::NT_U32;
         #pragma unroll
         for (int nt = 0; nt < NT; ++nt) mma_bt<KF>(acc[nt], A, tb, nt, lane);
     }
@@ -648,12 +669,12 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
         for (int mt = 0; mt < 2; ++mt) {
             const int row = gid + 8 * mt, el = row / 5, k = row - 5 * el;
             const bool ok = row < 5 * ne;
-            am[mt][0] = ok ? __ldcg(a.Fref + (int64_t)grp.face[el][tq] * 5 + k) : 0.0;
+            am[mt][0] = ok ? __ldcg(face_rec_fs<NQF>(a.dev + (int64_t)grp.face[el][tq] * FR) + k) : 0.0;
             am[mt][1] = (ok && a.volume && tq < 3) ? sm.sGb[el][3 * k + tq] : 0.0;
             if (ok && tq == 0) {  // the exact mode-0 face sums, in a fixed order
                 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const double v = __ldcg(a.S0 + (int64_t)grp.face[el][q] * 5 + k);
+                    const double v = __ldcg(face_rec_fs<NQF>(a.dev + (int64_t)grp.face[el][q] * FR) + 5 + k);
                     s0[mt] += (grp.meta[q] >> 8) ? -v : v;
                 }
             }
@@ -677,19 +698,315 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
     __syncwarp();
     // epilogue over the group's DOFs in memory order (coalesced FP64 traffic)
     const double* sR = reinterpret_cast<const double*>(&sm.sG[0][0]);
+    if (a.mode == 0) {
+        for (int i = lane; i < ne * 5 * NB; i += 32) {
+            const int el = i / (5 * NB), r = i - el * (5 * NB);
+            const int4 d = T.dof[r];
+            const int64_t idx = (int64_t)sm.sE[el] * (5 * NB) + r;
+            const double R = sR[(el * 5 + d.y) * LDR + d.x];
+            a.out[idx] = a.Rv ? R - a.Rv[idx] : R;
+        }
+    } else {
+        // RK update. The state rows are read in batches of EB DOFs per lane, every load of a batch
+        // issued before its first use, so a group pays two dependent round trips for them instead
+        // of one per round of 32 DOFs. Stage 1 has a0 = 0: U^n is not read twice. U^n may be the
+        // output buffer (stage 3) and is read through the coherent path.
+        unsigned short* mir16 = reinterpret_cast<unsigned short*>(a.mir_out);
+        constexpr int NPL = (15 * NB + 31) / 32, EB = (NPL + 1) / 2;
+        const int ndof = ne * 5 * NB;
+        const bool u0 = a.a0 != 0.0;
+        #pragma unroll
+        for (int b0 = 0; b0 < NPL; b0 += EB) {
+            double uu[EB], vv[EB];
+            int64_t ix[EB];
+            #pragma unroll
+            for (int j = 0; j < EB; ++j) {
+                const int i = lane + 32 * (b0 + j);
+                const int el = i / (5 * NB), r = i - el * (5 * NB);
+                ix[j] = i < ndof ? (int64_t)sm.sE[el] * (5 * NB) + r : -1;
+                uu[j] = ix[j] >= 0 ? __ldg(a.U + ix[j]) : 0.0;
+                vv[j] = (ix[j] >= 0 && u0) ? a.U0[ix[j]] : 0.0;
+            }
+            #pragma unroll
+            for (int j = 0; j < EB; ++j) {
+                if (ix[j] < 0) continue;
+                const int i = lane + 32 * (b0 + j);
+                const int el = i / (5 * NB), r = i - el * (5 * NB);
+                const int4 d = T.dof[r];  // j, k, hi offset, lo offset
+                const double R = a.Rv ? sR[(el * 5 + d.y) * LDR + d.x] - a.Rv[ix[j]] : sR[(el * 5 + d.y) * LDR + d.x];
+                const double un = (u0 ? a.a0 * vv[j] : 0.0) + a.a1 * (uu[j] - sm.sDT[el] * T.inv_mass[d.x] * R);
+                a.out[ix[j]] = un;
+                if (d.x > 0) {
+                    unsigned short h, l;
+                    split1((float)un, h, l);
+                    unsigned short* mrow = mir16 + (int64_t)sm.sE[el] * (10 * KB);
+                    mrow[d.z] = h;
+                    mrow[d.w] = l;
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// ------------------------------------------------------------------------------------------------
+// Staged element kernel. The plain element kernel issues its global loads phase by phase (the
+// split rows, the face records, the FP64 parts, then ten rounds of state rows in the update), so a
+// group waits for about fifteen dependent L2/DRAM round trips. Here lane 0 of the warp issues TMA
+// bulk copies of every row the group reads (split rows, the four face records of each element,
+// the stage input and U^n rows, the geometry) into the warp's staging area as soon as the group
+// record is known; the warp waits once on its mbarrier and every later phase reads shared memory.
+// State rows must be whole 16-byte units (5 NB doubles: P1..P3).
+// ------------------------------------------------------------------------------------------------
+template <int NB, int NQF>
+struct alignas(16) ElemStage {
+    static constexpr int KB = pad8(NB - 1), FR = face_rec_words(NQF);
+    static constexpr unsigned MIRB = 5 * KB * 4, FRB = FR * 4, UB = 5 * NB * 8, GEOB = 80;
+    uint32_t mir[3][5 * KB];  // split deviation coefficients of the stage input (A rows)
+    uint32_t face[3][4][FR];  // the face records of each element's faces, canonical face order
+    double U[3][5 * NB];      // stage input rows
+    double U0[3][5 * NB];     // U^n rows (stages with a0 != 0)
+    double geo[3][10];        // J^-T row-major, det J
+    uint64_t bar;             // completion of the group's copies (one phase per group)
+};
+
+template <int K>
+__device__ __forceinline__ void load_afrag_smem(AFrag<K>& A, const uint32_t* r0, const uint32_t* r1, int lane,
+                                                uint32_t flip = 0u) {
+    const int tq = lane & 3;
+    #pragma unroll
+    for (int t = 0; t < KTiles<K>::N16; ++t) {
+        uint4 v0 = make_uint4(0u, 0u, 0u, 0u), v1 = v0;
+        if (r0) v0 = *reinterpret_cast<const uint4*>(r0 + t * 16 + tq * 4);
+        if (r1) v1 = *reinterpret_cast<const uint4*>(r1 + t * 16 + tq * 4);
+        A.h[t][0] = v0.x ^ flip; A.h[t][1] = v1.x ^ flip; A.h[t][2] = v0.y ^ flip; A.h[t][3] = v1.y ^ flip;
+        A.l[t][0] = v0.z ^ flip; A.l[t][1] = v1.z ^ flip; A.l[t][2] = v0.w ^ flip; A.l[t][3] = v1.w ^ flip;
+    }
+    if constexpr (KTiles<K>::TAIL) {
+        constexpr int o = KTiles<K>::N16 * 16;
+        uint2 u0 = make_uint2(0u, 0u), u1 = u0;
+        if (r0) u0 = *reinterpret_cast<const uint2*>(r0 + o + tq * 2);
+        if (r1) u1 = *reinterpret_cast<const uint2*>(r1 + o + tq * 2);
+        A.th[0] = u0.x ^ flip; A.th[1] = u1.x ^ flip;
+        A.tl[0] = u0.y ^ flip; A.tl[1] = u1.y ^ flip;
+    }
+}
+
+// One element group from the staging area; returns false when the copies did not land within the
+// poll limit (the status word is set and the warp stops).
+template <int NB, int NQV, int NQF>
+__device__ __forceinline__ bool element_group_staged(const MixedElemArgs& a, int gi, ElemMixedSmem<NB, NQV, NQF>& sm,
+                                                     ElemStage<NB, NQF>& st, const ElemTables<NB>& T, int lane,
+                                                     const ElemBTabs& bt, unsigned parity) {
+    using S = ElemMixedSmem<NB, NQV, NQF>;
+    using G = ElemStage<NB, NQF>;
+    static_assert((5 * NB * 8) % 16 == 0, "state rows must be whole 16-byte units for the bulk copies");
+    constexpr int KB = pad8(NB - 1), MV = S::MV, KV = S::KV, MJ = S::MJ, KF = pad8(NQF), NT = MJ / 8, LDR = S::LDR;
+    const int gid = lane >> 2, tq = lane & 3;
+    const ElemGroup& grp = a.groups[gi];
+    const int ne = grp.n;
+    const int r0 = gid, r1 = gid + 8;
+    const bool v0 = r0 < 5 * ne, v1 = r1 < 5 * ne;
+    const bool need_u0 = a.mode != 0 && a.a0 != 0.0;
+    if (lane == 0) {
+        // the warp's reads of the previous group (generic proxy) are ordered before the copies'
+        // writes (async proxy) by the __syncwarp that ended that group and this fence
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const unsigned per = (a.volume ? G::MIRB : 0u) + 4u * G::FRB + G::UB + (need_u0 ? G::UB : 0u) + G::GEOB;
+        mbar_arrive_expect_tx(&st.bar, per * (unsigned)ne);
+        for (int el = 0; el < ne; ++el) {
+            const int64_t e = grp.e[el];
+            if (a.volume) bulk_copy_g2s(st.mir[el], a.mir + e * 5 * KB, G::MIRB, &st.bar);
+            #pragma unroll
+            for (int q = 0; q < 4; ++q)
+                bulk_copy_g2s(st.face[el][q], a.dev + (int64_t)grp.face[el][q] * G::FR, G::FRB, &st.bar);
+            bulk_copy_g2s(st.U[el], a.U + e * 5 * NB, G::UB, &st.bar);
+            if (need_u0) bulk_copy_g2s(st.U0[el], a.U0 + e * 5 * NB, G::UB, &st.bar);
+            bulk_copy_g2s(st.geo[el], a.geo + e * 10, G::GEOB, &st.bar);
+        }
+    }
+    if (lane < ne) {
+        const int e = grp.e[lane];
+        sm.sE[lane] = e;
+        const double dt = a.dt_inst ? __ldg(a.dt_inst + __ldg(a.elem_inst + e)) : a.dt;
+        sm.sDT[lane] = dt * __ldg(a.inv_detj + e);
+    }
+    if (!mbar_wait_bounded(&st.bar, parity, kBulkSpinLimit)) {
+        if (lane == 0 && a.err) atomicExch(a.err, DG_E_WATCHDOG);
+        mbar_wait_bounded(&st.bar, parity, kBulkSpinLimit);  // copies in flight land before the warp leaves
+        return false;
+    }
+    if (lane < 16) sm.sC0[lane] = lane < 5 * ne ? (float)st.U[lane / 5][lane % 5] : 0.f;
+    if (a.volume && lane < 5 * ne) {  // row k of G(c_0) = detJ F(c_0) J^-T, FP64, one lane per (element, var)
+        const int el = lane / 5, k = lane - 5 * el;
+        const double* geo = st.geo[el];
+        double c[5], J[9];
+        #pragma unroll
+        for (int i = 0; i < 5; ++i) c[i] = st.U[el][i];
+        #pragma unroll
+        for (int i = 0; i < 9; ++i) J[i] = geo[i];
+        const double dj = geo[9];
+        const double rho = c[0] > 1e-16 ? c[0] : 1e-16, ir = 1.0 / rho;
+        const double u[3] = {c[1] * ir, c[2] * ir, c[3] * ir}, en = c[4] * ir;
+        const double p = ((double)a.gamma - 1.0) * (rho * en - 0.5 * rho * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]));
+        double F[3];
+        if (k == 0) {
+            F[0] = rho * u[0]; F[1] = rho * u[1]; F[2] = rho * u[2];
+        } else if (k < 4) {
+            #pragma unroll
+            for (int i = 0; i < 3; ++i) F[i] = rho * u[i] * u[k - 1] + (i == k - 1 ? p : 0.0);
+        } else {
+            #pragma unroll
+            for (int i = 0; i < 3; ++i) F[i] = u[i] * (rho * en + p);
+        }
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double gb = dj * (F[0] * J[d] + F[1] * J[3 + d] + F[2] * J[6 + d]);
+            sm.sGb[el][3 * k + d] = gb;
+            sm.sGbf[el][3 * k + d] = (float)gb;
+        }
+        if (k == 0) {
+            #pragma unroll
+            for (int i = 0; i < 9; ++i) sm.sJ[el][i] = (float)(dj * J[i]);
+        }
+    }
+    __syncwarp();
+    float acc[NT][4];
+    #pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+        #pragma unroll
+        for (int r = 0; r < 4; ++r) acc[nt][r] = 0.f;
+    if (a.volume) {
+        {   // values at the volume points
+            AFrag<KB> A;
+            load_afrag_smem<KB>(A, v0 ? st.mir[r0 / 5] + (r0 % 5) * KB : nullptr,
+                                v1 ? st.mir[r1 / 5] + (r1 % 5) * KB : nullptr, lane);
+            const float c00 = sm.sC0[r0], c01 = sm.sC0[r1];
+            #pragma unroll
+            for (int nt = 0; nt < MV / 8; ++nt) {
+                float o[4] = {0.f, 0.f, 0.f, 0.f};
+                mma_bt<KB>(o, A, bt.tva, nt, lane);
+                *reinterpret_cast<float2*>(&sm.sU[r0][nt * 8 + 2 * tq]) = make_float2(o[0] + c00, o[1] + c00);
+                *reinterpret_cast<float2*>(&sm.sU[r1][nt * 8 + 2 * tq]) = make_float2(o[2] + c01, o[3] + c01);
+            }
+        }
+        if constexpr (KV > 3 * NQV) {
+            constexpr int w = KV - 3 * NQV;
+            for (int i = lane; i < 15 * w; i += 32) sm.sG[i / w][3 * NQV + i % w] = 0.f;
+        }
+        __syncwarp();
+        const float gm1 = a.gamma - 1.f;
+        for (int p = lane; p < ne * NQV; p += 32) {
+            const int el = p / NQV, g = p - el * NQV;
+            float U[5], F[5][3];
+            #pragma unroll
+            for (int k = 0; k < 5; ++k) U[k] = sm.sU[el * 5 + k][g];
+            flux_f32(U, gm1, F);
+            const float* J = sm.sJ[el];
+            #pragma unroll
+            for (int k = 0; k < 5; ++k)
+                #pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    sm.sG[el * 5 + k][3 * g + d] =
+                        fmaf(-F[k][0], J[d], fmaf(-F[k][1], J[3 + d], fmaf(-F[k][2], J[6 + d], sm.sGbf[el][3 * k + d])));
+        }
+        __syncwarp();
+        #pragma unroll
+        for (int t = 0; t < KTiles<KV>::N16; ++t) {
+            const int c = t * 16 + 2 * tq;
+            uint32_t h[4] = {0u, 0u, 0u, 0u}, l[4] = {0u, 0u, 0u, 0u};
+            if (v0) {
+                const float2 x = *reinterpret_cast<const float2*>(&sm.sG[r0][c]);
+                const float2 y = *reinterpret_cast<const float2*>(&sm.sG[r0][c + 8]);
+                split2(x.x, x.y, h[0], l[0]);
+                split2(y.x, y.y, h[2], l[2]);
+            }
+            if (v1) {
+                const float2 x = *reinterpret_cast<const float2*>(&sm.sG[r1][c]);
+                const float2 y = *reinterpret_cast<const float2*>(&sm.sG[r1][c + 8]);
+                split2(x.x, x.y, h[1], l[1]);
+                split2(y.x, y.y, h[3], l[3]);
+            }
+            #pragma unroll
+            for (int nt = 0; nt < NT; ++nt) mma3_tile(acc[nt], h, l, bt.tvp + nt * KTiles<KV>::NT_U32, t, lane);
+        }
+        if constexpr (KTiles<KV>::TAIL) {
+            const int c = KTiles<KV>::N16 * 16 + 2 * tq;
+            uint32_t h[2] = {0u, 0u}, l[2] = {0u, 0u};
+            if (v0) {
+                const float2 x = *reinterpret_cast<const float2*>(&sm.sG[r0][c]);
+                split2(x.x, x.y, h[0], l[0]);
+            }
+            if (v1) {
+                const float2 x = *reinterpret_cast<const float2*>(&sm.sG[r1][c]);
+                split2(x.x, x.y, h[1], l[1]);
+            }
+            #pragma unroll
+            for (int nt = 0; nt < NT; ++nt) mma3_tail<KV>(acc[nt], h, l, bt.tvp + nt * KTiles<KV>::NT_U32, lane);
+        }
+    }
+    // face integrals from the staged face records; side 1 negated exactly
+    #pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int perm = grp.meta[q] & 0xff;
+        const uint32_t flip = (grp.meta[q] >> 8) ? 0x80008000u : 0u;
+        AFrag<KF> A;
+        load_afrag_smem<KF>(A, v0 ? st.face[r0 / 5][q] + (r0 % 5) * KF : nullptr,
+                            v1 ? st.face[r1 / 5][q] + (r1 % 5) * KF : nullptr, lane, flip);
+        const uint32_t* tb = bt.tfl + perm * NT * KTiles<KF>::NT_U32;
+        #pragma unroll
+        for (int nt = 0; nt < NT; ++nt) mma_bt<KF>(acc[nt], A, tb, nt, lane);
+    }
+    __syncwarp();  // sG is free
+    {
+        double* sR = reinterpret_cast<double*>(&sm.sG[0][0]);
+        const int mq = grp.meta[tq];
+        const double sq = (mq >> 8) ? -1.0 : 1.0;
+        double am[2][2], s0[2] = {0.0, 0.0};
+        #pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            const int row = gid + 8 * mt, el = row / 5, k = row - 5 * el;
+            const bool ok = row < 5 * ne;
+            am[mt][0] = ok ? face_rec_fs<NQF>(st.face[el][tq])[k] : 0.0;
+            am[mt][1] = (ok && a.volume && tq < 3) ? sm.sGb[el][3 * k + tq] : 0.0;
+            if (ok && tq == 0) {
+                #pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const double v = face_rec_fs<NQF>(st.face[el][q])[5 + k];
+                    s0[mt] += (grp.meta[q] >> 8) ? -v : v;
+                }
+            }
+        }
+        #pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+            const int jb = nt * 8 + gid;
+            const double b0 = jb < NB ? sq * __ldg(a.t.mf + (mq & 0xff) * NB + jb) : 0.0;
+            const double b1 = (jb < NB && tq < 3) ? -__ldg(a.t.mv + 3 * jb + tq) : 0.0;
+            #pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                double d[2] = {(double)acc[nt][2 * mt], (double)acc[nt][2 * mt + 1]};
+                dmma884(d, am[mt][0], b0);
+                dmma884(d, am[mt][1], b1);
+                const int row = gid + 8 * mt;
+                if (nt == 0 && tq == 0) d[0] = s0[mt];
+                *reinterpret_cast<double2*>(sR + row * LDR + nt * 8 + 2 * tq) = make_double2(d[0], d[1]);
+            }
+        }
+    }
+    __syncwarp();
+    const double* sR = reinterpret_cast<const double*>(&sm.sG[0][0]);
     unsigned short* mir16 = reinterpret_cast<unsigned short*>(a.mir_out);
     for (int i = lane; i < ne * 5 * NB; i += 32) {
         const int el = i / (5 * NB), r = i - el * (5 * NB);
-        const int4 d = T.dof[r];  // j, k, hi offset, lo offset
+        const int4 d = T.dof[r];
         const int64_t e = sm.sE[el];
         const int64_t idx = e * (5 * NB) + r;
         const double R = a.Rv ? sR[(el * 5 + d.y) * LDR + d.x] - a.Rv[idx] : sR[(el * 5 + d.y) * LDR + d.x];
         if (a.mode == 0) {
             a.out[idx] = R;
         } else {
-            // stage 1 has a0 = 0: U^n is not read twice
-            const double u0 = a.a0 != 0.0 ? a.a0 * a.U0[idx] : 0.0;
-            const double un = u0 + a.a1 * (__ldg(a.U + idx) - sm.sDT[el] * T.inv_mass[d.x] * R);
+            const double u0 = need_u0 ? a.a0 * st.U0[el][r] : 0.0;
+            const double un = u0 + a.a1 * (st.U[el][r] - sm.sDT[el] * T.inv_mass[d.x] * R);
             a.out[idx] = un;
             if (d.x > 0) {
                 unsigned short h, l;
@@ -701,6 +1018,40 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
         }
     }
     __syncwarp();
+    return true;
+}
+
+template <int NB, int NQV, int NQF, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) element_mixed_staged(MixedElemArgs a) {
+    using S = ElemMixedSmem<NB, NQV, NQF>;
+    using G = ElemStage<NB, NQF>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ ElemTables<NB> tabs;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    S& sm = reinterpret_cast<S*>(smem_raw)[warp];
+    G& st = reinterpret_cast<G*>(smem_raw + sizeof(S) * WARPS)[warp];
+    if (lane == 0) mbar_init(&st.bar, 1);
+    element_tables_init(tabs, a.t.inv_mass);  // ends in __syncthreads: the barriers are initialised
+    const ElemBTabs bt{a.t.tva, a.t.tvp, a.t.tfl};
+    unsigned parity = 0;
+    for (int gi = blockIdx.x * WARPS + warp; gi < a.ngroups; gi += gridDim.x * WARPS) {
+        if (!element_group_staged<NB, NQV, NQF>(a, gi, sm, st, tabs, lane, bt, parity)) break;
+        parity ^= 1u;
+    }
+}
+
+template <int NB, int NQV, int NQF>
+__host__ __device__ constexpr size_t elem_staged_warp_smem() {
+    return sizeof(ElemMixedSmem<NB, NQV, NQF>) + sizeof(ElemStage<NB, NQF>);
+}
+// Warps per CTA of the staged kernel with `ctas` resident CTAs per SM: what fits in the SM's 228 KB
+// (1 KB reserved per CTA, 3 KB for the static tables), at most 11 (one CTA) or 5 (two CTAs).
+template <int NB, int NQV, int NQF>
+__host__ __device__ constexpr int elem_staged_warps(int ctas) {
+    const long long per_cta = 233472ll / ctas - 1024 - 3072;
+    const long long w = per_cta / (long long)elem_staged_warp_smem<NB, NQV, NQF>();
+    const int cap = ctas == 1 ? 11 : 5;
+    return w > cap ? cap : (w < 1 ? 1 : (int)w);
 }
 
 // 8 warps: four CTAs per SM (64 registers a thread); 4 warps (P4): six, at most 85 registers
@@ -712,8 +1063,9 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 8 ? 4 : 6) element_mixed(
     element_tables_init(tabs, a.t.inv_mass);
     S& sm = reinterpret_cast<S*>(smem_raw)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
+    const ElemBTabs bt{a.t.tva, a.t.tvp, a.t.tfl};
     for (int gi = blockIdx.x * WARPS + (threadIdx.x >> 5); gi < a.ngroups; gi += gridDim.x * WARPS)
-        element_group_mixed<NB, NQV, NQF>(a, gi, sm, tabs, lane);
+        element_group_mixed<NB, NQV, NQF>(a, gi, sm, tabs, lane, bt);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -736,12 +1088,15 @@ struct MixedData {
     const double* geo = nullptr;
     const double* inv_detj = nullptr;
     const double* UD = nullptr;
-    uint32_t* dev = nullptr;
-    double* Fref = nullptr;
-    double* S0 = nullptr;
+    uint32_t* dev = nullptr;          // face records [nface][face_rec_words(nqf)]
     const double* dt_inst = nullptr;  // ensembles: per-instance dt (device), else null
     const int* elem_inst = nullptr;
     const double* Rv = nullptr;       // Navier-Stokes stepping: the stage input's viscous residual
+    int* err = nullptr;               // device status word of the mixed kernels (bounded waits)
+    // element kernel: 0 = loads phase by phase (8-warp CTAs, four per SM), 2 = each group's rows
+    // staged by TMA bulk copies (P1..P3, 16-byte aligned state buffers); chosen by dg_autotune
+    int elem_kernel = 0;
+    int elem_ctas = 1;                // resident CTAs per SM of the staged kernel: 1 or 2
     // A rows of the deviation coefficients of the states Un, Ua, Ub and of a residual input
     uint32_t* mir[4] = {nullptr, nullptr, nullptr, nullptr};
     // host copies the tile schedule of the persistent form is built from
@@ -941,11 +1296,10 @@ inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>
         m.hface_cells[2 * f + 1] = hfi[f].c1;
     }
     // padding columns of the A rows stay zero: allocation clears them and no kernel writes them
-    if ((rc = mixed_alloc(m, &m.dev, (size_t)nface * 5 * KF)) || (rc = mixed_alloc(m, &m.Fref, (size_t)nface * 5)) ||
-        (rc = mixed_alloc(m, &m.S0, (size_t)nface * 5)))
-        return rc;
+    if ((rc = mixed_alloc(m, &m.dev, (size_t)nface * face_rec_words(NQF)))) return rc;
     for (int i = 0; i < 4; ++i)
         if ((rc = mixed_alloc(m, &m.mir[i], (size_t)ncell * 5 * KB))) return rc;
+    if ((rc = mixed_alloc(m, &m.err, 1))) return rc;
     m.fi = d_fi; m.geo = d_geo;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -966,7 +1320,7 @@ inline MixedFaceArgs face_args(const MixedData& m, const double* U, int mir_in, 
                                int g1 = -1) {
     MixedFaceArgs fa;
     fa.U = U; fa.mir = m.mir[mir_in]; fa.fi = m.fi; fa.groups = m.fgroups; fa.UD = m.UD; fa.dev = m.dev;
-    fa.Fref = m.Fref; fa.S0 = m.S0; fa.t = m.t; fa.ngroups = m.nfgroups; fa.gamma = m.gamma; fa.flux = m.flux;
+    fa.t = m.t; fa.ngroups = m.nfgroups; fa.gamma = m.gamma; fa.flux = m.flux;
     if (g1 >= 0) {  // face groups [g0, g1) only
         fa.groups = m.fgroups + g0;
         fa.ngroups = g1 - g0;
@@ -979,11 +1333,12 @@ inline MixedElemArgs elem_args(const MixedData& m, const double* U, const double
                                double dt, double a0, double a1, int with_volume, int mir_in, int mir_out) {
     MixedElemArgs ea;
     ea.U = U; ea.U0 = U0; ea.out = out; ea.mir = m.mir[mir_in]; ea.mir_out = mir_out >= 0 ? m.mir[mir_out] : nullptr;
-    ea.dev = m.dev; ea.Fref = m.Fref; ea.S0 = m.S0; ea.geo = m.geo; ea.inv_detj = m.inv_detj; ea.groups = m.egroups;
+    ea.dev = m.dev; ea.geo = m.geo; ea.inv_detj = m.inv_detj; ea.groups = m.egroups;
     ea.t = m.t; ea.ngroups = m.negroups; ea.gamma = m.gamma; ea.volume = with_volume;
     ea.dt = dt; ea.a0 = a0; ea.a1 = a1; ea.mode = mode;
     ea.dt_inst = mode == 1 ? m.dt_inst : nullptr; ea.elem_inst = m.elem_inst;
     ea.Rv = mode == 1 ? m.Rv : nullptr;
+    ea.err = m.err;
     return ea;
 }
 
@@ -1013,6 +1368,28 @@ inline int mixed_launch(MixedData& m, int which, const double* U, const double* 
         const int n = g1 < 0 ? m.nfgroups : g1 - g0;
         const int g = (int)std::min<int64_t>((n + W - 1) / W, (int64_t)m.sms * 64);
         face_flux_mixed<NB, NQF, W><<<g, W * 32, 0, s>>>(face_args(m, U, mir_in, face_mask, g0, g1));
+    } else if (m.elem_kernel == 2 && (5 * NB * 8) % 16 == 0 && ((uintptr_t)U & 15) == 0 &&
+               ((uintptr_t)U0 & 15) == 0) {
+        if constexpr ((5 * NB * 8) % 16 == 0) {
+            const auto ea = elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out);
+            if (m.elem_ctas == 2) {
+                constexpr int W = elem_staged_warps<NB, NQV, NQF>(2);
+                constexpr size_t smem = elem_staged_warp_smem<NB, NQV, NQF>() * W;
+                static unsigned long long done = 0;
+                int rc = ensure_smem(element_mixed_staged<NB, NQV, NQF, W, 2>, smem, done);
+                if (rc) return rc;
+                const int g = (int)std::min<int64_t>((m.negroups + W - 1) / W, (int64_t)m.sms * 2);
+                element_mixed_staged<NB, NQV, NQF, W, 2><<<g, W * 32, smem, s>>>(ea);
+            } else {
+                constexpr int W = elem_staged_warps<NB, NQV, NQF>(1);
+                constexpr size_t smem = elem_staged_warp_smem<NB, NQV, NQF>() * W;
+                static unsigned long long done = 0;
+                int rc = ensure_smem(element_mixed_staged<NB, NQV, NQF, W, 1>, smem, done);
+                if (rc) return rc;
+                const int g = (int)std::min<int64_t>((m.negroups + W - 1) / W, (int64_t)m.sms);
+                element_mixed_staged<NB, NQV, NQF, W, 1><<<g, W * 32, smem, s>>>(ea);
+            }
+        }
     } else {
         constexpr size_t smem = sizeof(ElemMixedSmem<NB, NQV, NQF>) * WE;
         static unsigned long long done = 0;
@@ -1023,6 +1400,28 @@ inline int mixed_launch(MixedData& m, int which, const double* U, const double* 
             elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out));
     }
     return cuda_status(cudaGetLastError());
+}
+
+// Element-kernel shapes of the two-launch schedule that dg_autotune times: the kernel (0: loads
+// phase by phase, 2: rows staged by bulk copies), warps per CTA (three elements each) and resident
+// CTAs per SM. Returns how many apply to this order and rule pair.
+struct ElemShape {
+    int kernel, warps, ctas;
+};
+inline int mixed_elem_shapes(const MixedData& m, ElemShape out[3]) {
+#define X(P, QV, QF, NB, NQV, NQF, W)                                                 \
+    if (m.order == P && m.qv == QV && m.qf == QF) {                                   \
+        int n = 0;                                                                    \
+        out[n++] = ElemShape{0, W, W == 8 ? 4 : 6};                                   \
+        if ((5 * NB * 8) % 16 == 0) {                                                 \
+            out[n++] = ElemShape{2, elem_staged_warps<NB, NQV, NQF>(1), 1};           \
+            out[n++] = ElemShape{2, elem_staged_warps<NB, NQV, NQF>(2), 2};           \
+        }                                                                             \
+        return n;                                                                     \
+    }
+    FVEDG_MIXED_COMBOS(X)
+#undef X
+    return 0;
 }
 
 // mir_in: mirror of U (0..3); mir_out: mirror the update writes (RK mode), or -1.

@@ -108,7 +108,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 8 ? FVEDG_PERSIST_MINB8 :
             if (threadIdx.x == 0) atomicAdd(&q->done[tl.w], (unsigned int)(tl.z - tl.y));
         } else {
             auto& esm = *reinterpret_cast<ElemMixedSmem<NB, NQV, NQF>*>(wsm);
-            for (int gi = tl.y + warp; gi < tl.z; gi += WARPS) element_group_mixed<NB, NQV, NQF>(ea, gi, esm, tabs, lane);
+            const ElemBTabs bt{ea.t.tva, ea.t.tvp, ea.t.tfl};
+            for (int gi = tl.y + warp; gi < tl.z; gi += WARPS) element_group_mixed<NB, NQV, NQF>(ea, gi, esm, tabs, lane, bt);
             __syncthreads();
         }
     }

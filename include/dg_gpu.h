@@ -182,10 +182,18 @@ int dg_ensemble_offsets(const dg_ctx* ctx, int64_t* elem_offsets);
  * graph per step (the dt values are read from device memory, so one graph serves any dt). */
 int dg_ssprk3_ensemble(dg_ctx* ctx, const double* dt, int nsteps, int use_graph);
 
-/* Autotuner of the persistent schedule: times each candidate (face and element groups per tile,
- * CTAs per SM, mesh regions, lag) on the current state (restored afterwards), keeps the fastest and
- * writes a JSON record of every candidate and the choice into report[len]. */
+/* Autotuner of the mixed-precision form: times each candidate on the current state (restored
+ * afterwards), keeps the fastest and writes a JSON record of every candidate and the choice into
+ * report[len]. Persistent schedule: face and element groups per tile, CTAs per SM, mesh regions,
+ * lag. Two-launch schedule: the element kernel's shape (elements per CTA and CTAs per SM, with its
+ * loads issued phase by phase or each group's rows staged in shared memory by TMA bulk copies). */
 int dg_autotune(dg_ctx* ctx, double dt, char* report, size_t len);
+/* Pins the element-kernel shape of the two-launch mixed schedule (what dg_autotune chooses; this
+ * replays a recorded choice without timing): staged = 0 issues the group's loads phase by phase,
+ * staged = 1 stages each group's rows in shared memory by TMA bulk copies (orders 1..3) with
+ * ctas_per_sm = 1 or 2 resident CTAs. Both shapes give bit-identical results. DG_E_ARG for other
+ * values, an FP64 context or a staged shape at order 4. New: no reference counterpart. */
+int dg_set_element_shape(dg_ctx* ctx, int staged, int ctas_per_sm);
 
 /* Self-test of the failure detection of the batched persistent form (mixed precision, schedule 1):
  * runs stage 0 of one SSP-RK3 step with the completion count that face region 0 must reach raised

@@ -68,3 +68,43 @@ def test_mixed_graph_matches_stream():
     mix.set_state(U0)
     mix.ssprk3(1e-3, 3, graph=True)
     assert np.array_equal(a, mix.get_state())
+
+
+@pytest.mark.parametrize("P,qv,qf", [(1, 0, 1), (2, 1, 2), (3, 3, 3)])
+def test_staged_element_kernel_is_bit_identical(P, qv, qf):
+    """The element kernel whose group rows arrive by TMA bulk copies (one or two CTAs per SM) does the
+    same arithmetic in the same order as the one that loads them phase by phase."""
+    m = box_mesh(4, jitter=0.1, seed=7)
+    U0 = problems.project(m, P, problems.density_wave())
+    U0 += 1e-3 * np.random.default_rng(P).standard_normal(U0.shape)
+    got = []
+    for shape in ((0, 1), (1, 1), (1, 2)):
+        c = ExplicitConvection(m, order=P, flux="Roe", quad_vol=qv, quad_face=qf, precision="mixed")
+        c.set_element_shape(*shape)
+        R = c.eval(U0)
+        c.set_state(U0)
+        c.ssprk3(1e-3, 2)
+        c.ssprk3(1e-3, 2, graph=True)
+        got.append((R, c.get_state()))
+        c.close()
+    for R, S in got[1:]:
+        assert np.array_equal(R, got[0][0])
+        assert np.array_equal(S, got[0][1])
+
+
+def test_two_launch_autotune_records_element_shapes():
+    m = box_mesh(6, hi=(2 * np.pi,) * 3)
+    U = problems.project(m, 3, problems.taylor_green())
+    c = ExplicitConvection(m, order=3, flux="Roe", quad_vol=3, quad_face=3, precision="mixed")
+    c.set_state(U)
+    rep = c.autotune(1e-3)
+    assert np.array_equal(c.get_state(), U)
+    assert rep["schedule"] == "two-launch" and len(rep["candidates"]) == 3
+    assert rep["chosen"]["ms_per_step"] == min(x["ms_per_step"] for x in rep["candidates"])
+    c.ssprk3(1e-3, 2)
+    assert c.check_state() == 0
+    c.close()
+    p4 = ExplicitConvection(box_mesh(2), order=4, quad_vol=5, quad_face=3, precision="mixed")
+    with pytest.raises(RuntimeError):
+        p4.set_element_shape(1, 1)  # P4 state rows are not whole 16-byte units
+    p4.close()
