@@ -492,10 +492,10 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
     const int ne = grp.n;
     const int r0 = gid, r1 = gid + 8;
     const bool v0 = r0 < 5 * ne, v1 = r1 < 5 * ne;
-    // Pull everything this group reads from global memory into L2 first (the addresses are known
-    // from the group record): the face data, the state rows of the update and the split rows of the
-    // volume term arrive while the earlier phases run, instead of one dependent DRAM round trip per
-    // phase. Prefetches take no registers; every address lies inside its row.
+    // Pull the group's face records and split rows into L2 first (the addresses are known from the
+    // group record): they arrive while the earlier phases run, instead of one dependent DRAM round
+    // trip per phase. (The state rows of the update are read in batches there; prefetching them
+    // too measured no gain.) Prefetches take no registers; every address lies inside its row.
     constexpr int FR = face_rec_words(NQF);
     {
         constexpr int NL = (FR * 4 + 127) / 128;
@@ -504,15 +504,6 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
             const int64_t f = grp.face[fq >> 2][fq & 3];
             const char* addr = reinterpret_cast<const char*>(a.dev + f * FR) + part * 128;
             asm volatile("prefetch.global.L2 [%0];" ::"l"(addr));
-        }
-    }
-    if (a.mode != 0) {
-        constexpr int SB = 5 * NB * 8, SL = (SB + 127) / 128;
-        const int n2 = a.a0 != 0.0 ? 2 : 1;
-        for (int i = lane; i < ne * n2 * SL; i += 32) {
-            const int el = i / (n2 * SL), r = i - el * (n2 * SL), w = r / SL, part = r - w * SL;
-            const double* base = (w ? a.U0 : a.U) + (int64_t)grp.e[el] * 5 * NB;
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char*>(base) + part * 128));
         }
     }
     if (a.volume) {

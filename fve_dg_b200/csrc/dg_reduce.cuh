@@ -1,7 +1,8 @@
 // Deterministic reductions over the device state: conservation sums, the largest wave speed (for a
 // CFL time step, cf. examples/TaylerGreenVortex/TGBatch.cpp:358-383) and the non-physical point
-// count. Each is a fixed grid of per-block partials followed by one block that sums them in a
-// fixed order, so results do not depend on scheduling.
+// count. Each is a fixed grid of per-block partials (a fixed assignment of elements to warps and of
+// volume points to lanes) followed by one block that sums them in a fixed order, so results do not
+// depend on scheduling.
 #pragma once
 #include <atomic>
 #include <cstdint>
@@ -25,12 +26,15 @@ __global__ void __launch_bounds__(kRedThreads) state_reduce_kernel(const double*
         int ncell, int nb, int nqv, double gamma, int kind, double* __restrict__ partial) {
     __shared__ double sh[kRedThreads][6];
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ncell; e += gridDim.x * blockDim.x) {
+    // one warp per element, its lanes over the volume points: the element's row is read by
+    // broadcast loads (one transaction per warp and value) instead of one row per thread
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int e = blockIdx.x * wpb + (threadIdx.x >> 5); e < ncell; e += gridDim.x * wpb) {
         const double* c = U + (int64_t)e * 5 * nb;
         const double dj = geo ? geo[(int64_t)e * 10 + 9] : 0.0;
-        if (kind == RED_CONSERVATION)
+        if (kind == RED_CONSERVATION && lane == 0)
             for (int k = 0; k < 5; ++k) acc[k] += c[k] * dj / 6.0;
-        for (int g = 0; g < nqv; ++g) {
+        for (int g = lane; g < nqv; g += 32) {
             double Ug[5] = {0, 0, 0, 0, 0};
             for (int b = 0; b < nb; ++b) {
                 const double p = phi_v[g * nb + b];
