@@ -1045,9 +1045,11 @@ __host__ __device__ constexpr int elem_staged_warps(int ctas) {
     return w > cap ? cap : (w < 1 ? 1 : (int)w);
 }
 
-// 8 warps: four CTAs per SM (64 registers a thread); 4 warps (P4): six, at most 85 registers
+// 8 warps: three CTAs per SM, at most 85 registers a thread (80 without spills; four CTAs at 64
+// registers spill 20 bytes and measured 3 % slower with the batched update loads); 4 warps (P4):
+// six CTAs, at most 85 registers
 template <int NB, int NQV, int NQF, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 8 ? 4 : 6) element_mixed(MixedElemArgs a) {
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 8 ? 3 : 6) element_mixed(MixedElemArgs a) {
     using S = ElemMixedSmem<NB, NQV, NQF>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ ElemTables<NB> tabs;
@@ -1403,7 +1405,7 @@ inline int mixed_elem_shapes(const MixedData& m, ElemShape out[3]) {
 #define X(P, QV, QF, NB, NQV, NQF, W)                                                 \
     if (m.order == P && m.qv == QV && m.qf == QF) {                                   \
         int n = 0;                                                                    \
-        out[n++] = ElemShape{0, W, W == 8 ? 4 : 6};                                   \
+        out[n++] = ElemShape{0, W, W == 8 ? 3 : 6};                                   \
         if ((5 * NB * 8) % 16 == 0) {                                                 \
             out[n++] = ElemShape{2, elem_staged_warps<NB, NQV, NQF>(1), 1};           \
             out[n++] = ElemShape{2, elem_staged_warps<NB, NQV, NQF>(2), 2};           \
