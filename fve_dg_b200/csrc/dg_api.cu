@@ -190,10 +190,12 @@ int dispatch_face(int order, int qv, int qf, const FaceArgs& a, cudaStream_t s) 
     FVEDG_FIXED_COMBOS(X)
 #undef X
     switch (order) {
+        case 0: return launch_face<1>(a, s);
         case 1: return launch_face<4>(a, s);
         case 2: return launch_face<10>(a, s);
         case 3: return launch_face<20>(a, s);
         case 4: return launch_face<35>(a, s);
+        case 5: return launch_face<56>(a, s);
     }
     return DG_E_ARG;
 }
@@ -203,10 +205,12 @@ int dispatch_element(int order, int qv, int qf, const StageArgs& a, cudaStream_t
     FVEDG_FIXED_COMBOS(X)
 #undef X
     switch (order) {
+        case 0: return launch_element<1, 32>(a, s);
         case 1: return launch_element<4, 32>(a, s);
         case 2: return launch_element<10, 16>(a, s);
         case 3: return launch_element<20, 8>(a, s);
         case 4: return launch_element<35, 4>(a, s);
+        case 5: return launch_element<56, 4>(a, s);
     }
     return DG_E_ARG;
 }
@@ -576,7 +580,7 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
         return nullptr;
     };
     if (!mesh || !cfg) return fail(nullptr, DG_E_ARG);
-    if (cfg->order < 1 || cfg->order > kMaxOrder || !(cfg->gamma > 1.0)) return fail(nullptr, DG_E_ARG);
+    if (cfg->order < 0 || cfg->order > kMaxOrder || !(cfg->gamma > 1.0)) return fail(nullptr, DG_E_ARG);
     if (cfg->flux != DG_FLUX_LF && cfg->flux != DG_FLUX_ROE) return fail(nullptr, DG_E_ARG);
     if (cfg->precision != DG_PREC_FP64 && cfg->precision != DG_PREC_MIXED) return fail(nullptr, DG_E_ARG);
     if (cfg->schedule != 0 && !(cfg->schedule == 1 && cfg->precision == DG_PREC_MIXED)) return fail(nullptr, DG_E_ARG);
@@ -586,6 +590,7 @@ dg_ctx* create_impl(const dg_mesh_desc* mesh, const dg_config* cfg, int* err, co
     if (cfg->limiter < 0 || cfg->limiter > 2 || (cfg->limiter && !limiter_supported(cfg->order, qv)))
         return fail(nullptr, DG_E_ARG);
     if (!(cfg->mu >= 0.0) || (cfg->mu > 0.0 && !(cfg->prandtl > 0.0))) return fail(nullptr, DG_E_ARG);
+    if (cfg->mu > 0.0 && (cfg->order < 1 || cfg->order > 4)) return fail(nullptr, DG_E_ARG);  // viscous kernels: P1..P4
     if (mesh->ncell <= 0 || mesh->ncell > (int64_t)1 << 30 || mesh->nface <= 0 || mesh->nface > (int64_t)1 << 30)
         return fail(nullptr, DG_E_ARG);
     Geometry geo;

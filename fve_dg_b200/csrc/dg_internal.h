@@ -7,7 +7,7 @@
 
 namespace fvedg {
 
-constexpr int kMaxOrder = 4;
+constexpr int kMaxOrder = 5;
 constexpr int kNumPerms = 24;
 
 inline int num_basis(int order) { return (order + 1) * (order + 2) * (order + 3) / 6; }

@@ -9,11 +9,12 @@ float, so the committed file carries the exact bits. Provenance of each rule:
   scripts/codegen/QuadTet.py from data/QuadData/NME_6313_cubature_tetra_p*_n*.dat, weights / 6;
   Degree5Points15 from include/GaussQuadrature/QuadTetLowerOrder.h:1):
     0 Degree2Points4   1 Degree4Points11  2 Degree5Points15  3 Degree6Points23
-    4 Degree7Points31  5 Degree8Points44  6 Degree9Points57
+    4 Degree7Points31  5 Degree8Points44  6 Degree9Points57  7 Degree11Points94 (the P5 Auto rule)
   tri (include/GaussQuadrature/QuadTriLowerOrder.h:1-69 and QuadTriHighOrder.h:1-24, the latter
   from data/QuadData/rotationalsymmetry.txt, weights / 2):
     0 Degree3Points4   1 Degree3Points6   2 Degree4Points7 (exact to degree 5)
     3 Degree10Points24 (rotationally symmetric only; exact to about 1e-10)
+    4 Degree13Points36 (QuadTriHighOrder.h, the P5 Auto rule)
 
 Run from the repository root after building the reference library:
     python fve_dg_b200/csrc/gen_quad_tables.py
@@ -25,10 +26,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 TET = ["Degree2Points4", "Degree4Points11", "Degree5Points15", "Degree6Points23",
-       "Degree7Points31", "Degree8Points44", "Degree9Points57"]
-TRI = ["Degree3Points4", "Degree3Points6", "Degree4Points7", "Degree10Points24"]
-TET_DEG = [2, 4, 5, 6, 7, 8, 9]
-TRI_DEG = [3, 3, 5, 10]
+       "Degree7Points31", "Degree8Points44", "Degree9Points57", "Degree11Points94"]
+TRI = ["Degree3Points4", "Degree3Points6", "Degree4Points7", "Degree10Points24", "Degree13Points36"]
+TET_DEG = [2, 4, 5, 6, 7, 8, 9, 11]
+TRI_DEG = [3, 3, 5, 10, 13]
 
 
 def main():

@@ -6,18 +6,20 @@
 
 namespace fvedg {
 
-int auto_tet_rule(int order) {  // AutoQuadSelectorTet.h:2-25
+int auto_tet_rule(int order) {  // AutoQuadSelectorTet.h:2-30
     switch (order) {
         case 0: case 1: case 2: return DG_TET_D5P15;
         case 3: return DG_TET_D7P31;
         case 4: return DG_TET_D9P57;
+        case 5: return DG_TET_D11P94;
     }
     return -1;
 }
-int auto_tri_rule(int order) {  // AutoQuadSelectorTri.h:1-21
+int auto_tri_rule(int order) {  // AutoQuadSelectorTri.h:1-27
     switch (order) {
         case 0: case 1: return DG_TRI_D4P7;
         case 2: case 3: case 4: return DG_TRI_D10P24;
+        case 5: return DG_TRI_D13P36;
     }
     return -1;
 }

@@ -33,10 +33,12 @@ template <> struct rule_id<GaussLegendreTet::Degree6Points23> { static constexpr
 template <> struct rule_id<GaussLegendreTet::Degree7Points31> { static constexpr int value = DG_TET_D7P31; };
 template <> struct rule_id<GaussLegendreTet::Degree8Points44> { static constexpr int value = DG_TET_D8P44; };
 template <> struct rule_id<GaussLegendreTet::Degree9Points57> { static constexpr int value = DG_TET_D9P57; };
+template <> struct rule_id<GaussLegendreTet::Degree11Points94> { static constexpr int value = DG_TET_D11P94; };
 template <> struct rule_id<GaussLegendreTri::Degree3Points4> { static constexpr int value = DG_TRI_D3P4; };
 template <> struct rule_id<GaussLegendreTri::Degree3Points6> { static constexpr int value = DG_TRI_D3P6; };
 template <> struct rule_id<GaussLegendreTri::Degree4Points7> { static constexpr int value = DG_TRI_D4P7; };
 template <> struct rule_id<GaussLegendreTri::Degree10Points24> { static constexpr int value = DG_TRI_D10P24; };
+template <> struct rule_id<GaussLegendreTri::Degree13Points36> { static constexpr int value = DG_TRI_D13P36; };
 
 inline void check(int rc, const char* what) {
     if (rc == DG_E_CUDA)
@@ -56,7 +58,7 @@ class ExplicitConvectionGPU {
     static constexpr int kVol = fvedg_adaptor::rule_id<GaussQuadCell>::value;
     static constexpr int kFace = fvedg_adaptor::rule_id<GaussQuadFace>::value;
     static_assert(kVol != -2 && kFace != -2, "quadrature rule not supported by the B200 operator");
-    static_assert(Order >= 1 && Order <= 4, "the B200 operator covers P1..P4");
+    static_assert(Order <= 5, "the B200 operator covers P0..P5 (the orders ExplicitConvection.cpp:5-16 instantiates)");
 
 public:
     static constexpr uInt N = Basis::NumBasis;

@@ -1,5 +1,5 @@
 /* dg_gpu.h — C ABI of the B200 explicit DG operator for the 3D compressible Euler equations on
- * affine tetrahedra (modal basis P1..P4, Lax-Friedrichs or Roe flux, SSP-RK3).
+ * affine tetrahedra (modal basis P0..P5, Lax-Friedrichs or Roe flux, SSP-RK3).
  *
  * It replaces the reference's explicit convection path:
  *   ExplicitConvection<Order, Flux, QuadC, QuadF>::eval(mesh, U, t)
@@ -58,9 +58,9 @@ enum dg_boundary {
  * (include/GaussQuadrature/AutoQuadSelectorTet.h:2-50, AutoQuadSelectorTri.h:1-45). */
 enum dg_tet_rule {
     DG_TET_D2P4 = 0, DG_TET_D4P11 = 1, DG_TET_D5P15 = 2, DG_TET_D6P23 = 3,
-    DG_TET_D7P31 = 4, DG_TET_D8P44 = 5, DG_TET_D9P57 = 6
+    DG_TET_D7P31 = 4, DG_TET_D8P44 = 5, DG_TET_D9P57 = 6, DG_TET_D11P94 = 7
 };
-enum dg_tri_rule { DG_TRI_D3P4 = 0, DG_TRI_D3P6 = 1, DG_TRI_D4P7 = 2, DG_TRI_D10P24 = 3 };
+enum dg_tri_rule { DG_TRI_D3P4 = 0, DG_TRI_D3P6 = 1, DG_TRI_D4P7 = 2, DG_TRI_D10P24 = 3, DG_TRI_D13P36 = 4 };
 
 /* Flattened mesh. Topology follows DGMesh (include/Mesh/MeshGenerator.h:46-57) and
  * ComputingMesh(const DGMesh&) (src/Mesh/ComputingMesh.cpp:268-298); geometry follows
@@ -106,7 +106,7 @@ typedef struct dg_mesh_desc {
 } dg_mesh_desc;
 
 typedef struct dg_config {
-    int order;       /* 1..4 */
+    int order;       /* 0..5 (FP64 tensor-core kernels and the mixed-precision form: 1..4) */
     int flux;        /* dg_flux_kind */
     int quad_vol;    /* dg_tet_rule or -1 */
     int quad_face;   /* dg_tri_rule or -1 */

@@ -187,6 +187,8 @@ int main() {
         bad += check<3, T::Degree6Points23, F::Degree10Points24>(*m, name);
         bad += check<4, T::Degree8Points44, F::Degree10Points24>(*m, name);
         bad += check<3, GaussLegendreTet::Auto, GaussLegendreTri::Auto>(*m, name);
+        bad += check<0, GaussLegendreTet::Auto, GaussLegendreTri::Auto>(*m, name);
+        bad += check<5, GaussLegendreTet::Auto, GaussLegendreTri::Auto>(*m, name);
         bad += check_diffusion<1, T::Degree2Points4, F::Degree3Points6>(*m, name);
         bad += check_diffusion<2, T::Degree4Points11, F::Degree4Points7>(*m, name);
         bad += check_diffusion<3, T::Degree6Points23, F::Degree10Points24>(*m, name);

@@ -550,6 +550,7 @@ int run_project(const ComputingMesh& m, int id, const double* prm, double* U) {
 
 // (order, tet rule, tri rule) combinations instantiated here. X(P, qv, qf, QC, QF)
 #define FVEREF_COMBOS(X)                                   \
+    X(0, 2, 2, T::Degree5Points15, F::Degree4Points7)      \
     X(1, 0, 1, T::Degree2Points4, F::Degree3Points6)       \
     X(1, 0, 0, T::Degree2Points4, F::Degree3Points4)       \
     X(1, 0, 2, T::Degree2Points4, F::Degree4Points7)       \
@@ -560,7 +561,8 @@ int run_project(const ComputingMesh& m, int id, const double* prm, double* U) {
     X(3, 3, 3, T::Degree6Points23, F::Degree10Points24)    \
     X(3, 4, 3, T::Degree7Points31, F::Degree10Points24)    \
     X(4, 5, 3, T::Degree8Points44, F::Degree10Points24)    \
-    X(4, 6, 3, T::Degree9Points57, F::Degree10Points24)
+    X(4, 6, 3, T::Degree9Points57, F::Degree10Points24)    \
+    X(5, 7, 4, T::Degree11Points94, F::Degree13Points36)
 
 extern "C" {
 
@@ -573,6 +575,7 @@ int fveref_quad_tet(int id, double* pts, double* w) {
         case 4: return copy_rule3<T::Degree7Points31>(pts, w);
         case 5: return copy_rule3<T::Degree8Points44>(pts, w);
         case 6: return copy_rule3<T::Degree9Points57>(pts, w);
+        case 7: return copy_rule3<T::Degree11Points94>(pts, w);
     }
     return -1;
 }
@@ -583,6 +586,7 @@ int fveref_quad_tri(int id, double* pts, double* w) {
         case 1: return copy_rule2<F::Degree3Points6>(pts, w);
         case 2: return copy_rule2<F::Degree4Points7>(pts, w);
         case 3: return copy_rule2<F::Degree10Points24>(pts, w);
+        case 4: return copy_rule2<F::Degree13Points36>(pts, w);
     }
     return -1;
 }
@@ -602,10 +606,12 @@ int fveref_basis(int order, int npts, const double* xyz, double* phi, double* gr
 // Bytes of one element block of LongVector<5*Nb>, i.e. the reference's padded element stride.
 size_t fveref_block_bytes(int order) {
     switch (order) {
+        case 0: return sizeof(DenseMatrix<5 * DGBasisEvaluator<0>::NumBasis, 1>);
         case 1: return sizeof(DenseMatrix<5 * DGBasisEvaluator<1>::NumBasis, 1>);
         case 2: return sizeof(DenseMatrix<5 * DGBasisEvaluator<2>::NumBasis, 1>);
         case 3: return sizeof(DenseMatrix<5 * DGBasisEvaluator<3>::NumBasis, 1>);
         case 4: return sizeof(DenseMatrix<5 * DGBasisEvaluator<4>::NumBasis, 1>);
+        case 5: return sizeof(DenseMatrix<5 * DGBasisEvaluator<5>::NumBasis, 1>);
     }
     return 0;
 }
@@ -710,6 +716,7 @@ int fveref_limit(void* p, int order, int qv, double* Ucur, const double* Uprev, 
 int fveref_mass(void* p, int order, int qv, double* mass) {
     const ComputingMesh& m = *static_cast<RefMesh*>(p)->cm;
     switch (order * 16 + qv) {
+        case 0 * 16 + 2: return run_mass<0, T::Degree5Points15>(m, mass);
         case 1 * 16 + 0: return run_mass<1, T::Degree2Points4>(m, mass);
         case 1 * 16 + 2: return run_mass<1, T::Degree5Points15>(m, mass);
         case 2 * 16 + 1: return run_mass<2, T::Degree4Points11>(m, mass);
@@ -718,6 +725,7 @@ int fveref_mass(void* p, int order, int qv, double* mass) {
         case 3 * 16 + 4: return run_mass<3, T::Degree7Points31>(m, mass);
         case 4 * 16 + 5: return run_mass<4, T::Degree8Points44>(m, mass);
         case 4 * 16 + 6: return run_mass<4, T::Degree9Points57>(m, mass);
+        case 5 * 16 + 7: return run_mass<5, T::Degree11Points94>(m, mass);
     }
     return -1;
 }
@@ -763,10 +771,12 @@ int fveref_project(void* p, int order, int id, const double* params, double* U) 
     const ComputingMesh& m = *static_cast<RefMesh*>(p)->cm;
     if (id < 0 || id > 2) return -2;
     switch (order) {
+        case 0: return run_project<0>(m, id, params, U);
         case 1: return run_project<1>(m, id, params, U);
         case 2: return run_project<2>(m, id, params, U);
         case 3: return run_project<3>(m, id, params, U);
         case 4: return run_project<4>(m, id, params, U);
+        case 5: return run_project<5>(m, id, params, U);
     }
     return -1;
 }

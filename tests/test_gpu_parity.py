@@ -176,3 +176,29 @@ def test_errors_are_reported():
     bad[1, :] = np.nan
     conv.set_state(bad)
     assert conv.check_state() > 0
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("P", [0, 5])
+def test_orders_0_and_5_match_reference(mesh3, P):
+    """P0 (finite volume) and P5, the other orders the reference instantiates
+    (ExplicitConvection.cpp:5-16), with its Auto rules: residual and its parts against the
+    reference's eval, Roe against the oracle, SSP-RK3 steps against the reference's LongVector loop.
+    They run the runtime-size FP64 kernels; the mixed form is not built for them."""
+    qv, qf = problems.auto_rules(P)
+    U = noisy_state(mesh3, P, 40 + P)
+    ref = RefLib()
+    rm = RefMesh.from_mesh(ref, mesh3)
+    conv = ExplicitConvection(mesh3, order=P, quad_vol=qv, quad_face=qf)
+    assert rel_l2(conv.eval(U), rm.eval(U, P, qv, qf)) < TOL
+    assert rel_l2(conv.eval_cells(U), rm.eval(U, P, qv, qf, part=1)) < TOL
+    assert rel_l2(conv.eval_internals(U), rm.eval(U, P, qv, qf, part=2)) < TOL
+    roe = ExplicitConvection(mesh3, order=P, flux="Roe", quad_vol=qv, quad_face=qf)
+    assert rel_l2(roe.eval(U), Oracle.from_mesh(mesh3).residual(U, P, qv, qf, flux="Roe")) < TOL
+    U0 = problems.project(mesh3, P, problems.density_wave())
+    conv.set_state(U0)
+    conv.ssprk3(1e-3, 3)
+    Ur = rm.ssprk3(U0, rm.mass(P, qv), P, qv, qf, 1e-3, 3)
+    assert rel_l2(conv.get_state(), Ur) < TOL
+    with pytest.raises(RuntimeError):
+        ExplicitConvection(mesh3, order=P, quad_vol=qv, quad_face=qf, precision="mixed")

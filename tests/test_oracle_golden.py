@@ -132,3 +132,42 @@ def test_reference_padded_block_size():
     """LongVector pads each block to 32 bytes (DenseMatrix alignas(32)): P1..P4 strides."""
     ref = RefLib()
     assert [ref.block_bytes(P) for P in (1, 2, 3, 4)] == [160, 416, 800, 1408]
+    assert [ref.block_bytes(P) for P in (0, 5)] == [64, 2240]
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference library not built")
+def test_quadrature_tables_are_the_references_bit_for_bit():
+    """Every rule of quad_tables.inc, the P5 Auto rules (Degree11Points94, Degree13Points36)
+    included, equals the reference's own points and weights exactly."""
+    ref = RefLib()
+    for kind, nrules in ((0, 8), (1, 5)):
+        for rid in range(nrules):
+            p_ref, w_ref = ref.quad(kind, rid)
+            p, w = problems.quad_rule(kind, rid)
+            assert np.array_equal(p, p_ref) and np.array_equal(w, w_ref), (kind, rid)
+    assert problems.auto_rules(0) == (2, 2) and problems.auto_rules(5) == (7, 4)
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("P", [0, 5])
+def test_orders_0_and_5_match_reference_live(P):
+    """P0 (finite volume) and P5, the other orders ExplicitConvection.cpp:5-16 instantiates, with
+    the reference's Auto rules: basis values and gradients, and the oracle's residual against the
+    reference's eval."""
+    qv, qf = problems.auto_rules(P)
+    m = box_mesh(3, jitter=0.1, seed=200 + P)
+    ref = RefLib()
+    pts, _ = problems.quad_rule(0, qv)
+    phi_r, grad_r = ref.basis(P, pts)
+    phi, grad = problems.basis(P, pts)
+    assert np.abs(phi - phi_r).max() <= 1e-13 * np.abs(phi_r).max()
+    assert np.abs(grad - grad_r).max() <= 1e-13 * max(np.abs(grad_r).max(), 1.0)
+    U = problems.project(m, P, problems.taylor_green())
+    U = U + 1e-2 * np.random.default_rng(P).standard_normal(U.shape)
+    rm = RefMesh.from_mesh(ref, m)
+    o = Oracle.from_mesh(m)
+    assert rel_l2(o.residual(U, P, qv, qf), rm.eval(U, P, qv, qf)) < 1e-12
+    b = rm.mass(P, qv)
+    assert rel_l2(o.mass(P, qv), b) < 1e-14
+    U0 = problems.project(m, P, problems.density_wave())
+    assert rel_l2(o.ssprk3(U0, P, qv, qf, 1e-3, 2), rm.ssprk3(U0, b, P, qv, qf, 1e-3, 2)) < 1e-13

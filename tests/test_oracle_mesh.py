@@ -48,7 +48,7 @@ PROBLEMS = {
 
 
 @pytest.mark.parametrize("name", sorted(PROBLEMS))
-@pytest.mark.parametrize("P", [1, 2, 3, 4])
+@pytest.mark.parametrize("P", [0, 1, 2, 3, 4, 5])
 def test_projection_matches_reference_func2coef(name, P):
     func, prm, L, jit = PROBLEMS[name]
     ref = RefLib()
