@@ -92,6 +92,16 @@ def lib():
         "dg_ssprk3_ensemble": (ctypes.c_int, [vp, c_double_p, ctypes.c_int, ctypes.c_int]),
         "dg_autotune": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_char_p, ctypes.c_size_t]),
         "dg_set_element_shape": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+        "dg_partition_create": (vp, [ctypes.POINTER(MeshDesc), ctypes.POINTER(ctypes.c_int32), ctypes.c_int, c_int_p]),
+        "dg_partition_destroy": (None, [vp]),
+        "dg_partition_local_mesh": (ctypes.c_int, [vp, ctypes.POINTER(MeshDesc)]),
+        "dg_partition_counts": (ctypes.c_int, [vp, c_int64_p, c_int64_p, c_int_p, c_int_p]),
+        "dg_partition_l2g": (c_int64_p, [vp]),
+        "dg_partition_global_faces": (c_int64_p, [vp]),
+        "dg_partition_send": (ctypes.c_int, [vp, ctypes.c_int, c_int_p, c_int64_p, ctypes.POINTER(c_int64_p)]),
+        "dg_partition_recv": (ctypes.c_int, [vp, ctypes.c_int, c_int_p, c_int64_p, ctypes.POINTER(c_int64_p)]),
+        "dg_halo_pack": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int64, vp, vp]),
+        "dg_halo_unpack": (ctypes.c_int, [vp, ctypes.c_int, vp, ctypes.c_int64, vp, vp]),
         "dg_set_dirichlet": (ctypes.c_int, [vp, c_double_p]),
         "dg_conservation": (ctypes.c_int, [vp, c_double_p]),
         "dg_max_wave_speed": (ctypes.c_int, [vp, c_double_p]),
@@ -125,7 +135,9 @@ def exported_symbols():
             "dg_static_scratch_capacity", "dg_set_state", "dg_get_state",
             "dg_ssprk3", "dg_ssprk3_graph", "dg_ssprk3_timed", "dg_stream", "dg_state_device",
             "dg_refresh_split", "dg_ssprk3_stage", "dg_ssprk3_stage_phase", "dg_create_ensemble",
-            "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_set_element_shape", "dg_watchdog_selftest", "dg_mass", "dg_limit", "dg_limit_device", "dg_viscous_residual", "dg_viscous_residual_device",
+            "dg_ensemble_offsets", "dg_ssprk3_ensemble", "dg_autotune", "dg_set_element_shape", "dg_partition_create", "dg_partition_destroy",
+            "dg_partition_local_mesh", "dg_partition_counts", "dg_partition_l2g", "dg_partition_global_faces",
+            "dg_partition_send", "dg_partition_recv", "dg_halo_pack", "dg_halo_unpack", "dg_watchdog_selftest", "dg_mass", "dg_limit", "dg_limit_device", "dg_viscous_residual", "dg_viscous_residual_device",
             "dg_save_checkpoint", "dg_load_checkpoint",
             "dg_set_dirichlet", "dg_conservation",
             "dg_max_wave_speed", "dg_check_state", "dg_info", "dg_mesh_geometry", "dg_face_perms", "dg_basis",

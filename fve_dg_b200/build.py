@@ -16,7 +16,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libfvedg_b200.so")
 OBJ = os.path.join(PKG, "_build")
-HOST_SRCS = ["host_mesh.cpp", "host_tables.cpp"]
+HOST_SRCS = ["host_mesh.cpp", "host_tables.cpp", "host_partition.cpp"]
 CUDA_SRCS = ["dg_api.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"

@@ -1104,6 +1104,48 @@ double* dg_state_device(dg_ctx* c, int which) {
     return which == 0 ? c->d_Un : which == 1 ? c->d_Ua : c->d_Ub;
 }
 
+}  // extern "C"
+
+namespace {
+// Whole element rows (5 Nb doubles) between a state buffer and a packed exchange buffer: pack
+// copies rows[i] of the state to slot i of buf, unpack copies slot i into rows[i]. Rows outside
+// [0, ncell) are skipped. One thread per double, consecutive threads along a row.
+__global__ void halo_rows(double* __restrict__ state, double* __restrict__ buf, const int64_t* __restrict__ rows,
+                          int64_t n, int row_len, int64_t ncell, int unpack) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * row_len) return;
+    const int64_t slot = i / row_len;
+    const int j = (int)(i - slot * row_len);
+    const int64_t r = rows[slot];
+    if (r < 0 || r >= ncell) return;
+    if (unpack) state[r * row_len + j] = buf[i];
+    else buf[i] = state[r * row_len + j];
+}
+
+int halo_copy(dg_ctx* c, int which, const int64_t* rows, int64_t n, double* buf, void* stream, int unpack) {
+    if (!c || which < 0 || which > 2 || n < 0 || (n > 0 && (!rows || !buf))) return DG_E_ARG;
+    if (n == 0) return DG_OK;
+    DG_CUDA(cudaSetDevice(c->cfg.device));
+    const cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    const int row_len = 5 * c->tab.nb;
+    const int64_t total = n * row_len;
+    halo_rows<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(dg_state_device(c, which), buf, rows, n, row_len,
+                                                             c->ncell, unpack);
+    ++g_launches;
+    return cuda_ok(cudaGetLastError());
+}
+}  // namespace
+
+extern "C" {
+
+int dg_halo_pack(dg_ctx* c, int which, const int64_t* rows_dev, int64_t n, double* buf_dev, void* stream) {
+    return halo_copy(c, which, rows_dev, n, buf_dev, stream, 0);
+}
+
+int dg_halo_unpack(dg_ctx* c, int which, const int64_t* rows_dev, int64_t n, const double* buf_dev, void* stream) {
+    return halo_copy(c, which, rows_dev, n, const_cast<double*>(buf_dev), stream, 1);
+}
+
 int dg_refresh_split(dg_ctx* c, int which, const int64_t* elems, int64_t n, void* stream) {
     if (!c || which < 0 || which > 2 || n < 0 || (n > 0 && !elems)) return DG_E_ARG;
     if (c->cfg.precision != DG_PREC_MIXED || n == 0) return DG_OK;

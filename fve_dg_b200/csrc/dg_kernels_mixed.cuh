@@ -1016,7 +1016,7 @@ template <int NB, int NQV, int NQF, int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) element_mixed_staged(MixedElemArgs a) {
     using S = ElemMixedSmem<NB, NQV, NQF>;
     using G = ElemStage<NB, NQF>;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ ElemTables<NB> tabs;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     S& sm = reinterpret_cast<S*>(smem_raw)[warp];

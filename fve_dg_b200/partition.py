@@ -12,8 +12,10 @@ reduction for them), and its state is overwritten by its owner's before every st
 Before each RK stage the stage input's ghost entries are refreshed: every rank sends, to each
 neighbouring rank, the coefficient blocks of its owned elements that are ghosts there, and
 unpacks what it receives into its ghost slots (one send and one receive per neighbour,
-`torch.distributed.batch_isend_irecv`, NCCL between GPUs). Owned results then equal the
-whole-mesh results: the same faces, in the same order, see the same inputs.
+`torch.distributed.batch_isend_irecv`, NCCL between GPUs; on CUDA the gathers and scatters are the
+library's own kernels, dg_halo_pack and dg_halo_unpack). Owned results then equal the whole-mesh
+results: the same faces, in the same order, see the same inputs. The library builds the same plan
+natively (dg_partition_create, NativePlan) for drivers in C or C++.
 """
 import ctypes
 
@@ -171,6 +173,51 @@ class PartitionedConvection:
         L.check(L.lib().dg_refresh_split(self.conv._ctx, int(which), ctypes.c_void_p(self._ghost_dev.data_ptr()),
                                          int(self._ghost_dev.numel()), None), "dg_refresh_split")
 
+    def rows_dev(self, kind, q):
+        """Device copy of the local rows this part sends to ("send") or receives from ("recv") q."""
+        import torch
+        cache = self.__dict__.setdefault("_rows_cache", {})
+        if (kind, q) not in cache:
+            rows = (self.lm.send if kind == "send" else self.lm.recv)[q]
+            cache[kind, q] = torch.as_tensor(np.ascontiguousarray(rows, dtype=np.int64),
+                                             device=torch.device("cuda", self.device))
+        return cache[kind, q]
+
+    def pack(self, which, q, buf, stream):
+        """Rows of state buffer `which` that peer q needs, into buf, by the library's gather kernel
+        (dg_halo_pack) on `stream`."""
+        idx = self.rows_dev("send", q)
+        L.check(L.lib().dg_halo_pack(self.conv._ctx, int(which), ctypes.c_void_p(idx.data_ptr()), int(idx.numel()),
+                                     ctypes.c_void_p(buf.data_ptr()), ctypes.c_void_p(stream)), "dg_halo_pack")
+
+    def unpack(self, which, q, buf, stream):
+        """buf (peer q's rows) into this part's ghost rows of state buffer `which` (dg_halo_unpack)."""
+        idx = self.rows_dev("recv", q)
+        L.check(L.lib().dg_halo_unpack(self.conv._ctx, int(which), ctypes.c_void_p(idx.data_ptr()), int(idx.numel()),
+                                       ctypes.c_void_p(buf.data_ptr()), ctypes.c_void_p(stream)), "dg_halo_unpack")
+
+    def _halo(self, which):
+        """The NCCL halo exchange of state buffer `which` on the current torch stream: the library's
+        gather kernel per peer, one send and one receive per neighbouring rank, its scatter kernel."""
+        import torch
+        stream = torch.cuda.current_stream().cuda_stream
+        dev = torch.device("cuda", self.device)
+        row = 5 * self.conv.num_basis
+        ops, recvs = [], []
+        for q in sorted(self.lm.send):
+            buf = torch.empty((len(self.lm.send[q]), row), dtype=torch.float64, device=dev)
+            self.pack(which, q, buf, stream)
+            ops.append(self.dist.P2POp(self.dist.isend, buf, q))
+        for q in sorted(self.lm.recv):
+            buf = torch.empty((len(self.lm.recv[q]), row), dtype=torch.float64, device=dev)
+            recvs.append((q, buf))
+            ops.append(self.dist.P2POp(self.dist.irecv, buf, q))
+        if ops:
+            for r in self.dist.batch_isend_irecv(ops):
+                r.wait()
+        for q, buf in recvs:
+            self.unpack(which, q, buf, stream)
+
     def exchange(self, which):
         """Fill the ghost rows of state buffer `which` from their owners (stream-ordered)."""
         import torch
@@ -178,7 +225,7 @@ class PartitionedConvection:
             if self._exchange is not None:
                 self._exchange(which)
             else:
-                halo_exchange(self.state_view(which), self.lm, self.dist)
+                self._halo(which)
         self._refresh(which)
 
     def stage(self, dt, st):
@@ -205,7 +252,7 @@ class PartitionedConvection:
             if self._exchange is not None:
                 self._exchange(st)
             else:
-                halo_exchange(self.state_view(st), self.lm, self.dist)
+                self._halo(st)
         done = torch.cuda.Event()
         done.record(self._comm)
         main.wait_event(done)
@@ -229,21 +276,23 @@ class PartitionedConvection:
 
 
 def emulated_ranks(mesh, nparts, **kw):
-    """nparts PartitionedConvection objects in one process on one GPU, exchanging ghost rows by
-    device copies; step them together with `step_emulated` (the decomposition on one GPU)."""
+    """nparts PartitionedConvection objects in one process on one GPU, exchanging ghost rows through
+    the library's gather and scatter kernels (the owner's dg_halo_pack, then dg_halo_unpack); step
+    them together with `step_emulated` (the decomposition on one GPU)."""
     import torch
     part = partition_elements(mesh, nparts)
     ranks = []
 
     def make_exchange(r):
-        def ex(which):
+        def ex(which):  # the owner's gather kernel into a buffer, then this part's scatter kernel
             dst = ranks[r]
-            view = dst.state_view(which)
-            for q, idx in sorted(dst.lm.recv.items()):
+            stream = torch.cuda.current_stream().cuda_stream
+            for q in sorted(dst.lm.recv):
                 src = ranks[q]
-                sidx = np.searchsorted(src.lm.owned, dst.lm.l2g[idx])
-                view.index_copy_(0, torch.as_tensor(idx, device=view.device),
-                                 src.state_view(which).index_select(0, torch.as_tensor(sidx, device=view.device)))
+                buf = torch.empty((len(dst.lm.recv[q]), 5 * dst.conv.num_basis), dtype=torch.float64,
+                                  device=torch.device("cuda", dst.device))
+                src.pack(which, r, buf, stream)
+                dst.unpack(which, q, buf, stream)
         return ex
 
     for r in range(nparts):
@@ -271,3 +320,51 @@ def step_emulated(ranks, dt, nsteps=1, phased=False):
                     r.stage(dt, st)
     for r in ranks:
         r.wait()
+
+
+class NativePlan:
+    """The same part and exchange plan built by the library (dg_partition_create), for drivers in
+    C or C++; read back into numpy arrays named as in LocalMesh."""
+
+    def __init__(self, mesh, part, rank):
+        lib = L.lib()
+        owner = np.ascontiguousarray(part, dtype=np.int32)
+        d = mesh.desc()
+        err = ctypes.c_int(0)
+        h = lib.dg_partition_create(ctypes.byref(d), owner.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), int(rank),
+                                    ctypes.byref(err))
+        if not h:
+            raise L.DGError(err.value, "dg_partition_create")
+        try:
+            no, ng = ctypes.c_int64(), ctypes.c_int64()
+            ns, nr = ctypes.c_int(), ctypes.c_int()
+            L.check(lib.dg_partition_counts(h, ctypes.byref(no), ctypes.byref(ng), ctypes.byref(ns), ctypes.byref(nr)),
+                    "dg_partition_counts")
+            self.n_owned, self.n_ghost = no.value, ng.value
+            nloc = no.value + ng.value
+            self.l2g = np.ctypeslib.as_array(lib.dg_partition_l2g(h), shape=(nloc,)).copy()
+            ld = L.MeshDesc()
+            L.check(lib.dg_partition_local_mesh(h, ctypes.byref(ld)), "dg_partition_local_mesh")
+            nf = ld.nface
+
+            def arr(p, n_):
+                return np.ctypeslib.as_array(p, shape=(n_,)).copy() if p else None
+
+            self.global_face = np.ctypeslib.as_array(lib.dg_partition_global_faces(h), shape=(nf,)).copy()
+            self.face_cells = arr(ld.face_cells, 2 * nf).reshape(nf, 2)
+            self.cells = arr(ld.cell_nodes, 4 * nloc).reshape(nloc, 4)
+            self.faces = arr(ld.face_nodes, 3 * nf).reshape(nf, 3)
+            fn1 = arr(ld.face_nodes1, 3 * nf)
+            self.face_nodes1 = fn1.reshape(nf, 3) if fn1 is not None else None
+            self.periodic = arr(ld.face_periodic, nf)
+            self.bc = arr(ld.face_bc, nf)
+            self.nghost = ld.nghost
+            self.send, self.recv = {}, {}
+            for count, fn, out in ((ns.value, lib.dg_partition_send, self.send), (nr.value, lib.dg_partition_recv, self.recv)):
+                for i in range(count):
+                    peer, n = ctypes.c_int(), ctypes.c_int64()
+                    rows = L.c_int64_p()
+                    L.check(fn(h, i, ctypes.byref(peer), ctypes.byref(n), ctypes.byref(rows)), "dg_partition_send/recv")
+                    out[peer.value] = np.ctypeslib.as_array(rows, shape=(n.value,)).copy()
+        finally:
+            lib.dg_partition_destroy(h)

@@ -234,6 +234,37 @@ int dg_ssprk3_stage(dg_ctx* ctx, double dt, int stage);
  * call dg_refresh_split); phases 0 then 1 launch exactly what dg_ssprk3_stage launches. */
 int dg_ssprk3_stage_phase(dg_ctx* ctx, double dt, int stage, int phase);
 
+/* One mesh split across processes, for drivers that exchange halos with MPI or NCCL themselves
+ * (fve_dg_b200/partition.py is the Python form of the same plan). New: the reference runs one
+ * mesh per process.
+ * dg_partition_create: rank `rank`'s part under owner[ncell] (values 0..nparts-1) of a raw-topology
+ * mesh (form (b), nghost = 0). Its local mesh holds the owned elements (ascending global id), then
+ * the ghosts: face neighbours of owned elements that other ranks own (ascending). Its faces are the
+ * global faces that touch an owned element, in global order and orientation, so an owned element's
+ * residual equals its whole-mesh residual once the ghost rows hold their owners' values. The plan
+ * sends to each peer q the rows of owned elements that are ghosts of q and receives from q the
+ * ghosts q owns, both in ascending global order, so the lists of the two sides match. */
+typedef struct dg_partition dg_partition;
+dg_partition* dg_partition_create(const dg_mesh_desc* mesh, const int32_t* owner, int rank, int* err);
+void dg_partition_destroy(dg_partition* part);
+/* The local mesh as a descriptor for dg_create (nghost set; pointers into the plan, the points
+ * shared with the global mesh's array), valid until dg_partition_destroy. */
+int dg_partition_local_mesh(const dg_partition* part, dg_mesh_desc* local);
+int dg_partition_counts(const dg_partition* part, int64_t* n_owned, int64_t* n_ghost, int* n_send_peers,
+                        int* n_recv_peers);
+/* Global element id of every local element [n_owned + n_ghost]; global face id of every local face. */
+const int64_t* dg_partition_l2g(const dg_partition* part);
+const int64_t* dg_partition_global_faces(const dg_partition* part);
+/* Peer i (ascending rank) to send to / receive from: its rank, the row count and the local rows. */
+int dg_partition_send(const dg_partition* part, int i, int* peer, int64_t* n, const int64_t** rows);
+int dg_partition_recv(const dg_partition* part, int i, int* peer, int64_t* n, const int64_t** rows);
+/* Device gather / scatter of whole element rows (5 Nb doubles) of state buffer `which` (as
+ * dg_state_device) for the exchange, on `stream` (0 = the context's stream): pack copies row
+ * rows_dev[i] to slot i of buf_dev, unpack copies slot i into row rows_dev[i]. Rows outside the
+ * context's cells are skipped. After an unpack the mixed form needs dg_refresh_split of those rows. */
+int dg_halo_pack(dg_ctx* ctx, int which, const int64_t* rows_dev, int64_t n, double* buf_dev, void* stream);
+int dg_halo_unpack(dg_ctx* ctx, int which, const int64_t* rows_dev, int64_t n, const double* buf_dev, void* stream);
+
 /* Explicit viscous operator, replaces ExplicitDiffusion<Order, QuadC, QuadF>::eval(mesh, U, t)
  * (include/DG/DG_Schemes/ExplicitDiffusion.h:133-626) with the context's order and rules: the
  * interior-penalty Navier-Stokes viscous residual R of U, same sign and scaling as the reference

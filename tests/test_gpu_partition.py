@@ -1,6 +1,7 @@
 """GPU: one mesh split into parts with ghost elements (fve_dg_b200/partition.py), each part its own
 context, stepped one SSP-RK3 stage at a time (dg_ssprk3_stage) with the ghost rows of every stage
-input filled from their owners by device copies in between. The owned states must equal the
+input filled from their owners by the library's gather and scatter kernels (dg_halo_pack,
+dg_halo_unpack) in between. The owned states must equal the
 whole-mesh context's. (Parts run as separate contexts on one GPU, one after another; the NCCL
 exchange between processes is the same plan, checked on CPU over gloo.)"""
 import ctypes

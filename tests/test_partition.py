@@ -152,3 +152,30 @@ def test_two_rank_ssprk3_over_gloo_equals_whole_mesh(mi):
     for _, owned, Uo in res:
         got[owned] = Uo
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("nparts,kw", [(2, dict(n=3)), (3, dict(n=4, jitter=0.1, seed=3)),
+                                       (4, dict(n=3, periodic=(1, 1, 0), bc="Pseudo3DZ"))])
+def test_native_plan_is_the_python_plan(nparts, kw):
+    """dg_partition_create (native, for C/C++ drivers) builds exactly LocalMesh's part: the same
+    local elements, faces (nodes, cells, orientation data) and exchange lists, for every rank."""
+    from fve_dg_b200.partition import LocalMesh, NativePlan, partition_elements
+    m = box_mesh(**kw)
+    part = partition_elements(m, nparts)
+    for r in range(nparts):
+        lm, nat = LocalMesh(m, part, r), NativePlan(m, part, r)
+        assert nat.n_owned == lm.n_owned and nat.n_ghost == len(lm.ghosts) == nat.nghost
+        assert np.array_equal(nat.l2g, lm.l2g)
+        assert np.array_equal(nat.global_face, lm.global_face)
+        lmm = lm.mesh
+        assert np.array_equal(nat.face_cells, lmm.face_cells.reshape(-1, 2))
+        assert np.array_equal(nat.cells, lmm.cells.reshape(-1, 4))
+        assert np.array_equal(nat.faces, lmm.faces.reshape(-1, 3))
+        assert np.array_equal(nat.face_nodes1, lmm.face_nodes1.reshape(-1, 3))
+        assert np.array_equal(nat.periodic, lmm.periodic.reshape(-1))
+        assert np.array_equal(nat.bc, lmm.bc.reshape(-1))
+        assert sorted(nat.send) == sorted(lm.send) and sorted(nat.recv) == sorted(lm.recv)
+        for q in lm.send:
+            assert np.array_equal(nat.send[q], lm.send[q])
+        for q in lm.recv:
+            assert np.array_equal(nat.recv[q], lm.recv[q])
