@@ -310,6 +310,13 @@ static void num_flux(int kind, const double* UL, const double* UR, const double*
     else flux_lf(UL, UR, n, gam, Fh);
 }
 
+int orc_numerical_flux(int kind, const double* UL, const double* UR, const double* n, double gamma,
+                       double* Fh) {
+    if (!UL || !UR || !n || !Fh || (kind != ORC_FLUX_LF && kind != ORC_FLUX_ROE)) return -1;
+    num_flux(kind, UL, UR, n, gamma, Fh);
+    return 0;
+}
+
 /* ------------------------------------------------------------------------------------------ */
 /* Residual R = R_cells + R_internal + R_boundary, ExplicitConvection.cpp:136-272               */
 /* ------------------------------------------------------------------------------------------ */

@@ -49,6 +49,8 @@ int orc_ssprk3(const orc_mesh* m, int order, double gamma, int flux, int qv, int
                const double* mass, double dt, int nsteps, double t0, const double* dirichlet10);
 int orc_conservation(const orc_mesh* m, int order, int qv, double gamma, const double* U,
                      double out6[6]);
+/* The numerical flux 2A-free F^(UL, UR, n) of one face point (ORC_FLUX_LF or ORC_FLUX_ROE). */
+int orc_numerical_flux(int kind, const double* UL, const double* UR, const double* n, double gamma, double* Fh);
 
 #ifdef __cplusplus
 }
