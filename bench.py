@@ -150,18 +150,14 @@ def kernel_bytes(name, P, ncell, nface, nqf):
     if name == "viscous":                # state read by both launches, residual written, face blocks
         return 3 * state + 3 * nface * 8 * (5 * nqf + nb) + ncell * (80 + 8 + 32) + nface * 96
     kf = (nqf + 7) // 8 * 8
-    kb = (nb - 1 + 7) // 8 * 8
-    fj = nface * (5 * kf * 4 + 2 * 5 * 8)  # split flux deviations (A rows) + FP64 reference and mode-0 sums
+    fj = nface * (5 * kf * 4 + 2 * 5 * 8)  # face records: split flux deviations (A rows), FP64 reference, mode-0 sums
     grp = ncell * 96 // 3                  # element-group records
-    mir = ncell * 5 * kb * 4               # split deviation coefficients of the stage input (A rows)
-    mir_w = ncell * 5 * (nb - 1) * 4       # the A-row columns the update writes
-    c0 = ncell * 5 * 8                     # FP64 element means
-    if name == "face_flux_mixed":          # A rows + means read once, face records, face data written
-        return mir + c0 + nface * face_rec + fj
-    if name == "element_mixed":            # A rows, geometry, face data, stage state + U^n read; new stage written
-        return mir + ncell * 88 + grp + fj + 3 * state + mir_w
-    if name == "stage_persistent_mixed":   # both phases, the face data written and read once
-        return 2 * mir + c0 + nface * face_rec + ncell * 88 + grp + 2 * fj + 3 * state + mir_w
+    if name == "face_flux_mixed":          # stage input rows (split in registers), face infos, face records written
+        return state + nface * face_rec + fj
+    if name == "element_mixed":            # geometry, face records, stage input + U^n read; new stage written
+        return ncell * 88 + grp + fj + 3 * state
+    if name == "stage_persistent_mixed":   # both phases, the face records written and read once
+        return nface * face_rec + ncell * 88 + grp + 2 * fj + 3 * state
     raise ValueError(name)
 
 

@@ -381,17 +381,16 @@ int viscous_stage(dg_ctx* c, const double* in, cudaStream_t s) {
 }
 
 // Limiter after stage st (dg_config.limiter): bounds from the stage input's statistics, the output
-// limited in place and its statistics written for the next stage; mir = the output's split rows in
-// the mixed form (refreshed where the limiter acted). The input's statistics come from the previous
-// stage's launch, except after the state was set from outside (computed here at stage 0) and for
-// ghost cells (computed here every stage: a halo exchange rewrote their rows).
-int limit_stage(dg_ctx* c, int st, const double* in, double* out, uint32_t* mir, cudaStream_t s) {
+// limited in place and its statistics written for the next stage. The input's statistics come from
+// the previous stage's launch, except after the state was set from outside (computed here at stage
+// 0) and for ghost cells (computed here every stage: a halo exchange rewrote their rows).
+int limit_stage(dg_ctx* c, int st, const double* in, double* out, cudaStream_t s) {
     if (!c->cfg.limiter) return DG_OK;
     const int64_t stats_begin = (st == 0 && !c->lim_valid) ? 0 : c->nowned;
     const int rc = timed(c, 4, s, [&] {
         return launch_limiter_stage(c->cfg.order, c->qv, out, in, c->d_lim_nbr, c->d_phi_v, c->ncell, c->nowned,
                                     stats_begin, c->cfg.gamma, c->cfg.limiter == 2, c->d_lim_stats[st],
-                                    c->d_lim_stats[(st + 1) % 3], mir, c->sms, s, &g_launches);
+                                    c->d_lim_stats[(st + 1) % 3], c->sms, s, &g_launches);
     });
     if (rc == DG_OK && st != 1) c->lim_valid = true;  // stage 0 made them valid, stage 2 rewrote them
     return rc;
@@ -419,7 +418,7 @@ int step_fp64(dg_ctx* c, double dt, cudaStream_t s, int st0, int st1) {
         if (rc) return rc;
         rc = timed(c, 1, s, [&] { return fp64_element(c, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 1, s); });
         if (rc) return rc;
-        if ((rc = limit_stage(c, st, in[st], out[st], nullptr, s))) return rc;
+        if ((rc = limit_stage(c, st, in[st], out[st], s))) return rc;
     }
     return DG_OK;
 }
@@ -429,10 +428,7 @@ int step(dg_ctx* c, double dt, cudaStream_t s, int st0 = 0, int st1 = 3) {
     if (c->has_dirichlet && !c->d_UD) return DG_E_STATE;
     auto tm = [&](int cls, auto&& fn) { return timed(c, cls, s, fn); };
     if (c->cfg.precision == DG_PREC_MIXED) {
-        // post(in, out, mir_out) after stage st, whose output mirror is mir_out = (st + 1) % 3
-        auto post = [&](const double* in, double* out, int mir) {
-            return limit_stage(c, (mir + 2) % 3, in, out, c->mixed.mir[mir], s);
-        };
+        auto post = [&](const double* in, double* out, int st) { return limit_stage(c, st, in, out, s); };
         auto stages = [&](int a0, int a1) {
             if (c->cfg.schedule == 1)
                 return step_persistent(c->mixed, c->d_queue, c->qs, c->pp, c->d_Un, c->d_Ua, c->d_Ub, dt, s,
@@ -461,16 +457,14 @@ int stage_phase_mixed(dg_ctx* c, double dt, int st, int phase, cudaStream_t s) {
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
     const double* in[3] = {c->d_Un, c->d_Ua, c->d_Ub};
     double* out[3] = {c->d_Ua, c->d_Ub, c->d_Un};
-    const int mi = st, mo = (st + 1) % 3;
     auto K = [&](int which, int g0, int g1) {
-        return mixed_kernel(m, which, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, &g_launches, mi, mo,
-                            g0, g1);
+        return mixed_kernel(m, which, in[st], c->d_Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, &g_launches, g0, g1);
     };
     if (phase == 0) return timed(c, 0, s, [&] { return K(0, 0, m.nfgroups_inner); });
     int rc = viscous_stage(c, in[st], s);
     if (rc || (rc = timed(c, 0, s, [&] { return K(0, m.nfgroups_inner, m.nfgroups); }))) return rc;
     if ((rc = timed(c, 1, s, [&] { return K(1, 0, -1); }))) return rc;
-    return limit_stage(c, st, in[st], out[st], m.mir[mo], s);
+    return limit_stage(c, st, in[st], out[st], s);
 }
 
 int launches_per_step(const dg_ctx* c) {
@@ -968,7 +962,6 @@ int autotune_two_launch(dg_ctx* c, double dt, double* save, size_t nstate, char*
                         ", \"ms_per_step\": " + std::to_string(best) + "}}"
                   : std::string("null}");
     cudaMemcpyAsync(c->d_Un, save, nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
-    mixed_mirror(c->mixed, c->d_Un, 0, c->stream, &g_launches);
     c->lim_valid = false;
     cudaStreamSynchronize(c->stream);
     cudaFree(save);
@@ -1007,7 +1000,7 @@ int dg_limit_device(dg_ctx* c, double* U, const double* Uprev, int only_avg, voi
     if (!c->d_lim_bnd && (rc = dev_alloc(&c->d_lim_bnd, (size_t)c->ncell * 10))) return rc;
     g_launches += 2;
     return launch_limiter(c->cfg.order, c->qv, U, Uprev, c->d_lim_nbr, c->d_phi_v, c->ncell, c->nowned,
-                          c->cfg.gamma, only_avg != 0, c->d_lim_bnd, nullptr, c->sms, (cudaStream_t)stream);
+                          c->cfg.gamma, only_avg != 0, c->d_lim_bnd, c->sms, (cudaStream_t)stream);
 }
 
 int dg_limit(dg_ctx* c, double* U, const double* Uprev, size_t stride, int only_avg) {
@@ -1030,9 +1023,6 @@ int dg_set_state(dg_ctx* c, const double* U, size_t stride) {
     c->lim_valid = false;
     int rc = copy_in(c, c->d_Un, U, stride, c->stream);
     if (rc) return rc;
-    // the mixed form reads U^n's split deviation coefficients from a mirror the steps keep current
-    if (c->cfg.precision == DG_PREC_MIXED && (rc = mixed_mirror(c->mixed, c->d_Un, 0, c->stream, &g_launches)))
-        return rc;
     c->have_state = true;
     return cuda_ok(cudaStreamSynchronize(c->stream));
 }
@@ -1147,11 +1137,9 @@ int dg_halo_unpack(dg_ctx* c, int which, const int64_t* rows_dev, int64_t n, con
 }
 
 int dg_refresh_split(dg_ctx* c, int which, const int64_t* elems, int64_t n, void* stream) {
+    (void)stream;
     if (!c || which < 0 || which > 2 || n < 0 || (n > 0 && !elems)) return DG_E_ARG;
-    if (c->cfg.precision != DG_PREC_MIXED || n == 0) return DG_OK;
-    DG_CUDA(cudaSetDevice(c->cfg.device));
-    const cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    return mixed_mirror_list(c->mixed, dg_state_device(c, which), which, elems, n, s, &g_launches);
+    return DG_OK;  // the mixed kernels split the FP64 rows as they load them: no copy to refresh
 }
 
 int dg_ssprk3_stage_phase(dg_ctx* c, double dt, int stage, int phase) {
@@ -1295,7 +1283,6 @@ int dg_autotune(dg_ctx* c, double dt, char* report, size_t len) {
           ", \"regions\": " + std::to_string(c->qs.nregions) + ", \"lag\": " + std::to_string(bestp.lag) +
           ", \"ms_per_step\": " + std::to_string(best) + "}}";
     cudaMemcpyAsync(c->d_Un, save, nstate * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
-    mixed_mirror(c->mixed, c->d_Un, 0, c->stream, &g_launches);
     c->lim_valid = false;
     cudaStreamSynchronize(c->stream);
     cudaFree(save);

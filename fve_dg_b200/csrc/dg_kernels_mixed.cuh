@@ -122,7 +122,6 @@ struct ElemGroup {   // up to three elements with equal face maps in canonical f
 
 struct MixedFaceArgs {
     const double* U;
-    const uint32_t* mir;    // U's deviation coefficients c_b (b >= 1) as A rows, [ncell][5][KB]
     const FaceInfo* fi;
     const FaceGroup* groups;
     const double* UD;
@@ -138,8 +137,6 @@ struct MixedElemArgs {
     const double* U;
     const double* U0;
     double* out;
-    const uint32_t* mir;     // U's split deviation coefficients
-    uint32_t* mir_out;       // RK mode: the new stage's split deviation coefficients
     const uint32_t* dev;     // face records (written by the face kernel)
     const double* geo;       // [ncell][10] J^-T row-major, detJ
     const double* inv_detj;  // [ncell]
@@ -221,6 +218,32 @@ __device__ __forceinline__ void load_afrag(AFrag<K>& A, const uint32_t* r0, cons
     }
 }
 
+// Rows gid and gid + 8 of an A operand straight from FP64 state rows (null: a zero row): r points
+// at a cell's variable-k coefficients, mode b at r[5 b]; column x of the row is mode x + 1 (the
+// deviation modes), split into BF16 hi/lo in registers exactly as a stored split row would be.
+template <int K, int NB, bool SMEM = false>
+__device__ __forceinline__ void load_afrag_state(AFrag<K>& A, const double* r0, const double* r1, int lane) {
+    const int tq = lane & 3;
+    auto v = [&](const double* r, int x) -> float {
+        if (!r || x + 1 >= NB) return 0.f;
+        if constexpr (SMEM) return (float)r[5 * (x + 1)];
+        else return (float)__ldg(r + 5 * (x + 1));
+    };
+    #pragma unroll
+    for (int t = 0; t < KTiles<K>::N16; ++t) {
+        const int c = t * 16 + 2 * tq;
+        split2(v(r0, c), v(r0, c + 1), A.h[t][0], A.l[t][0]);
+        split2(v(r1, c), v(r1, c + 1), A.h[t][1], A.l[t][1]);
+        split2(v(r0, c + 8), v(r0, c + 9), A.h[t][2], A.l[t][2]);
+        split2(v(r1, c + 8), v(r1, c + 9), A.h[t][3], A.l[t][3]);
+    }
+    if constexpr (KTiles<K>::TAIL) {
+        const int c = KTiles<K>::N16 * 16 + 2 * tq;
+        split2(v(r0, c), v(r0, c + 1), A.th[0], A.tl[0]);
+        split2(v(r1, c), v(r1, c + 1), A.th[1], A.tl[1]);
+    }
+}
+
 // acc += A(full tile t) * B(n-tile at tbn, tile t): three products
 __device__ __forceinline__ void mma3_tile(float acc[4], const uint32_t h[4], const uint32_t l[4], const uint32_t* tbn,
                                           int t, int lane) {
@@ -245,29 +268,6 @@ __device__ __forceinline__ void mma_bt(float acc[4], const AFrag<K>& A, const ui
     #pragma unroll
     for (int t = 0; t < KTiles<K>::N16; ++t) mma3_tile(acc, A.h[t], A.l[t], tbn, t, lane);
     if constexpr (KTiles<K>::TAIL) mma3_tail<K>(acc, A.th, A.tl, tbn, lane);
-}
-
-// Writes the split deviation coefficients of a state as A rows (after an upload, or for a residual
-// of an arbitrary state): one thread per (element, var, column pair).
-template <int NB>
-__global__ void mirror_split(const double* __restrict__ U, uint32_t* __restrict__ mir, int64_t ncell,
-                             const int64_t* __restrict__ list) {
-    constexpr int KB = pad8(NB - 1), NP = KB / 2;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ncell * 5 * NP) return;
-    const int64_t r = i / NP;
-    const int x = 2 * (int)(i - r * NP);
-    const int64_t j = r / 5;
-    const int k = (int)(r - j * 5);
-    const int64_t e = list ? list[j] : j;  // the listed elements only (ghost rows after an exchange)
-    const int64_t row = e * 5 + k;
-    const double* u = U + e * (5 * NB) + k;
-    const float v0 = x + 1 < NB ? (float)u[5 * (x + 1)] : 0.f;
-    const float v1 = x + 2 < NB ? (float)u[5 * (x + 2)] : 0.f;
-    uint32_t hi, lo;
-    split2(v0, v1, hi, lo);
-    mir[row * KB + arow_hi_word<KB>(x)] = hi;
-    mir[row * KB + arow_lo_word<KB>(x)] = lo;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -330,18 +330,18 @@ __device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi,
     }
     __syncwarp();
     for (int s = 0; s < nside; ++s) {
-        const uint32_t* p0 = nullptr;
-        const uint32_t* p1 = nullptr;
+        const double* p0 = nullptr;
+        const double* p1 = nullptr;
         if (gid < 5 * grp.n) {
             const FaceInfo& F = a.fi[grp.f[gid / 5]];
-            p0 = a.mir + ((int64_t)(s ? F.c1 : F.c0) * 5 + gid % 5) * KB;
+            p0 = a.U + (int64_t)(s ? F.c1 : F.c0) * (5 * NB) + gid % 5;
         }
         if (gid + 8 < 5 * grp.n) {
             const FaceInfo& F = a.fi[grp.f[(gid + 8) / 5]];
-            p1 = a.mir + ((int64_t)(s ? F.c1 : F.c0) * 5 + (gid + 8) % 5) * KB;
+            p1 = a.U + (int64_t)(s ? F.c1 : F.c0) * (5 * NB) + (gid + 8) % 5;
         }
         AFrag<KB> A;
-        load_afrag<KB, false>(A, p0, p1, lane);
+        load_afrag_state<KB, NB>(A, p0, p1, lane);
         const uint32_t* tb = a.t.tfa + perm[s] * (MF / 8) * KTiles<KB>::NT_U32;
         const float c00 = sm.sC0[s][gid], c01 = sm.sC0[s][gid + 8];
         #pragma unroll
@@ -444,28 +444,31 @@ struct alignas(16) ElemMixedSmem {
     int sE[3];
 };
 
-// Per-block tables of the element kernel's epilogue: for DOF r = 5 j + k of an element, (j, k) and
-// the BF16 offsets of its hi/lo parts in the element's A rows; and the inverse reference mass.
+// Per-block tables of the element kernel's epilogue: for DOF r = 5 j + k of an element, (j, k); and
+// the inverse reference mass.
 template <int NB>
 struct ElemTables {
-    int4 dof[5 * NB];
+    int2 dof[5 * NB];
     double inv_mass[NB];
 };
 
 template <int NB>
 __device__ __forceinline__ void element_tables_init(ElemTables<NB>& T, const double* inv_mass) {
-    constexpr int KB = pad8(NB - 1);
     for (int r = threadIdx.x; r < 5 * NB; r += blockDim.x) {
         const int j = r / 5, k = r - 5 * j;
-        int hw = 0, lw = 0;
-        if (j > 0) {
-            hw = 2 * (k * KB + arow_hi_word<KB>(j - 1)) + ((j - 1) & 1);
-            lw = 2 * (k * KB + arow_lo_word<KB>(j - 1)) + ((j - 1) & 1);
-        }
-        T.dof[r] = make_int4(j, k, hw, lw);
+        T.dof[r] = make_int2(j, k);
     }
     for (int j = threadIdx.x; j < NB; j += blockDim.x) T.inv_mass[j] = inv_mass[j];
     __syncthreads();
+}
+
+// One DOF of the SSP-RK3 stage update, a0 U^n + a1 (U - s R) with s = dt / (det J M_j), every
+// product and sum rounded explicitly, so that every element kernel computes it bit for bit alike
+// (left to the compiler, the contraction into FMAs may differ between kernels).
+__device__ __forceinline__ double rk_update(bool with_u0, double a0, double u0, double a1, double u, double s,
+                                            double R) {
+    const double x = __fma_rn(-s, R, u);
+    return with_u0 ? __fma_rn(a1, x, __dmul_rn(a0, u0)) : __dmul_rn(a1, x);
 }
 
 __device__ __forceinline__ void dmma884(double d[2], double a, double b) {
@@ -506,12 +509,12 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
             asm volatile("prefetch.global.L2 [%0];" ::"l"(addr));
         }
     }
-    if (a.volume) {
-        constexpr int MB = 5 * KB * 4, ML = (MB + 127) / 128;
+    {
+        constexpr int MB = 5 * NB * 8, ML = (MB + 127) / 128;
         for (int i = lane; i < ne * ML; i += 32) {
             const int el = i / ML, part = i - el * ML;
             asm volatile("prefetch.global.L2 [%0];" ::"l"(
-                reinterpret_cast<const char*>(a.mir + (int64_t)grp.e[el] * 5 * KB) + part * 128));
+                reinterpret_cast<const char*>(a.U + (int64_t)grp.e[el] * 5 * NB) + part * 128));
         }
     }
     if (lane < 16) sm.sC0[lane] = lane < 5 * ne ? (float)__ldg(a.U + (int64_t)grp.e[lane / 5] * (5 * NB) + lane % 5) : 0.f;
@@ -564,8 +567,8 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
     if (a.volume) {
         {   // values at the volume points
             AFrag<KB> A;
-            load_afrag<KB, false>(A, v0 ? a.mir + ((int64_t)grp.e[r0 / 5] * 5 + r0 % 5) * KB : nullptr,
-                                  v1 ? a.mir + ((int64_t)grp.e[r1 / 5] * 5 + r1 % 5) * KB : nullptr, lane);
+            load_afrag_state<KB, NB>(A, v0 ? a.U + (int64_t)grp.e[r0 / 5] * (5 * NB) + r0 % 5 : nullptr,
+                                     v1 ? a.U + (int64_t)grp.e[r1 / 5] * (5 * NB) + r1 % 5 : nullptr, lane);
             const float c00 = sm.sC0[r0], c01 = sm.sC0[r1];
             #pragma unroll
             for (int nt = 0; nt < MV / 8; ++nt) {
@@ -692,7 +695,7 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
     if (a.mode == 0) {
         for (int i = lane; i < ne * 5 * NB; i += 32) {
             const int el = i / (5 * NB), r = i - el * (5 * NB);
-            const int4 d = T.dof[r];
+            const int2 d = T.dof[r];
             const int64_t idx = (int64_t)sm.sE[el] * (5 * NB) + r;
             const double R = sR[(el * 5 + d.y) * LDR + d.x];
             a.out[idx] = a.Rv ? R - a.Rv[idx] : R;
@@ -702,7 +705,6 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
         // issued before its first use, so a group pays two dependent round trips for them instead
         // of one per round of 32 DOFs. Stage 1 has a0 = 0: U^n is not read twice. U^n may be the
         // output buffer (stage 3) and is read through the coherent path.
-        unsigned short* mir16 = reinterpret_cast<unsigned short*>(a.mir_out);
         constexpr int NPL = (15 * NB + 31) / 32, EB = (NPL + 1) / 2;
         const int ndof = ne * 5 * NB;
         const bool u0 = a.a0 != 0.0;
@@ -723,17 +725,10 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
                 if (ix[j] < 0) continue;
                 const int i = lane + 32 * (b0 + j);
                 const int el = i / (5 * NB), r = i - el * (5 * NB);
-                const int4 d = T.dof[r];  // j, k, hi offset, lo offset
+                const int2 d = T.dof[r];  // mode j, variable k
                 const double R = a.Rv ? sR[(el * 5 + d.y) * LDR + d.x] - a.Rv[ix[j]] : sR[(el * 5 + d.y) * LDR + d.x];
-                const double un = (u0 ? a.a0 * vv[j] : 0.0) + a.a1 * (uu[j] - sm.sDT[el] * T.inv_mass[d.x] * R);
+                const double un = rk_update(u0, a.a0, vv[j], a.a1, uu[j], __dmul_rn(sm.sDT[el], T.inv_mass[d.x]), R);
                 a.out[ix[j]] = un;
-                if (d.x > 0) {
-                    unsigned short h, l;
-                    split1((float)un, h, l);
-                    unsigned short* mrow = mir16 + (int64_t)sm.sE[el] * (10 * KB);
-                    mrow[d.z] = h;
-                    mrow[d.w] = l;
-                }
             }
         }
     }
@@ -742,18 +737,17 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
 
 // ------------------------------------------------------------------------------------------------
 // Staged element kernel. The plain element kernel issues its global loads phase by phase (the
-// split rows, the face records, the FP64 parts, then ten rounds of state rows in the update), so a
-// group waits for about fifteen dependent L2/DRAM round trips. Here lane 0 of the warp issues TMA
-// bulk copies of every row the group reads (split rows, the four face records of each element,
-// the stage input and U^n rows, the geometry) into the warp's staging area as soon as the group
-// record is known; the warp waits once on its mbarrier and every later phase reads shared memory.
+// stage input rows, the face records, the FP64 parts, then the state rows of the update), so a
+// group waits for several dependent L2/DRAM round trips. Here lane 0 of the warp issues TMA bulk
+// copies of every row the group reads (the four face records of each element, the stage input and
+// U^n rows, the geometry) into the warp's staging area as soon as the group record is known; the
+// warp waits once on its mbarrier and every later phase reads shared memory.
 // State rows must be whole 16-byte units (5 NB doubles: P1..P3).
 // ------------------------------------------------------------------------------------------------
 template <int NB, int NQF>
 struct alignas(16) ElemStage {
     static constexpr int KB = pad8(NB - 1), FR = face_rec_words(NQF);
-    static constexpr unsigned MIRB = 5 * KB * 4, FRB = FR * 4, UB = 5 * NB * 8, GEOB = 80;
-    uint32_t mir[3][5 * KB];  // split deviation coefficients of the stage input (A rows)
+    static constexpr unsigned FRB = FR * 4, UB = 5 * NB * 8, GEOB = 80;
     uint32_t face[3][4][FR];  // the face records of each element's faces, canonical face order
     double U[3][5 * NB];      // stage input rows
     double U0[3][5 * NB];     // U^n rows (stages with a0 != 0)
@@ -803,11 +797,10 @@ __device__ __forceinline__ bool element_group_staged(const MixedElemArgs& a, int
         // the warp's reads of the previous group (generic proxy) are ordered before the copies'
         // writes (async proxy) by the __syncwarp that ended that group and this fence
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const unsigned per = (a.volume ? G::MIRB : 0u) + 4u * G::FRB + G::UB + (need_u0 ? G::UB : 0u) + G::GEOB;
+        const unsigned per = 4u * G::FRB + G::UB + (need_u0 ? G::UB : 0u) + G::GEOB;
         mbar_arrive_expect_tx(&st.bar, per * (unsigned)ne);
         for (int el = 0; el < ne; ++el) {
             const int64_t e = grp.e[el];
-            if (a.volume) bulk_copy_g2s(st.mir[el], a.mir + e * 5 * KB, G::MIRB, &st.bar);
             #pragma unroll
             for (int q = 0; q < 4; ++q)
                 bulk_copy_g2s(st.face[el][q], a.dev + (int64_t)grp.face[el][q] * G::FR, G::FRB, &st.bar);
@@ -870,8 +863,8 @@ __device__ __forceinline__ bool element_group_staged(const MixedElemArgs& a, int
     if (a.volume) {
         {   // values at the volume points
             AFrag<KB> A;
-            load_afrag_smem<KB>(A, v0 ? st.mir[r0 / 5] + (r0 % 5) * KB : nullptr,
-                                v1 ? st.mir[r1 / 5] + (r1 % 5) * KB : nullptr, lane);
+            load_afrag_state<KB, NB, true>(A, v0 ? st.U[r0 / 5] + r0 % 5 : nullptr,
+                                           v1 ? st.U[r1 / 5] + r1 % 5 : nullptr, lane);
             const float c00 = sm.sC0[r0], c01 = sm.sC0[r1];
             #pragma unroll
             for (int nt = 0; nt < MV / 8; ++nt) {
@@ -986,26 +979,18 @@ __device__ __forceinline__ bool element_group_staged(const MixedElemArgs& a, int
     }
     __syncwarp();
     const double* sR = reinterpret_cast<const double*>(&sm.sG[0][0]);
-    unsigned short* mir16 = reinterpret_cast<unsigned short*>(a.mir_out);
     for (int i = lane; i < ne * 5 * NB; i += 32) {
         const int el = i / (5 * NB), r = i - el * (5 * NB);
-        const int4 d = T.dof[r];
+        const int2 d = T.dof[r];
         const int64_t e = sm.sE[el];
         const int64_t idx = e * (5 * NB) + r;
         const double R = a.Rv ? sR[(el * 5 + d.y) * LDR + d.x] - a.Rv[idx] : sR[(el * 5 + d.y) * LDR + d.x];
         if (a.mode == 0) {
             a.out[idx] = R;
         } else {
-            const double u0 = need_u0 ? a.a0 * st.U0[el][r] : 0.0;
-            const double un = u0 + a.a1 * (st.U[el][r] - sm.sDT[el] * T.inv_mass[d.x] * R);
+            const double un = rk_update(need_u0, a.a0, need_u0 ? st.U0[el][r] : 0.0, a.a1, st.U[el][r],
+                                        __dmul_rn(sm.sDT[el], T.inv_mass[d.x]), R);
             a.out[idx] = un;
-            if (d.x > 0) {
-                unsigned short h, l;
-                split1((float)un, h, l);
-                unsigned short* mrow = mir16 + e * (10 * KB);
-                mrow[d.z] = h;
-                mrow[d.w] = l;
-            }
         }
     }
     __syncwarp();
@@ -1090,8 +1075,6 @@ struct MixedData {
     // staged by TMA bulk copies (P1..P3, 16-byte aligned state buffers); chosen by dg_autotune
     int elem_kernel = 0;
     int elem_ctas = 1;                // resident CTAs per SM of the staged kernel: 1 or 2
-    // A rows of the deviation coefficients of the states Un, Ua, Ub and of a residual input
-    uint32_t* mir[4] = {nullptr, nullptr, nullptr, nullptr};
     // host copies the tile schedule of the persistent form is built from
     std::vector<FaceGroup> hfg;
     std::vector<ElemGroup> heg;
@@ -1290,8 +1273,6 @@ inline int init_mixed(MixedData& m, const Tables& tab, const std::vector<double>
     }
     // padding columns of the A rows stay zero: allocation clears them and no kernel writes them
     if ((rc = mixed_alloc(m, &m.dev, (size_t)nface * face_rec_words(NQF)))) return rc;
-    for (int i = 0; i < 4; ++i)
-        if ((rc = mixed_alloc(m, &m.mir[i], (size_t)ncell * 5 * KB))) return rc;
     if ((rc = mixed_alloc(m, &m.err, 1))) return rc;
     m.fi = d_fi; m.geo = d_geo;
     int dev = 0;
@@ -1309,10 +1290,9 @@ inline void free_mixed(MixedData& m) {
 
 inline void set_mixed_dirichlet(MixedData& m, const double* UD) { m.UD = UD; }
 
-inline MixedFaceArgs face_args(const MixedData& m, const double* U, int mir_in, int face_mask, int g0 = 0,
-                               int g1 = -1) {
+inline MixedFaceArgs face_args(const MixedData& m, const double* U, int face_mask, int g0 = 0, int g1 = -1) {
     MixedFaceArgs fa;
-    fa.U = U; fa.mir = m.mir[mir_in]; fa.fi = m.fi; fa.groups = m.fgroups; fa.UD = m.UD; fa.dev = m.dev;
+    fa.U = U; fa.fi = m.fi; fa.groups = m.fgroups; fa.UD = m.UD; fa.dev = m.dev;
     fa.t = m.t; fa.ngroups = m.nfgroups; fa.gamma = m.gamma; fa.flux = m.flux;
     if (g1 >= 0) {  // face groups [g0, g1) only
         fa.groups = m.fgroups + g0;
@@ -1323,9 +1303,9 @@ inline MixedFaceArgs face_args(const MixedData& m, const double* U, int mir_in, 
 }
 
 inline MixedElemArgs elem_args(const MixedData& m, const double* U, const double* U0, double* out, int mode,
-                               double dt, double a0, double a1, int with_volume, int mir_in, int mir_out) {
+                               double dt, double a0, double a1, int with_volume) {
     MixedElemArgs ea;
-    ea.U = U; ea.U0 = U0; ea.out = out; ea.mir = m.mir[mir_in]; ea.mir_out = mir_out >= 0 ? m.mir[mir_out] : nullptr;
+    ea.U = U; ea.U0 = U0; ea.out = out;
     ea.dev = m.dev; ea.geo = m.geo; ea.inv_detj = m.inv_detj; ea.groups = m.egroups;
     ea.t = m.t; ea.ngroups = m.negroups; ea.gamma = m.gamma; ea.volume = with_volume;
     ea.dt = dt; ea.a0 = a0; ea.a1 = a1; ea.mode = mode;
@@ -1348,23 +1328,20 @@ inline int ensure_smem(Kernel k, size_t smem, unsigned long long& done_mask) {
     return DG_OK;
 }
 
-// which: 0 = face fluxes, 1 = element kernel (volume + face integrals + update), 4 = mirror split.
+// which: 0 = face fluxes, 1 = element kernel (volume + face integrals + update).
 template <int NB, int NQV, int NQF, int WE>
 inline int mixed_launch(MixedData& m, int which, const double* U, const double* U0, double* out, int mode,
-                        double dt, double a0, double a1, int face_mask, int with_volume, cudaStream_t s,
-                        int mir_in, int mir_out, int g0, int g1) {
-    if (which == 4) {
-        const int64_t n = m.ncell * 5 * (pad8(NB - 1) / 2);
-        mirror_split<NB><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(U, m.mir[mir_in], m.ncell, nullptr);
-    } else if (which == 0) {
+                        double dt, double a0, double a1, int face_mask, int with_volume, cudaStream_t s, int g0,
+                        int g1) {
+    if (which == 0) {
         constexpr int W = 4;  // 4-warp CTAs: finer-grained scheduling than 8 at the same occupancy
         const int n = g1 < 0 ? m.nfgroups : g1 - g0;
         const int g = (int)std::min<int64_t>((n + W - 1) / W, (int64_t)m.sms * 64);
-        face_flux_mixed<NB, NQF, W><<<g, W * 32, 0, s>>>(face_args(m, U, mir_in, face_mask, g0, g1));
+        face_flux_mixed<NB, NQF, W><<<g, W * 32, 0, s>>>(face_args(m, U, face_mask, g0, g1));
     } else if (m.elem_kernel == 2 && (5 * NB * 8) % 16 == 0 && ((uintptr_t)U & 15) == 0 &&
                ((uintptr_t)U0 & 15) == 0) {
         if constexpr ((5 * NB * 8) % 16 == 0) {
-            const auto ea = elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out);
+            const auto ea = elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume);
             if (m.elem_ctas == 2) {
                 constexpr int W = elem_staged_warps<NB, NQV, NQF>(2);
                 constexpr size_t smem = elem_staged_warp_smem<NB, NQV, NQF>() * W;
@@ -1390,7 +1367,7 @@ inline int mixed_launch(MixedData& m, int which, const double* U, const double* 
         if (rc) return rc;
         const int g = (int)std::min<int64_t>((m.negroups + WE - 1) / WE, (int64_t)m.sms * 32);
         element_mixed<NB, NQV, NQF, WE><<<g, WE * 32, smem, s>>>(
-            elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out));
+            elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume));
     }
     return cuda_status(cudaGetLastError());
 }
@@ -1417,18 +1394,17 @@ inline int mixed_elem_shapes(const MixedData& m, ElemShape out[3]) {
     return 0;
 }
 
-// mir_in: mirror of U (0..3); mir_out: mirror the update writes (RK mode), or -1.
 // Face launches (which 0) cover face groups [g0, g1) (g1 < 0: all of them).
 inline int mixed_kernel(MixedData& m, int which, const double* U, const double* U0, double* out, int mode,
                         double dt, double a0, double a1, int face_mask, int with_volume, cudaStream_t s,
-                        std::atomic<int64_t>* launches, int mir_in, int mir_out, int g0 = 0, int g1 = -1) {
+                        std::atomic<int64_t>* launches, int g0 = 0, int g1 = -1) {
     if (!m.ready) return DG_E_ARG;
     if (which == 0 && g1 >= 0 && g1 <= g0) return DG_OK;  // an empty range: nothing to launch
     ++*launches;
 #define X(P, QV, QF, NB, NQV, NQF, W)                                                                           \
     if (m.order == P && m.qv == QV && m.qf == QF)                                                               \
         return mixed_launch<NB, NQV, NQF, W>(m, which, U, U0, out, mode, dt, a0, a1, face_mask, with_volume, s, \
-                                             mir_in, mir_out, g0, g1);
+                                             g0, g1);
     FVEDG_MIXED_COMBOS(X)
 #undef X
     return DG_E_ARG;
@@ -1438,52 +1414,26 @@ inline int mixed_kernel(MixedData& m, int which, const double* U, const double* 
 template <class Timed>
 inline int mixed_stage(MixedData& m, const double* U, const double* U0, double* out, int mode, double dt, double a0,
                        double a1, int face_mask, int with_volume, cudaStream_t s, std::atomic<int64_t>* launches,
-                       Timed&& timed, int mir_in, int mir_out) {
+                       Timed&& timed) {
     auto K = [&](int which) {
-        return mixed_kernel(m, which, U, U0, out, mode, dt, a0, a1, face_mask, with_volume, s, launches, mir_in,
-                            mir_out);
+        return mixed_kernel(m, which, U, U0, out, mode, dt, a0, a1, face_mask, with_volume, s, launches);
     };
     const int rc = timed(0, [&] { return K(0); });
     if (rc) return rc;
     return timed(1, [&] { return K(1); });
 }
 
-// The mirror of an arbitrary state (the upload, the residual input) is written by a split kernel.
-inline int mixed_mirror(MixedData& m, const double* U, int mir, cudaStream_t s, std::atomic<int64_t>* launches) {
-    return mixed_kernel(m, 4, U, U, nullptr, 0, 0.0, 0.0, 0.0, 0, 0, s, launches, mir, -1);
-}
-
-// Rewrites the mirror rows of the listed elements only (device list of n element indices).
-inline int mixed_mirror_list(MixedData& m, const double* U, int mir, const int64_t* list, int64_t n, cudaStream_t s,
-                             std::atomic<int64_t>* launches) {
-    if (!m.ready) return DG_E_ARG;
-    if (n == 0) return DG_OK;
-#define X(P, QV, QF, NB, NQV, NQF, W)                                                                   \
-    if (m.order == P && m.qv == QV && m.qf == QF) {                                                     \
-        const int64_t nt = n * 5 * (pad8(NB - 1) / 2);                                                  \
-        ++*launches;                                                                                    \
-        mirror_split<NB><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(U, m.mir[mir], n, list);          \
-        return cuda_status(cudaGetLastError());                                   \
-    }
-    FVEDG_MIXED_COMBOS(X)
-#undef X
-    return DG_E_ARG;
-}
-
 inline int residual_mixed(MixedData& m, const double* U, double* R, int part, cudaStream_t s,
                           std::atomic<int64_t>* launches) {
     const int mask = part == 0 ? 3 : part == 1 ? 0 : part == 2 ? 1 : 2;
-    int rc = mixed_mirror(m, U, 3, s, launches);
-    if (rc) return rc;
     return mixed_stage(m, U, U, R, 0, 0.0, 0.0, 0.0, mask, part == 0 || part == 1, s, launches,
-                       [](int, auto&& fn) { return fn(); }, 3, -1);
+                       [](int, auto&& fn) { return fn(); });
 }
 
 inline int mixed_launches_per_step(const MixedData&) { return 6; }
 
-// SSP-RK3 step; `timed(cls, fn)` runs fn (one launch) and may bracket it with timing events. The
-// mirror of Un must be current (the upload writes it, and stage 3 of every step rewrites it).
-// `post(in, out, mir_out)` runs after every stage (the limiter, or nothing). Stages st0..st1-1 only
+// SSP-RK3 step; `timed(cls, fn)` runs fn (one launch) and may bracket it with timing events.
+// `post(in, out, st)` runs after every stage st (the limiter, or nothing). Stages st0..st1-1 only
 // (one stage at a time when a halo exchange runs between stages).
 template <class Timed, class Post>
 inline int step_mixed(MixedData& m, double* Un, double* Ua, double* Ub, double dt, cudaStream_t s,
@@ -1492,10 +1442,9 @@ inline int step_mixed(MixedData& m, double* Un, double* Ua, double* Ub, double d
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
     const double* in[3] = {Un, Ua, Ub};
     double* out[3] = {Ua, Ub, Un};
-    const int mi[3] = {0, 1, 2}, mo[3] = {1, 2, 0};
     for (int st = st0; st < st1; ++st) {
-        int rc = mixed_stage(m, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches, timed, mi[st], mo[st]);
-        if (rc || (rc = post(in[st], out[st], mo[st]))) return rc;
+        int rc = mixed_stage(m, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches, timed);
+        if (rc || (rc = post(in[st], out[st], st))) return rc;
     }
     return DG_OK;
 }

@@ -169,17 +169,15 @@ __global__ void __launch_bounds__(kLimWarps * 32)
 // [ncell][4], the cell itself across a boundary face), which is the max/min over the cell's faces of
 // the face bounds. Point values are evaluated once; after a step scales the modes l >= 1 of a
 // variable by theta, its point values become avg + theta (v - avg) (phi_0 = 1), which is what the
-// reference re-evaluates. A step whose test passes at every point costs one vote. mir: when
-// non-null, the element's split coefficient rows (A rows, [ncell][5][KB]) are rewritten if the
-// limiter changed the element. stats_out: when non-null, the statistics of the limited state (as
+// reference re-evaluates. A step whose test passes at every point costs one vote. stats_out: when
+// non-null, the statistics of the limited state (as
 // limiter_cell_stats computes them: re-evaluated from the new coefficients where the limiter acted),
 // the next stage's bounds.
 template <int NB, int NQV>
 __global__ void __launch_bounds__(kLimWarps * 32)
     limiter_apply(double* __restrict__ U, const int* __restrict__ nbr, const double* __restrict__ stats,
-                  const double* __restrict__ phi, int64_t ncell, double gamma, int only_avg, uint32_t* __restrict__ mir,
+                  const double* __restrict__ phi, int64_t ncell, double gamma, int only_avg,
                   double* __restrict__ stats_out) {
-    constexpr int KB = pad8(NB - 1);
     constexpr int G = LimGroup<NQV>::G, CPW = 32 / G;
     constexpr int PPL = (NQV + G - 1) / G;  // points per lane
     static_assert(NQV <= kLimMaxPts, "volume rule too large");
@@ -317,18 +315,6 @@ __global__ void __launch_bounds__(kLimWarps * 32)
                     ug[5 + i] = c;
                 }
                 __syncwarp(gmask);
-                if (mir) {  // refresh the split rows of the changed element
-                    for (int i = gl; i < 5 * (KB / 2); i += G) {
-                        const int k = i / (KB / 2), x = 2 * (i - k * (KB / 2));
-                        const float v0 = x + 1 < NB ? (float)u[5 * (x + 1) + k] : 0.f;
-                        const float v1 = x + 2 < NB ? (float)u[5 * (x + 2) + k] : 0.f;
-                        uint32_t h, l;
-                        split2(v0, v1, h, l);
-                        uint32_t* row = mir + (e * 5 + k) * KB;
-                        row[arow_hi_word<KB>(x)] = h;
-                        row[arow_lo_word<KB>(x)] = l;
-                    }
-                }
                 if (stats_out && !only_avg) {  // the limited state's point values, re-evaluated
                     #pragma unroll
                     for (int r = 0; r < PPL; ++r) {
@@ -365,13 +351,13 @@ inline bool limiter_supported(int order, int qv) {
 // Bounds from Uprev, then the three steps on U (in place) for cells [0, napply) (the owned cells;
 // the statistics cover ghost cells too). stats: [ncell][10] scratch.
 inline int launch_limiter(int order, int qv, double* U, const double* Uprev, const int* nbr, const double* phi_v,
-                          int64_t ncell, int64_t napply, double gamma, int only_avg, double* stats, uint32_t* mir,
-                          int sms, cudaStream_t s) {
+                          int64_t ncell, int64_t napply, double gamma, int only_avg, double* stats, int sms,
+                          cudaStream_t s) {
 #define X(P, QV, NB, NQV)                                                                                        \
     if (order == P && qv == QV) {                                                                                \
         const unsigned ge = (unsigned)std::min<int64_t>((ncell + kLimWarps - 1) / kLimWarps, (int64_t)sms * 16); \
         limiter_cell_stats<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(Uprev, phi_v, 0, ncell, only_avg, stats);      \
-        limiter_apply<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(U, nbr, stats, phi_v, napply, gamma, only_avg, mir,  \
+        limiter_apply<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(U, nbr, stats, phi_v, napply, gamma, only_avg,       \
                                                              nullptr);                                           \
         return cuda_status(cudaGetLastError());                                            \
     }
@@ -405,7 +391,7 @@ inline int launch_limiter_stats(int order, int qv, const double* U, const double
 // exchange rewrote; none when stats_begin == ncell).
 inline int launch_limiter_stage(int order, int qv, double* U, const double* Uin, const int* nbr, const double* phi_v,
                                 int64_t ncell, int64_t napply, int64_t stats_begin, double gamma, int only_avg,
-                                double* stats_in, double* stats_out, uint32_t* mir, int sms, cudaStream_t s,
+                                double* stats_in, double* stats_out, int sms, cudaStream_t s,
                                 std::atomic<int64_t>* launches) {
     int rc = launch_limiter_stats(order, qv, Uin, phi_v, stats_begin, ncell, only_avg, stats_in, sms, s, launches);
     if (rc) return rc;
@@ -413,7 +399,7 @@ inline int launch_limiter_stage(int order, int qv, double* U, const double* Uin,
     if (order == P && qv == QV) {                                                                                 \
         const unsigned ge = (unsigned)std::min<int64_t>((napply + kLimWarps - 1) / kLimWarps, (int64_t)sms * 16); \
         limiter_apply<NB, NQV><<<ge, kLimWarps * 32, 0, s>>>(U, nbr, stats_in, phi_v, napply, gamma, only_avg,    \
-                                                             mir, stats_out);                                     \
+                                                             stats_out);                                          \
         ++*launches;                                                                                              \
         return cuda_status(cudaGetLastError());                                             \
     }

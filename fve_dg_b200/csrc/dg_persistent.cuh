@@ -220,7 +220,7 @@ inline void free_schedule(QueueSchedule& qs) {
 template <int NB, int NQV, int NQF, int W = 8>
 inline int persistent_launch(MixedData& m, QueueState* q, const QueueSchedule& qs, const PersistentParams& pp,
                              const double* U, const double* U0, double* out, int mode, double dt, double a0, double a1,
-                             int face_mask, int with_volume, cudaStream_t s, int mir_in, int mir_out) {
+                             int face_mask, int with_volume, cudaStream_t s) {
     if (!qs.ready || !(qs.built == pp)) return DG_E_STATE;
     auto kern = stage_persistent_mixed<NB, NQV, NQF, W>;
     constexpr size_t smem = persistent_warp_smem<NB, NQV, NQF>() * W;
@@ -238,8 +238,8 @@ inline int persistent_launch(MixedData& m, QueueState* q, const QueueSchedule& q
         done |= 1ull << (dev & 63);
     }
     const int bps = pp.max_blocks > 0 ? std::min(per_sm[dev & 63], pp.max_blocks) : per_sm[dev & 63];
-    const MixedFaceArgs fa = face_args(m, U, mir_in, face_mask);
-    const MixedElemArgs ea = elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume, mir_in, mir_out);
+    const MixedFaceArgs fa = face_args(m, U, face_mask);
+    const MixedElemArgs ea = elem_args(m, U, U0, out, mode, dt, a0, a1, with_volume);
     kern<<<m.sms * bps, W * 32, smem, s>>>(fa, ea, q, qs.tiles, qs.ntiles, qs.deps, qs.total,
                                            pp.spin_limit > 0 ? pp.spin_limit : kSpinLimit);
     return cuda_status(cudaGetLastError());
@@ -247,14 +247,13 @@ inline int persistent_launch(MixedData& m, QueueState* q, const QueueSchedule& q
 
 inline int persistent_kernel(MixedData& m, QueueState* q, const QueueSchedule& qs, const PersistentParams& pp,
                              const double* U, const double* U0, double* out, int mode, double dt, double a0, double a1,
-                             int face_mask, int with_volume, cudaStream_t s, std::atomic<int64_t>* launches, int mir_in,
-                             int mir_out) {
+                             int face_mask, int with_volume, cudaStream_t s, std::atomic<int64_t>* launches) {
     if (!m.ready) return DG_E_ARG;
     ++*launches;
 #define X(P, QV, QF, NB, NQV, NQF, W)                                                                              \
     if (m.order == P && m.qv == QV && m.qf == QF)                                                                  \
         return persistent_launch<NB, NQV, NQF, W>(m, q, qs, pp, U, U0, out, mode, dt, a0, a1, face_mask,           \
-                                                  with_volume, s, mir_in, mir_out);
+                                                  with_volume, s);
     FVEDG_MIXED_COMBOS(X)
 #undef X
     return DG_E_ARG;
@@ -269,14 +268,12 @@ inline int step_persistent(MixedData& m, QueueState* q, const QueueSchedule& qs,
     const double A1[3] = {1.0, 0.25, 2.0 / 3.0};
     const double* in[3] = {Un, Ua, Ub};
     double* out[3] = {Ua, Ub, Un};
-    const int mi[3] = {0, 1, 2}, mo[3] = {1, 2, 0};
     for (int st = st0; st < st1; ++st) {
         int rc = timed(2, [&] {
-            return persistent_kernel(m, q, qs, pp, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches,
-                                     mi[st], mo[st]);
+            return persistent_kernel(m, q, qs, pp, in[st], Un, out[st], 1, dt, A0[st], A1[st], 3, 1, s, launches);
         });
         if (rc) return rc;
-        if ((rc = post(in[st], out[st], mo[st]))) return rc;
+        if ((rc = post(in[st], out[st], st))) return rc;
     }
     return DG_OK;
 }

@@ -139,7 +139,6 @@ class PartitionedConvection:
         self.conv = ExplicitConvection(self.lm.mesh, device=device, **kw)
         self.dist, self._exchange, self.device = dist, exchange, device
         self.mixed = self.conv.precision == "mixed"
-        self._ghost_dev = None
         self._comm = None  # the exchange's stream when it overlaps the stage's first phase
 
     def torch_stream(self):
@@ -160,18 +159,6 @@ class PartitionedConvection:
 
     def get_owned(self):
         return self.conv.get_state()[: self.lm.n_owned]
-
-    def _refresh(self, which):
-        """After ghost rows of buffer `which` changed: the mixed form re-splits their coefficients."""
-        if not self.mixed or not len(self.lm.ghosts):
-            return
-        import torch
-        if self._ghost_dev is None:  # made on the context's stream, which the refresh then runs on
-            with torch.cuda.stream(self.torch_stream()):
-                self._ghost_dev = torch.arange(self.lm.n_owned, self.lm.ncell, dtype=torch.int64,
-                                               device=torch.device("cuda", self.device))
-        L.check(L.lib().dg_refresh_split(self.conv._ctx, int(which), ctypes.c_void_p(self._ghost_dev.data_ptr()),
-                                         int(self._ghost_dev.numel()), None), "dg_refresh_split")
 
     def rows_dev(self, kind, q):
         """Device copy of the local rows this part sends to ("send") or receives from ("recv") q."""
@@ -226,7 +213,6 @@ class PartitionedConvection:
                 self._exchange(which)
             else:
                 self._halo(which)
-        self._refresh(which)
 
     def stage(self, dt, st):
         L.check(L.lib().dg_ssprk3_stage(self.conv._ctx, float(dt), int(st)), "dg_ssprk3_stage")
@@ -256,7 +242,6 @@ class PartitionedConvection:
         done = torch.cuda.Event()
         done.record(self._comm)
         main.wait_event(done)
-        self._refresh(st)
         self.phase(dt, st, 1)
 
     def wait(self):

@@ -220,9 +220,10 @@ void* dg_stream(dg_ctx* ctx);
  * State buffer `which` on the device, packed [ncell][5*Nb]: 0 = U^n, 1 = U^(1), 2 = U^(2); stage s
  * reads buffer s and writes buffer (s + 1) mod 3. NULL for a bad argument. */
 double* dg_state_device(dg_ctx* ctx, int which);
-/* After rows of state buffer `which` were written from outside the library (a halo exchange): the
- * mixed form re-splits the coefficients of the n listed elements (device array of element indices)
- * on `stream` (a cudaStream_t, 0 = the context's stream). Nothing to do in the FP64 form. */
+/* After rows of state buffer `which` were written from outside the library (a halo exchange): kept
+ * for drivers written against earlier versions, in which the mixed form held split copies of the
+ * coefficients. Now every kernel splits the FP64 rows as it loads them, so there is nothing to
+ * refresh: it checks its arguments and returns DG_OK. */
 int dg_refresh_split(dg_ctx* ctx, int which, const int64_t* elems_dev, int64_t n, void* stream);
 /* Enqueues stage `stage` (0, 1, 2) of one SSP-RK3 step, with the limiter when configured, on the
  * context's stream and returns; dg_ssprk3(ctx, dt, 0) waits for it and reports a watchdog error.
@@ -230,8 +231,8 @@ int dg_refresh_split(dg_ctx* ctx, int which, const int64_t* elems_dev, int64_t n
 int dg_ssprk3_stage(dg_ctx* ctx, double dt, int stage);
 /* The same stage in two phases, so that a halo exchange overlaps work: phase 0 enqueues what reads
  * no ghost row (in the mixed two-launch form, the fluxes of the faces between owned elements;
- * otherwise nothing), phase 1 the rest. Between them, write the ghost rows of the stage input (and
- * call dg_refresh_split); phases 0 then 1 launch exactly what dg_ssprk3_stage launches. */
+ * otherwise nothing), phase 1 the rest. Between them, write the ghost rows of the stage input;
+ * phases 0 then 1 launch exactly what dg_ssprk3_stage launches. */
 int dg_ssprk3_stage_phase(dg_ctx* ctx, double dt, int stage, int phase);
 
 /* One mesh split across processes, for drivers that exchange halos with MPI or NCCL themselves
@@ -261,7 +262,7 @@ int dg_partition_recv(const dg_partition* part, int i, int* peer, int64_t* n, co
 /* Device gather / scatter of whole element rows (5 Nb doubles) of state buffer `which` (as
  * dg_state_device) for the exchange, on `stream` (0 = the context's stream): pack copies row
  * rows_dev[i] to slot i of buf_dev, unpack copies slot i into row rows_dev[i]. Rows outside the
- * context's cells are skipped. After an unpack the mixed form needs dg_refresh_split of those rows. */
+ * context's cells are skipped. */
 int dg_halo_pack(dg_ctx* ctx, int which, const int64_t* rows_dev, int64_t n, double* buf_dev, void* stream);
 int dg_halo_unpack(dg_ctx* ctx, int which, const int64_t* rows_dev, int64_t n, const double* buf_dev, void* stream);
 
