@@ -412,7 +412,7 @@ __device__ __forceinline__ void face_group_mixed(const MixedFaceArgs& a, int gi,
 }
 
 template <int NB, int NQF, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) face_flux_mixed(MixedFaceArgs a) {
+__global__ void __launch_bounds__(WARPS * 32, NB <= 20 ? 36 / WARPS : 24 / WARPS) face_flux_mixed(MixedFaceArgs a) {
     __shared__ FaceMixedSmem<NQF> sm[WARPS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int gi = blockIdx.x * WARPS + warp; gi < a.ngroups; gi += gridDim.x * WARPS)
