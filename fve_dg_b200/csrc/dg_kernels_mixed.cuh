@@ -14,11 +14,12 @@
 // Two kernels per RK stage. The face kernel interpolates both traces, evaluates the Riemann flux
 // and stores the flux deviations already split and in the element kernel's fragment order. The
 // element kernel does the volume term (values, flux, integral) and the four face integrals into
-// the same accumulators, then the FP64 parts and the RK update, and writes the new stage's split
-// coefficients for the next stage's MMAs.
+// the same accumulators, then the FP64 parts and the RK update (FP64 state only: both kernels split
+// the FP64 coefficient rows they read into BF16 hi/lo A fragments in registers, load_afrag_state).
 //
-// Operands in memory are kept in fragment order ("A rows", "B fragments" below): a lane fetches
-// its MMA registers for one 16-wide K tile, hi and lo, with one 128-bit load.
+// Operands kept in memory are in fragment order ("A rows" of the face records, "B fragments" of
+// the tables, below): a lane fetches its MMA registers for one 16-wide K tile, hi and lo, with one
+// 128-bit load.
 //
 // Only deviations go through the tensor cores: the mode-0 coefficient c_0 (phi_0 = 1) is added to
 // the traces in FP32 after the MMA; the volume flux is taken relative to the flux of the element
@@ -495,10 +496,9 @@ __device__ __forceinline__ void element_group_mixed(const MixedElemArgs& a, int 
     const int ne = grp.n;
     const int r0 = gid, r1 = gid + 8;
     const bool v0 = r0 < 5 * ne, v1 = r1 < 5 * ne;
-    // Pull the group's face records and split rows into L2 first (the addresses are known from the
-    // group record): they arrive while the earlier phases run, instead of one dependent DRAM round
-    // trip per phase. (The state rows of the update are read in batches there; prefetching them
-    // too measured no gain.) Prefetches take no registers; every address lies inside its row.
+    // Pull the group's face records and stage input rows into L2 first (the addresses are known
+    // from the group record): they arrive while the earlier phases run, instead of one dependent
+    // DRAM round trip per phase. Prefetches take no registers; every address lies inside its row.
     constexpr int FR = face_rec_words(NQF);
     {
         constexpr int NL = (FR * 4 + 127) / 128;
