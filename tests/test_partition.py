@@ -179,3 +179,29 @@ def test_native_plan_is_the_python_plan(nparts, kw):
             assert np.array_equal(nat.send[q], lm.send[q])
         for q in lm.recv:
             assert np.array_equal(nat.recv[q], lm.recv[q])
+
+
+def test_native_plan_rejects_bad_input():
+    import ctypes
+    from fve_dg_b200 import _lib as L
+    m = box_mesh(2)
+    lib = L.lib()
+    d = m.desc()
+    err = ctypes.c_int(0)
+    owner = np.zeros(m.ncell, dtype=np.int32)
+    op = owner.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    assert not lib.dg_partition_create(ctypes.byref(d), op, 1, ctypes.byref(err))  # rank beyond the parts
+    assert err.value == -1
+    owner[3] = -2
+    assert not lib.dg_partition_create(ctypes.byref(d), op, 0, ctypes.byref(err))  # negative owner
+    assert err.value == -1
+    assert not lib.dg_partition_create(None, op, 0, ctypes.byref(err))
+    owner[:] = 0
+    h = lib.dg_partition_create(ctypes.byref(d), op, 0, ctypes.byref(err))  # one part: no ghosts, no peers
+    assert h and err.value == 0
+    no, ng = ctypes.c_int64(), ctypes.c_int64()
+    ns, nr = ctypes.c_int(), ctypes.c_int()
+    assert lib.dg_partition_counts(h, ctypes.byref(no), ctypes.byref(ng), ctypes.byref(ns), ctypes.byref(nr)) == 0
+    assert (no.value, ng.value, ns.value, nr.value) == (m.ncell, 0, 0, 0)
+    assert lib.dg_partition_send(h, 0, None, None, None) == -1
+    lib.dg_partition_destroy(h)
